@@ -1,0 +1,308 @@
+"""Benchmark of the retarded-interaction time step on B200.
+
+Workload (default): N = 4096 dots uniform in a centred 0.2 cube (seeded),
+omega_0 ~ N(200, 0.5^2), T1 = T2 = 10, unit-random dipoles x 2e-3, Gaussian
+pulse (15, 5, 1, 200, (200,0,0), (0,0,1)), c = 1, hbar = 1, mu0 = 1,
+omega_L = 200, dt = 1e-3, 20000 steps, interpolation order 5, FP64 per-pair
+coefficient table.  A "step" is one time step of the integrator: the pair sum
+over all N(N-1)/2 pairs and 6 taps, then predictor + 11 evaluations + 10
+corrections for every dot.
+
+Metric: pair-updates/s = N^2 * steps / time (each ordered pair advanced one
+step counts once; the reference evaluates the pair sum 11 times per step,
+this implementation once plus the delay-0 terms per iteration, both credited
+the same N^2 per step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun), every rank advances its own independent ensemble
+(seed + rank) on its GPU: weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from quest_b200 import inputs as I  # noqa: E402
+
+FALLBACK_HBM_GBS = 6650.0
+TABLE_BYTES_PER_PAIR = lambda q: 4 + 16 * (q + 1)  # noqa: E731  int32 delay + (q+1) complex128
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch of the sweep kernel from the committed ncu
+    summary (profiles/<name>.md, line 'traffic_bytes_per_launch: X')."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"quest_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxs.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sms:
+            return None
+        return {"sm_mhz": float(np.median(sms)), "sm_max_mhz": float(max(maxs)), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def workload(args, rank: int) -> I.Workload:
+    return I.plain_table(seed=2 + rank, n=args.n, steps=args.warmup + args.steps, pulse_delay=args.pulse_delay)
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(args, kind="port"):
+    """The reference algorithm (faithful oracle: 11 full pair sweeps per step,
+    single thread like the reference) on a bounded sample of the workload:
+    `steps` steps from step t0 >= the largest delay on a synthetic history."""
+    from oracle import oracle as O
+    from quest_b200 import capi
+    wl = I.plain_table(seed=2, n=args.n, steps=args.cpu_t0 + args.cpu_steps)
+    c = wl.constants
+    ps, cs, fc = capi.pc_weights()
+    w = O.Weights(ps, cs, fc)
+    delays, coefs = O.build_table(wl.dots, c)
+    n = wl.n
+    T = c.num_timesteps
+    rng = np.random.default_rng(0)
+    hist = np.zeros((n, T + O.WINDOW, 2, 2), dtype=np.complex128)
+    hist[:, :, 0, 0] = 1.0
+    hist[:, : args.cpu_t0 + O.WINDOW, 0, 1] = 1e-4 * (rng.normal(size=(n, args.cpu_t0 + O.WINDOW)) +
+                                                     1j * rng.normal(size=(n, args.cpu_t0 + O.WINDOW)))
+    t0 = time.perf_counter()
+    done = O.faithful_steps(wl.dots, wl.pulse, c, w, T, delays, coefs, hist, args.cpu_t0, args.cpu_steps)
+    dt = time.perf_counter() - t0
+    value = n * n * done / dt
+    return {"value": value, "unit": "pair-updates/s", "cores": 1, "kind": kind,
+            "sample": f"N={n}, {done} faithful steps (11 full pair sweeps each) from step {args.cpu_t0} "
+                      f"on a synthetic history, {dt:.2f} s; table build not timed"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, args.cpu_steps))
+    a = argparse.Namespace(**vars(args))
+    a.cpu_steps = steps
+    base = cpu_baseline(a)
+    line = {"impl": "reference", "metric": "pair-updates/s", "value": base["value"], "unit": "pair-updates/s",
+            "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": args.n * args.n / base["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(args),
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "pair-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": f"fp64_table_N{args.n}_T{args.warmup + args.steps}", "N": args.n,
+            "steps_total": args.warmup + args.steps, "interpolation_order": 5, "side": 0.2,
+            "dt": 1e-3, "c0": 1.0, "hbar": 1.0, "mu0": 1.0, "laser_frequency": 200.0,
+            "pulse_delay": args.pulse_delay, "precision": "fp64", "coef_mode": "table",
+            "l2": "inputs larger than L2 (coefficient table %.0f MB > 126 MB)" %
+                  (args.n * (args.n - 1) / 2 * TABLE_BYTES_PER_PAIR(5) / 1e6),
+            "parallelism": "independent ensemble per GPU" if int(os.environ.get("WORLD_SIZE", "1")) > 1
+            else "1 GPU"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from quest_b200 import capi
+    torch.cuda.set_device(local)
+    wl = workload(args, rank)
+    n = wl.n
+    total = args.warmup + args.steps
+    weights = capi.pc_weights()
+
+    # ---- device-resident throughput (value) and the sweep kernel's roofline
+    sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights)
+    info = sim.info()
+    sim.run(args.warmup, record=False)
+    sim.set_option("profile", 1)
+    sim.kernel_time(reset=True)
+    stream = torch.cuda.ExternalStream(capi.lib().qg_stream(sim.h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        e0.record(stream)
+        sim.run(args.steps, record=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    pair_ms, launches = sim.kernel_time()
+    sim.close()
+    ms_max = max_over_ranks(ms, world)
+    value = world * n * n * args.steps / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI with host buffers: create (dots
+    # upload + table build), every step's rho (N x 2 complex) copied back
+    rho_host = np.empty((total, n, 2), dtype=np.complex128)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights) as sim2:
+        sim2.run(total, out=rho_host)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+    e2e_value = world * n * n * total / e2e_s
+
+    hbm, src = peaks()
+    q = 5
+    alg_bytes = info["num_pairs"] * TABLE_BYTES_PER_PAIR(q)
+    avg_ms = pair_ms / max(launches, 1)
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    traffic = profile_traffic("sweep_table_fp64_N4096")
+    line = {
+        "metric": "pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded dots and pulse of the stated distributions)",
+        "config": config_dict(args),
+        "roofline": {"bound": "hbm", "kernel": "sweep_table_kernel<5>", "achieved": achieved, "peak": hbm,
+                     "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+                     "share_of_step": pair_ms / ms if ms > 0 else None},
+        "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s,
+                "h2d_bytes_per_step": (n * 72 + 80) / total, "d2h_bytes_per_step": n * 32,
+                "includes": "qg_create (dots upload + table build) + qg_run with every step's rho read back"},
+        "gpu_launches": launches + args.steps * (1 if info["fused_step"] else 12),
+        "near_pairs": info["near_pairs"], "max_delay": info["max_delay"],
+        "table_build_ms": info["table_build_ms"],
+    }
+    cs = clocks.summary()
+    if cs is not None:
+        line["clocks"] = cs
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=19950)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--pulse-delay", type=float, default=5.0)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-t0", type=int, default=400)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,194 @@
+/*
+ * quest_gpu.h -- C ABI of the B200 (sm_100a) implementation of QuEST's
+ * retarded-interaction time step.
+ *
+ * The reference (cglosser/QuEST) exposes the path through three C++
+ * interfaces.  Each entry point below names the one it replaces:
+ *
+ *   Interaction::evaluate(int)          src/interactions/interaction.h:16
+ *   HistoryInteraction (ctor, table)    src/interactions/history_interaction.h:16-21,
+ *                                       history_interaction.cpp:5-45
+ *   HistoryInteraction::evaluate        history_interaction.cpp:47-70
+ *   PulseInteraction::evaluate          src/interactions/pulse_interaction.cpp:9-20
+ *   History::HistoryArray               src/history.h:13-14, history.cpp:3-9
+ *   PredictorCorrector::Weights         src/integrator.h:23-33, integrator.cpp:5-102
+ *   PredictorCorrector::Integrator      src/integrator.h:35-41, integrator.cpp:104-207
+ *
+ * Conventions.
+ *  - Complex numbers are interleaved double[2] (layout-compatible with
+ *    std::complex<double> and Eigen::Vector2cd components).
+ *  - Dots and pulses use the field order of the reference's dots.cfg and
+ *    pulse.cfg lines (src/quantum_dot.cpp:33-38, src/pulse.cpp:29-35).
+ *  - All host pointers are plain host memory; the library copies.
+ *  - Every call returns a qg_status; qg_last_error() gives the message of the
+ *    last failure on the calling thread.
+ *  - One handle owns one CUDA stream and its device state.  Calls on the same
+ *    handle must not overlap (the reference's objects are not reentrant
+ *    either); different handles are independent.
+ *  - The library allocates its device memory in qg_create and frees it in
+ *    qg_destroy; no call in between allocates device memory.
+ */
+#ifndef QUEST_GPU_H
+#define QUEST_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  QG_OK = 0,
+  QG_ERR_INVALID_ARG = 1,  /* a size, pointer or option is out of range */
+  QG_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  QG_ERR_OOM = 3,          /* device memory exhausted */
+  QG_ERR_NONFINITE = 4,    /* non-finite history: the reference's
+                              std::domain_error("unbounded history values at
+                              or before step N"), integrator.cpp:200-207 */
+  QG_ERR_UNSUPPORTED = 5   /* valid request this build does not implement */
+} qg_status;
+
+/* One quantum dot: x y z omega_0 T1 T2 dx dy dz (QuantumDot,
+ * src/quantum_dot.h:21-48). */
+typedef struct {
+  double pos[3];
+  double freq;
+  double t1, t2;
+  double dip[3];
+} qg_dot;
+
+/* Incident Gaussian pulse: E_0 delay sigma omega_L k p (Pulse,
+ * src/pulse.h:10-24).  The polarisation is used as given, matching the
+ * reference's read_pulse_config (pulse.cpp:29-45), which does not normalise. */
+typedef struct {
+  double amplitude, delay, width, freq;
+  double wavevector[3];
+  double polarization[3];
+} qg_pulse;
+
+typedef enum { QG_FRAME_ROTATING = 0, QG_FRAME_LAB = 1 } qg_frame;
+typedef enum { QG_PREC_FP64 = 0, QG_PREC_MIXED = 1 } qg_precision;
+typedef enum { QG_COEF_AUTO = 0, QG_COEF_TABLE = 1, QG_COEF_ON_THE_FLY = 2 } qg_coef_mode;
+
+/* Everything the reference reads from its global `config`
+ * (src/configuration.h:12-19) plus this library's options. */
+typedef struct {
+  double c0, hbar, mu0;
+  double laser_frequency;   /* config.omega: rotating frame and detuning */
+  double dt;
+  int interpolation_order;  /* q, 1..7 */
+  int num_timesteps;        /* T: steps 0..T-1, as config.num_timesteps */
+  int frame;                /* qg_frame */
+  int precision;            /* qg_precision */
+  int coef_mode;            /* qg_coef_mode */
+  int reserved[3];          /* must be zero */
+} qg_params;
+
+/* Predictor-corrector weights in the layout of PredictorCorrector::Weights:
+ * ps and cs are 2 x n_time row-major (row 0 for rho, row 1 for rho-dot
+ * already scaled by (n_time-1)/2), future_coef the corrector's weight on the
+ * new derivative. */
+typedef struct {
+  int n_time;               /* history width; the reference uses 22 */
+  double ps[2 * 32];
+  double cs[2 * 32];
+  double future_coef;
+} qg_weights;
+
+typedef struct qg_handle_s qg_handle;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *qg_last_error(void);
+
+/* Library version string. */
+const char *qg_version(void);
+
+/* PredictorCorrector::Weights(n_lambda, n_time, radius)
+ * (integrator.cpp:85-102): the contour-fitted weights, computed as the exact
+ * minimum-norm solution in 113-bit floating point and rounded to double (the
+ * fit's condition number is about 3e13, so double-precision solvers disagree
+ * in the third digit).  n_time <= 32. */
+qg_status qg_pc_weights(int n_lambda, int n_time, double radius, qg_weights *out);
+
+/* Builds the device state for N dots: HistoryInteraction's constructor and
+ * coefficient table (history_interaction.cpp:5-45), PulseInteraction, the
+ * History array initialised as main.cpp:30-36 does (rho = (1,0) for
+ * t <= 0), and the Integrator's weights.  weights == NULL uses
+ * qg_pc_weights(18, 22, 3.15), the values main.cpp:48-49 hard-codes. */
+qg_status qg_create(const qg_dot *dots, int n, const qg_pulse *pulse,
+                    const qg_params *params, const qg_weights *weights,
+                    qg_handle **out);
+
+qg_status qg_destroy(qg_handle *h);
+
+/* Integrator::solve over steps [next, next + n_steps) (integrator.cpp:120-140):
+ * predictor, evaluation, 10 x (corrector, evaluation) per step, with the
+ * pair sum over all N(N-1)/2 pairs and q+1 interpolation taps.
+ * rho_out (nullable): n_steps * N * 2 complex = (rho00, rho01) per dot per
+ * step, the rows History::write_history prints (history.cpp:27-33).
+ * On a non-finite value returns QG_ERR_NONFINITE with *bad_step (nullable)
+ * set to the first such step, as throw_if_unbounded_solution does.  Steps
+ * past num_timesteps are an error. */
+qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad_step);
+
+/* Index of the next step qg_run will compute. */
+qg_status qg_next_step(const qg_handle *h, int *step);
+
+/* HistoryInteraction::evaluate(step) (history_interaction.cpp:47-70):
+ * field[i] = sum over pairs and taps of coefficient * prefactor(rho01 of the
+ * partner at the retarded step).  rho01_step (nullable, N complex) first
+ * overwrites the history's rho01 at `step` (the integrator's current
+ * iterate); field_out receives N complex. */
+qg_status qg_history_evaluate(qg_handle *h, int step, const double *rho01_step,
+                              double *field_out);
+
+/* PulseInteraction::evaluate(step) (pulse_interaction.cpp:9-20): N complex. */
+qg_status qg_pulse_evaluate(qg_handle *h, int step, double *field_out);
+
+/* Writes rho01 (N complex per step, user order) for steps [t0, t0 + n) into
+ * the device history that the pair sum reads, as a caller filling
+ * History::HistoryArray[.][t][0][1] would.  t0 >= -22.  The device keeps the
+ * last W steps per dot (W = max delay + q + 2, qg_info.ring_depth); a step
+ * older than that is overwritten by later ones.  The integrator's own window
+ * (rho, rho-dot of the last 22 steps) is not changed. */
+qg_status qg_set_history(qg_handle *h, int t0, int n, const double *rho01);
+
+/* Reads back rho01 for steps [t0, t0 + n) still held on the device: N
+ * complex per step. */
+qg_status qg_get_history(qg_handle *h, int t0, int n, double *rho01_out);
+
+/* Diagnostics of the built state. */
+typedef struct {
+  int n;                 /* dots */
+  int max_delay;         /* largest floor delay over all pairs */
+  int ring_depth;        /* W: rho01 steps kept per dot */
+  long long num_pairs;   /* N(N-1)/2 */
+  long long near_pairs;  /* pairs with floor delay 0 (current-step coupling) */
+  int coef_mode;         /* resolved qg_coef_mode */
+  int precision;         /* qg_precision */
+  int fused_step;        /* 1 when all current-step coupling fits one block */
+  size_t device_bytes;   /* device memory held by the handle */
+  double table_build_ms; /* time of the coefficient-table kernel */
+} qg_info;
+
+qg_status qg_get_info(const qg_handle *h, qg_info *info);
+
+/* Device memory a handle with these inputs would hold (admission control). */
+qg_status qg_footprint(int n, const qg_params *params, double side, size_t *bytes);
+
+/* Timing hooks: the handle's cudaStream_t (as void*), and the device time in
+ * milliseconds of the pair-sum kernel, accumulated over qg_run calls made
+ * while the "profile" option is on. */
+void *qg_stream(qg_handle *h);
+qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *launches);
+
+/* Options: "graph" (1 = replay each step as a CUDA graph, default),
+ * "profile" (1 = launch per step with CUDA events around the pair-sum
+ * kernel), "reset" (restart the history at step 0, main.cpp:30-36). */
+qg_status qg_set_option(qg_handle *h, const char *key, int value);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,862 @@
+// C ABI of the library: handle lifetime, device memory, the step loop.
+//
+// A handle corresponds to the objects the reference's main() builds
+// (src/main.cpp:25-52): the dots, the History array, the PulseInteraction,
+// the HistoryInteraction with its coefficient table, and the
+// PredictorCorrector::Integrator.  Device memory is allocated once in
+// qg_create and released in qg_destroy.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "qg_internal.h"
+
+using namespace qg;
+
+static thread_local std::string g_last_error;
+
+qg_status qg_fail(qg_status code, const char *fmt, ...)
+{
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+extern "C" const char *qg_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *qg_version(void) { return "quest_b200 0.1 (sm_100a)"; }
+
+#define QG_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t err_ = (call);                                                               \
+    if(err_ != cudaSuccess) {                                                                \
+      qg_status code_ = (err_ == cudaErrorMemoryAllocation) ? QG_ERR_OOM : QG_ERR_CUDA;      \
+      return qg_fail(code_, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_),        \
+                     __FILE__, __LINE__);                                                    \
+    }                                                                                        \
+  } while(0)
+
+struct qg_handle_s {
+  int n = 0, n_pad = 0, nT = 0, q = 0, T = 0;
+  long long nblk = 0, P = 0;
+  qg_params params{};
+  qg_pulse pulse{};
+  PCW w{};
+  int device = 0;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+
+  std::vector<void *> allocs;
+  size_t bytes = 0;
+
+  double *d_pos = nullptr, *d_dip = nullptr, *d_freq = nullptr, *d_t1 = nullptr, *d_t2 = nullptr;
+  int *d_user = nullptr, *d_slot_dot = nullptr;
+  int *d_delay = nullptr;
+  double2 *d_coef = nullptr;
+  double2 *d_ring = nullptr;
+  int W = 0, stride = 0;
+  double2 *d_pcr = nullptr, *d_partial = nullptr, *d_scratch = nullptr;
+  int *d_fnear_ptr = nullptr, *d_fnear_idx = nullptr;  // fused: by slot, local partner
+  double2 *d_fnear_coef = nullptr;
+  int *d_gnear_ptr = nullptr, *d_gnear_idx = nullptr;  // general: by internal index
+  double2 *d_gnear_coef = nullptr;
+  int *d_ints = nullptr;  // 0 step, 1 done, 2 bad, 3 traj_t0, 4 eval_step, 5 max_delay
+  unsigned long long *d_u64 = nullptr;
+  double2 *d_traj = nullptr;  // 2 * traj_k steps x N x 2
+  double2 *h_traj = nullptr;  // pinned, same size
+  int traj_k = 0;
+  double2 *d_io = nullptr;    // N complex device staging for evaluate / set_history
+  double2 *h_io = nullptr;    // pinned N complex
+
+  bool fused = true;
+  int step_blocks = 0;
+  int max_delay = 0;
+  long long near_pairs = 0;
+  double table_ms = 0;
+  int next_step = 0;
+  int eval_cached = -0x7fffffff;
+
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [traj off, traj on]
+  bool use_graph = true;
+  bool profile = false;
+  cudaEvent_t ev_a[256], ev_b[256];
+  bool events_ready = false;
+  double pair_ms = 0;
+  int pair_launches = 0;
+  cudaEvent_t ev_chunk[2], ev_copy[2];
+
+  SweepArgs sweep_args() const
+  {
+    SweepArgs s{};
+    s.delay = d_delay;
+    s.coef = d_coef;
+    s.ring = d_ring;
+    s.partial = d_partial;
+    s.n_pad = n_pad;
+    s.nT = nT;
+    s.W = W;
+    s.stride = stride;
+    s.q = q;
+    s.frame = params.frame;
+    s.nblk = nblk;
+    s.d_step = d_ints + 0;
+    s.d_bad = d_ints + 2;
+    return s;
+  }
+
+  StepArgs step_args(bool general) const
+  {
+    StepArgs a{};
+    a.n = n;
+    a.n_pad = n_pad;
+    a.nT = nT;
+    a.W = W;
+    a.stride = stride;
+    a.q = q;
+    a.frame = params.frame;
+    a.dt = params.dt;
+    a.laser_freq = params.laser_frequency;
+    a.hbar = params.hbar;
+    for(int k = 0; k < 3; ++k) {
+      a.pulse.amp_pol[k] = pulse.amplitude / 2 * pulse.polarization[k];
+      a.pulse.k[k] = pulse.wavevector[k];
+    }
+    a.pulse.freq = pulse.freq;
+    a.pulse.delay = pulse.delay;
+    a.pulse.width = pulse.width;
+    a.pos = d_pos;
+    a.dip = d_dip;
+    a.freq = d_freq;
+    a.t1 = d_t1;
+    a.t2 = d_t2;
+    a.slot_dot = d_slot_dot;
+    a.user = d_user;
+    a.partial = d_partial;
+    a.pcr = d_pcr;
+    a.ring = d_ring;
+    a.near_ptr = general ? d_gnear_ptr : d_fnear_ptr;
+    a.near_idx = general ? d_gnear_idx : d_fnear_idx;
+    a.near_coef = general ? d_gnear_coef : d_fnear_coef;
+    a.scratch = d_scratch;
+    a.traj = nullptr;
+    a.traj_t0 = d_ints + 3;
+    a.d_step = d_ints + 0;
+    a.d_done = d_ints + 1;
+    a.d_bad = d_ints + 2;
+    a.w = w;
+    return a;
+  }
+};
+
+template <typename T>
+static qg_status dalloc(qg_handle *h, T **p, size_t count)
+{
+  void *ptr = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&ptr, bytes);
+  if(e != cudaSuccess) {
+    cudaGetLastError();
+    return qg_fail(e == cudaErrorMemoryAllocation ? QG_ERR_OOM : QG_ERR_CUDA,
+                   "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  h->allocs.push_back(ptr);
+  h->bytes += bytes;
+  *p = (T *)ptr;
+  return QG_OK;
+}
+
+#define QG_TRY(expr)                 \
+  do {                               \
+    qg_status st_ = (expr);          \
+    if(st_ != QG_OK) return st_;     \
+  } while(0)
+
+static void destroy_handle(qg_handle *h)
+{
+  if(!h) return;
+  if(h->stream) cudaStreamSynchronize(h->stream);
+  if(h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  for(auto &g : h->graph)
+    if(g) cudaGraphExecDestroy(g);
+  if(h->events_ready) {
+    for(int i = 0; i < 256; ++i) {
+      cudaEventDestroy(h->ev_a[i]);
+      cudaEventDestroy(h->ev_b[i]);
+    }
+    for(int i = 0; i < 2; ++i) {
+      cudaEventDestroy(h->ev_chunk[i]);
+      cudaEventDestroy(h->ev_copy[i]);
+    }
+  }
+  for(void *p : h->allocs) cudaFree(p);
+  if(h->h_traj) cudaFreeHost(h->h_traj);
+  if(h->h_io) cudaFreeHost(h->h_io);
+  if(h->stream) cudaStreamDestroy(h->stream);
+  if(h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  delete h;
+}
+
+// Morton (Z-order) key of a position quantised to 21 bits per axis.
+static inline uint64_t spread3(uint64_t x)
+{
+  x &= 0x1fffff;
+  x = (x | x << 32) & 0x1f00000000ffffULL;
+  x = (x | x << 16) & 0x1f0000ff0000ffULL;
+  x = (x | x << 8) & 0x100f00f00f00f00fULL;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+  x = (x | x << 2) & 0x1249249249249249ULL;
+  return x;
+}
+
+static std::vector<int> morton_order(const qg_dot *dots, int n)
+{
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for(int i = 0; i < n; ++i)
+    for(int k = 0; k < 3; ++k) {
+      const double v = dots[i].pos[k];
+      if(std::isfinite(v)) {
+        lo[k] = std::min(lo[k], v);
+        hi[k] = std::max(hi[k], v);
+      }
+    }
+  double ext = 0;
+  for(int k = 0; k < 3; ++k)
+    if(hi[k] > lo[k]) ext = std::max(ext, hi[k] - lo[k]);
+  std::vector<std::pair<uint64_t, int>> keys(n);
+  for(int i = 0; i < n; ++i) {
+    uint64_t code = 0;
+    for(int k = 0; k < 3; ++k) {
+      double v = dots[i].pos[k];
+      double f = (ext > 0 && std::isfinite(v)) ? (v - lo[k]) / ext : 0.0;
+      f = std::min(std::max(f, 0.0), 1.0);
+      code |= spread3((uint64_t)(f * 2097151.0)) << k;
+    }
+    keys[i] = {code, i};
+  }
+  std::sort(keys.begin(), keys.end());
+  std::vector<int> perm(n);
+  for(int i = 0; i < n; ++i) perm[i] = keys[i].second;
+  return perm;
+}
+
+// Union-find over the current-step (delay 0) coupling graph.
+struct DSU {
+  std::vector<int> p;
+  explicit DSU(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
+  int find(int x)
+  {
+    while(p[x] != x) x = p[x] = p[p[x]];
+    return x;
+  }
+  void unite(int a, int b) { p[find(a)] = find(b); }
+};
+
+static qg_status validate(const qg_dot *dots, int n, const qg_pulse *pulse, const qg_params *p)
+{
+  if(!dots || !pulse || !p) return qg_fail(QG_ERR_INVALID_ARG, "qg_create: NULL argument");
+  if(n < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_create: need at least one dot (n = %d)", n);
+  if(n > (1 << 24)) return qg_fail(QG_ERR_INVALID_ARG, "qg_create: n = %d exceeds 2^24", n);
+  if(p->interpolation_order < 1 || p->interpolation_order > kMaxOrder)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_create: interpolation_order %d outside [1, %d]",
+                   p->interpolation_order, kMaxOrder);
+  if(!(p->dt > 0) || !(p->c0 > 0) || !(p->hbar != 0) || !std::isfinite(p->dt))
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_create: dt and c0 must be positive, hbar non-zero");
+  if(p->num_timesteps < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_create: num_timesteps < 0");
+  if(p->frame != QG_FRAME_ROTATING && p->frame != QG_FRAME_LAB)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown frame %d", p->frame);
+  if(p->precision != QG_PREC_FP64)
+    return qg_fail(QG_ERR_UNSUPPORTED, "qg_create: only QG_PREC_FP64 is built in this handle type");
+  if(p->coef_mode == QG_COEF_ON_THE_FLY)
+    return qg_fail(QG_ERR_UNSUPPORTED, "qg_create: on-the-fly coefficients use qg_otf_* handles");
+  if(p->coef_mode != QG_COEF_AUTO && p->coef_mode != QG_COEF_TABLE)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown coef_mode %d", p->coef_mode);
+  return QG_OK;
+}
+
+static size_t table_bytes(long long nblk, int q)
+{
+  return (size_t)nblk * kTilePairs * (sizeof(int) + sizeof(double2) * (q + 1));
+}
+
+static qg_status build_near(qg_handle *h)
+{
+  // 1. extract delay-0 pairs
+  const unsigned long long cap = (unsigned long long)std::max<long long>(h->near_pairs, 1);
+  int *d_pairs = nullptr;
+  double2 *d_nc = nullptr;
+  QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 2 * cap));
+  QG_CUDA(cudaMalloc(&d_nc, sizeof(double2) * cap));
+  QG_CUDA(cudaMemsetAsync(h->d_u64 + 1, 0, sizeof(unsigned long long), h->stream));
+  if(h->near_pairs > 0)
+    launch_near_extract(h->d_delay, h->d_coef, h->nblk, h->nT, h->q, d_pairs, d_nc, h->d_u64 + 1, cap,
+                        h->stream);
+  std::vector<int> pairs(2 * cap);
+  std::vector<double2> nc(cap);
+  QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 2 * cap, cudaMemcpyDeviceToHost,
+                          h->stream));
+  QG_CUDA(cudaMemcpyAsync(nc.data(), d_nc, sizeof(double2) * cap, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaFree(d_pairs);
+  cudaFree(d_nc);
+  const long long m = h->near_pairs;
+
+  // 2. general CSR by internal index (both directions), sorted partners
+  const int n = h->n;
+  std::vector<std::vector<std::pair<int, double2>>> adj(n);
+  DSU dsu(n);
+  for(long long k = 0; k < m; ++k) {
+    const int a = pairs[2 * k], b = pairs[2 * k + 1];
+    adj[a].push_back({b, nc[k]});
+    adj[b].push_back({a, nc[k]});
+    dsu.unite(a, b);
+  }
+  for(auto &v : adj)
+    std::sort(v.begin(), v.end(), [](const std::pair<int, double2> &x,
+                                     const std::pair<int, double2> &y) { return x.first < y.first; });
+  std::vector<int> gptr(n + 1, 0), gidx;
+  std::vector<double2> gcoef;
+  gidx.reserve(2 * m);
+  gcoef.reserve(2 * m);
+  for(int i = 0; i < n; ++i) {
+    for(auto &e : adj[i]) {
+      gidx.push_back(e.first);
+      gcoef.push_back(e.second);
+    }
+    gptr[i + 1] = (int)gidx.size();
+  }
+
+  // 3. pack connected components into step blocks (fused form)
+  std::vector<std::vector<int>> comps;
+  {
+    std::vector<int> root_to_comp(n, -1);
+    for(int i = 0; i < n; ++i) {
+      if(adj[i].empty()) continue;
+      const int r = dsu.find(i);
+      if(root_to_comp[r] < 0) {
+        root_to_comp[r] = (int)comps.size();
+        comps.emplace_back();
+      }
+      comps[root_to_comp[r]].push_back(i);
+    }
+  }
+  size_t largest = 0;
+  for(auto &c : comps) largest = std::max(largest, c.size());
+  h->fused = largest <= (size_t)kStepBlock;
+  std::vector<int> slot_dot;
+  std::vector<int> fptr(1, 0), fidx;
+  std::vector<double2> fcoef;
+  if(h->fused) {
+    std::sort(comps.begin(), comps.end(),
+              [](const std::vector<int> &x, const std::vector<int> &y) { return x.size() > y.size(); });
+    std::vector<std::vector<int>> bins;
+    for(auto &c : comps) {
+      size_t b = 0;
+      for(; b < bins.size(); ++b)
+        if(bins[b].size() + c.size() <= (size_t)kStepBlock) break;
+      if(b == bins.size()) bins.emplace_back();
+      bins[b].insert(bins[b].end(), c.begin(), c.end());
+    }
+    size_t fill = 0;
+    for(int i = 0; i < n; ++i) {
+      if(!adj[i].empty()) continue;
+      while(fill < bins.size() && bins[fill].size() >= (size_t)kStepBlock) ++fill;
+      if(fill == bins.size()) bins.emplace_back();
+      bins[fill].push_back(i);
+    }
+    h->step_blocks = (int)bins.size();
+    slot_dot.assign((size_t)h->step_blocks * kStepBlock, -1);
+    std::vector<int> local(n, -1);
+    for(size_t b = 0; b < bins.size(); ++b)
+      for(size_t j = 0; j < bins[b].size(); ++j) {
+        slot_dot[b * kStepBlock + j] = bins[b][j];
+        local[bins[b][j]] = (int)j;
+      }
+    for(size_t s = 0; s < slot_dot.size(); ++s) {
+      const int i = slot_dot[s];
+      if(i >= 0)
+        for(auto &e : adj[i]) {
+          fidx.push_back(local[e.first]);
+          fcoef.push_back(e.second);
+        }
+      fptr.push_back((int)fidx.size());
+    }
+  } else {
+    h->step_blocks = (n + kStepBlock - 1) / kStepBlock;
+    slot_dot.assign((size_t)h->step_blocks * kStepBlock, -1);
+    for(int i = 0; i < n; ++i) slot_dot[i] = i;
+    fptr.assign(slot_dot.size() + 1, 0);
+  }
+
+  QG_TRY(dalloc(h, &h->d_gnear_ptr, gptr.size()));
+  QG_TRY(dalloc(h, &h->d_gnear_idx, gidx.size()));
+  QG_TRY(dalloc(h, &h->d_gnear_coef, gcoef.size()));
+  QG_TRY(dalloc(h, &h->d_fnear_ptr, fptr.size()));
+  QG_TRY(dalloc(h, &h->d_fnear_idx, fidx.size()));
+  QG_TRY(dalloc(h, &h->d_fnear_coef, fcoef.size()));
+  QG_TRY(dalloc(h, &h->d_slot_dot, slot_dot.size()));
+  QG_CUDA(cudaMemcpy(h->d_gnear_ptr, gptr.data(), sizeof(int) * gptr.size(), cudaMemcpyHostToDevice));
+  if(!gidx.empty()) {
+    QG_CUDA(cudaMemcpy(h->d_gnear_idx, gidx.data(), sizeof(int) * gidx.size(), cudaMemcpyHostToDevice));
+    QG_CUDA(cudaMemcpy(h->d_gnear_coef, gcoef.data(), sizeof(double2) * gcoef.size(),
+                       cudaMemcpyHostToDevice));
+  }
+  QG_CUDA(cudaMemcpy(h->d_fnear_ptr, fptr.data(), sizeof(int) * fptr.size(), cudaMemcpyHostToDevice));
+  if(!fidx.empty()) {
+    QG_CUDA(cudaMemcpy(h->d_fnear_idx, fidx.data(), sizeof(int) * fidx.size(), cudaMemcpyHostToDevice));
+    QG_CUDA(cudaMemcpy(h->d_fnear_coef, fcoef.data(), sizeof(double2) * fcoef.size(),
+                       cudaMemcpyHostToDevice));
+  }
+  QG_CUDA(cudaMemcpy(h->d_slot_dot, slot_dot.data(), sizeof(int) * slot_dot.size(),
+                     cudaMemcpyHostToDevice));
+  return QG_OK;
+}
+
+static qg_status reset_state(qg_handle *h)
+{
+  QG_CUDA(cudaMemsetAsync(h->d_ring, 0, sizeof(double2) * (size_t)h->n_pad * h->stride, h->stream));
+  QG_CUDA(cudaMemsetAsync(h->d_partial, 0, sizeof(double2) * (size_t)h->nT * h->n_pad, h->stream));
+  launch_init_state(h->step_args(false), h->stream);
+  int init[6] = {0, 0, kBadNone, 0, 0, 0};
+  QG_CUDA(cudaMemcpyAsync(h->d_ints, init, sizeof(int) * 5, cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  h->next_step = 0;
+  h->eval_cached = -0x7fffffff;
+  return QG_OK;
+}
+
+static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, const qg_params *p,
+                             const qg_weights *weights, qg_handle *h)
+{
+  QG_CUDA(cudaGetDevice(&h->device));
+  QG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  QG_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  h->n = n;
+  h->q = p->interpolation_order;
+  h->T = p->num_timesteps;
+  h->params = *p;
+  h->pulse = *pulse;
+  h->nT = (n + kTile - 1) / kTile;
+  h->n_pad = h->nT * kTile;
+  h->nblk = (long long)h->nT * (h->nT + 1) / 2;
+  h->P = (long long)n * (n - 1) / 2;
+
+  qg_weights wt;
+  if(weights) {
+    wt = *weights;
+    if(wt.n_time < 2 || wt.n_time > 32)
+      return qg_fail(QG_ERR_INVALID_ARG, "qg_create: weights.n_time %d outside [2, 32]", wt.n_time);
+    if(wt.n_time > kWindow)
+      return qg_fail(QG_ERR_UNSUPPORTED, "qg_create: weights.n_time %d exceeds the 22-step window",
+                     wt.n_time);
+  } else {
+    QG_TRY(qg_pc_weights(18, 22, 3.15, &wt));
+  }
+  h->w.n_time = wt.n_time;
+  for(int i = 0; i < 2 * wt.n_time; ++i) {
+    h->w.ps[i] = wt.ps[i];
+    h->w.cs[i] = wt.cs[i];
+  }
+  h->w.fc = wt.future_coef;
+
+  // internal order
+  const std::vector<int> perm = morton_order(dots, n);
+  std::vector<double> pos((size_t)h->n_pad * 3, 0.0), dip((size_t)h->n_pad * 3, 0.0);
+  std::vector<double> fr(h->n_pad, 0.0), t1(h->n_pad, 1.0), t2(h->n_pad, 1.0);
+  std::vector<int> user(h->n_pad, -1);
+  for(int i = 0; i < n; ++i) {
+    const qg_dot &d = dots[perm[i]];
+    for(int k = 0; k < 3; ++k) {
+      pos[3 * i + k] = d.pos[k];
+      dip[3 * i + k] = d.dip[k];
+    }
+    fr[i] = d.freq;
+    t1[i] = d.t1;
+    t2[i] = d.t2;
+    user[i] = perm[i];
+  }
+  QG_TRY(dalloc(h, &h->d_pos, pos.size()));
+  QG_TRY(dalloc(h, &h->d_dip, dip.size()));
+  QG_TRY(dalloc(h, &h->d_freq, fr.size()));
+  QG_TRY(dalloc(h, &h->d_t1, t1.size()));
+  QG_TRY(dalloc(h, &h->d_t2, t2.size()));
+  QG_TRY(dalloc(h, &h->d_user, user.size()));
+  QG_CUDA(cudaMemcpy(h->d_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpy(h->d_dip, dip.data(), sizeof(double) * dip.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpy(h->d_freq, fr.data(), sizeof(double) * fr.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpy(h->d_t1, t1.data(), sizeof(double) * t1.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpy(h->d_t2, t2.data(), sizeof(double) * t2.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpy(h->d_user, user.data(), sizeof(int) * user.size(), cudaMemcpyHostToDevice));
+  QG_TRY(dalloc(h, &h->d_ints, 16));
+  QG_TRY(dalloc(h, &h->d_u64, 4));
+  QG_CUDA(cudaMemset(h->d_ints, 0, sizeof(int) * 16));
+  QG_CUDA(cudaMemset(h->d_u64, 0, sizeof(unsigned long long) * 4));
+
+  // coefficient table
+  const size_t tb = table_bytes(h->nblk, h->q);
+  size_t free_b = 0, total_b = 0;
+  QG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if(tb > free_b * 0.9)
+    return qg_fail(QG_ERR_OOM, "qg_create: coefficient table needs %zu bytes, %zu free", tb, free_b);
+  QG_TRY(dalloc(h, &h->d_delay, (size_t)h->nblk * kTilePairs));
+  QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nblk * kTilePairs * (h->q + 1)));
+  TableArgs ta{};
+  ta.pos = h->d_pos;
+  ta.dip = h->d_dip;
+  ta.user = h->d_user;
+  ta.n = n;
+  ta.n_pad = h->n_pad;
+  ta.nT = h->nT;
+  ta.nblk = h->nblk;
+  ta.delay = h->d_delay;
+  ta.coef = h->d_coef;
+  ta.max_delay = h->d_ints + 5;
+  ta.near_count = h->d_u64;
+  ta.cp.c0 = p->c0;
+  ta.cp.dt = p->dt;
+  ta.cp.mu0 = p->mu0;
+  ta.cp.hbar = p->hbar;
+  ta.cp.omega = p->laser_frequency;
+  ta.cp.q = h->q;
+  ta.cp.frame = p->frame;
+  cudaEvent_t e0, e1;
+  QG_CUDA(cudaEventCreate(&e0));
+  QG_CUDA(cudaEventCreate(&e1));
+  QG_CUDA(cudaEventRecord(e0, h->stream));
+  launch_table_build(ta, h->q, h->stream);
+  QG_CUDA(cudaGetLastError());
+  QG_CUDA(cudaEventRecord(e1, h->stream));
+  int md = 0;
+  unsigned long long nn = 0;
+  QG_CUDA(cudaMemcpyAsync(&md, h->d_ints + 5, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaMemcpyAsync(&nn, h->d_u64, sizeof nn, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  float tms = 0;
+  cudaEventElapsedTime(&tms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->table_ms = tms;
+  if(md < 0 || md > (1 << 26))
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_create: floor delay %d out of range (non-finite positions?)",
+                   md);
+  h->max_delay = md;
+  h->near_pairs = (long long)nn;
+
+  // rings and scratch
+  h->W = std::max(md + h->q + 2, 8);
+  h->stride = h->W + kRingMirror;
+  QG_TRY(dalloc(h, &h->d_ring, (size_t)h->n_pad * h->stride));
+  QG_TRY(dalloc(h, &h->d_pcr, (size_t)kPcDepth * 4 * h->n_pad));
+  QG_TRY(dalloc(h, &h->d_partial, (size_t)h->nT * h->n_pad));
+  QG_TRY(dalloc(h, &h->d_scratch, (size_t)h->n_pad * 8));
+  h->traj_k = (int)std::max<long long>(1, std::min<long long>(256, (32ll << 20) / (32ll * n)));
+  QG_TRY(dalloc(h, &h->d_traj, (size_t)2 * h->traj_k * n * 2));
+  QG_CUDA(cudaMallocHost((void **)&h->h_traj, sizeof(double2) * (size_t)2 * h->traj_k * n * 2));
+  QG_TRY(dalloc(h, &h->d_io, (size_t)n));
+  QG_CUDA(cudaMallocHost((void **)&h->h_io, sizeof(double2) * (size_t)n));
+  for(int i = 0; i < 256; ++i) {
+    QG_CUDA(cudaEventCreate(&h->ev_a[i]));
+    QG_CUDA(cudaEventCreate(&h->ev_b[i]));
+  }
+  for(int i = 0; i < 2; ++i) {
+    QG_CUDA(cudaEventCreateWithFlags(&h->ev_chunk[i], cudaEventDisableTiming));
+    QG_CUDA(cudaEventCreateWithFlags(&h->ev_copy[i], cudaEventDisableTiming));
+  }
+  h->events_ready = true;
+
+  QG_TRY(build_near(h));
+  QG_TRY(reset_state(h));
+  return QG_OK;
+}
+
+extern "C" qg_status qg_create(const qg_dot *dots, int n, const qg_pulse *pulse,
+                               const qg_params *params, const qg_weights *weights, qg_handle **out)
+{
+  if(!out) return qg_fail(QG_ERR_INVALID_ARG, "qg_create: out is NULL");
+  *out = nullptr;
+  QG_TRY(validate(dots, n, pulse, params));
+  qg_handle *h = new qg_handle();
+  const qg_status st = create_impl(dots, n, pulse, params, weights, h);
+  if(st != QG_OK) {
+    destroy_handle(h);
+    return st;
+  }
+  *out = h;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_destroy(qg_handle *h)
+{
+  destroy_handle(h);
+  return QG_OK;
+}
+
+// One step's launches: the past pair sum, then the per-dot integrator.
+static void enqueue_step(qg_handle *h, bool traj, bool timed, int ev)
+{
+  SweepArgs sa = h->sweep_args();
+  if(timed) cudaEventRecord(h->ev_a[ev], h->stream);
+  if(h->nblk > 0) launch_sweep_table(sa, h->stream);
+  if(timed) cudaEventRecord(h->ev_b[ev], h->stream);
+  StepArgs a = h->step_args(!h->fused);
+  if(traj) a.traj = h->d_traj;
+  if(h->fused) {
+    launch_step_fused(a, h->step_blocks, h->stream);
+  } else {
+    for(int ph = 0; ph <= kCorrectorSteps + 1; ++ph) launch_step_general(a, ph, h->stream);
+  }
+}
+
+static qg_status ensure_graph(qg_handle *h, int traj)
+{
+  if(h->graph[traj]) return QG_OK;
+  cudaGraph_t g;
+  QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(h, traj != 0, false, 0);
+  QG_CUDA(cudaStreamEndCapture(h->stream, &g));
+  QG_CUDA(cudaGraphInstantiate(&h->graph[traj], g, 0));
+  cudaGraphDestroy(g);
+  return QG_OK;
+}
+
+static qg_status launch_steps(qg_handle *h, int count, bool traj)
+{
+  if(h->profile) {
+    for(int done = 0; done < count;) {
+      const int k = std::min(count - done, 256);
+      for(int j = 0; j < k; ++j) enqueue_step(h, traj, true, j);
+      QG_CUDA(cudaGetLastError());
+      QG_CUDA(cudaEventSynchronize(h->ev_b[k - 1]));
+      for(int j = 0; j < k; ++j) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev_a[j], h->ev_b[j]);
+        h->pair_ms += ms;
+      }
+      h->pair_launches += (h->nblk > 0) ? k : 0;
+      done += k;
+    }
+    return QG_OK;
+  }
+  if(h->use_graph) {
+    QG_TRY(ensure_graph(h, traj ? 1 : 0));
+    for(int j = 0; j < count; ++j) QG_CUDA(cudaGraphLaunch(h->graph[traj ? 1 : 0], h->stream));
+  } else {
+    for(int j = 0; j < count; ++j) enqueue_step(h, traj, false, 0);
+    QG_CUDA(cudaGetLastError());
+  }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad_step)
+{
+  if(!h) return qg_fail(QG_ERR_INVALID_ARG, "qg_run: NULL handle");
+  if(n_steps < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_run: n_steps < 0");
+  if(h->next_step + (long long)n_steps > h->T)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_run: steps [%d, %d) exceed num_timesteps %d", h->next_step,
+                   h->next_step + n_steps, h->T);
+  if(bad_step) *bad_step = -1;
+  QG_CUDA(cudaSetDevice(h->device));
+  const int t_start = h->next_step;
+  h->eval_cached = -0x7fffffff;
+  const size_t row = (size_t)h->n * 2;  // double2 per step
+  if(!rho_out) {
+    QG_TRY(launch_steps(h, n_steps, false));
+  } else {
+    const int K = h->traj_k;
+    const int nchunks = (n_steps + K - 1) / K;
+    auto drain = [&](int c) -> qg_status {
+      const int b = c & 1;
+      const int k = std::min(K, n_steps - c * K);
+      QG_CUDA(cudaEventSynchronize(h->ev_copy[b]));
+      std::memcpy(rho_out + (size_t)c * K * row * 2, h->h_traj + (size_t)b * K * row,
+                  sizeof(double2) * row * k);
+      return QG_OK;
+    };
+    for(int c = 0; c < nchunks; ++c) {
+      const int b = c & 1;
+      const int k = std::min(K, n_steps - c * K);
+      if(c >= 2) {
+        QG_TRY(drain(c - 2));
+        QG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_copy[b], 0));
+      }
+      launch_set_int(h->d_ints + 3, t_start + c * K - b * K, h->stream);
+      QG_TRY(launch_steps(h, k, true));
+      QG_CUDA(cudaEventRecord(h->ev_chunk[b], h->stream));
+      QG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ev_chunk[b], 0));
+      QG_CUDA(cudaMemcpyAsync(h->h_traj + (size_t)b * K * row, h->d_traj + (size_t)b * K * row,
+                              sizeof(double2) * row * k, cudaMemcpyDeviceToHost, h->copy_stream));
+      QG_CUDA(cudaEventRecord(h->ev_copy[b], h->copy_stream));
+    }
+    for(int c = std::max(0, nchunks - 2); c < nchunks; ++c) QG_TRY(drain(c));
+  }
+  int bad = kBadNone;
+  QG_CUDA(cudaMemcpyAsync(&bad, h->d_ints + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  QG_CUDA(cudaGetLastError());
+  h->next_step = t_start + n_steps;
+  if(bad != kBadNone) {
+    if(bad_step) *bad_step = bad;
+    return qg_fail(QG_ERR_NONFINITE, "unbounded history values at or before step %d", bad);
+  }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_next_step(const qg_handle *h, int *step)
+{
+  if(!h || !step) return qg_fail(QG_ERR_INVALID_ARG, "qg_next_step: NULL argument");
+  *step = h->next_step;
+  return QG_OK;
+}
+
+static qg_status upload_io(qg_handle *h, const double *src)
+{
+  std::memcpy(h->h_io, src, sizeof(double2) * h->n);
+  QG_CUDA(cudaMemcpyAsync(h->d_io, h->h_io, sizeof(double2) * h->n, cudaMemcpyHostToDevice, h->stream));
+  return QG_OK;
+}
+
+static qg_status download_io(qg_handle *h, double *dst)
+{
+  QG_CUDA(cudaMemcpyAsync(h->h_io, h->d_io, sizeof(double2) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  std::memcpy(dst, h->h_io, sizeof(double2) * h->n);
+  return QG_OK;
+}
+
+extern "C" qg_status qg_history_evaluate(qg_handle *h, int step, const double *rho01_step,
+                                         double *field_out)
+{
+  if(!h || !field_out) return qg_fail(QG_ERR_INVALID_ARG, "qg_history_evaluate: NULL argument");
+  if(step < 0 || step >= std::max(h->T, 1))
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_history_evaluate: step %d outside [0, %d)", step, h->T);
+  QG_CUDA(cudaSetDevice(h->device));
+  StepArgs a = h->step_args(true);
+  if(rho01_step) {
+    QG_TRY(upload_io(h, rho01_step));
+    launch_ring_write(a, step, h->d_io, h->stream);
+  }
+  if(h->eval_cached != step) {
+    launch_set_int(h->d_ints + 4, step, h->stream);
+    SweepArgs sa = h->sweep_args();
+    sa.d_step = h->d_ints + 4;
+    if(h->nblk > 0) launch_sweep_table(sa, h->stream);
+    h->eval_cached = step;
+  }
+  launch_eval_field(a, h->d_ints + 4, h->d_io, h->stream);
+  QG_CUDA(cudaGetLastError());
+  return download_io(h, field_out);
+}
+
+extern "C" qg_status qg_pulse_evaluate(qg_handle *h, int step, double *field_out)
+{
+  if(!h || !field_out) return qg_fail(QG_ERR_INVALID_ARG, "qg_pulse_evaluate: NULL argument");
+  QG_CUDA(cudaSetDevice(h->device));
+  launch_pulse_field(h->step_args(true), step, h->d_io, h->stream);
+  QG_CUDA(cudaGetLastError());
+  return download_io(h, field_out);
+}
+
+extern "C" qg_status qg_set_history(qg_handle *h, int t0, int n, const double *rho01)
+{
+  if(!h || (n > 0 && !rho01)) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_history: NULL argument");
+  if(t0 < -kWindow || n < 0)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_set_history: t0 = %d < -%d or n < 0", t0, kWindow);
+  QG_CUDA(cudaSetDevice(h->device));
+  StepArgs a = h->step_args(true);
+  for(int k = 0; k < n; ++k) {
+    QG_TRY(upload_io(h, rho01 + (size_t)k * h->n * 2));
+    launch_ring_write(a, t0 + k, h->d_io, h->stream);
+    QG_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  QG_CUDA(cudaGetLastError());
+  h->eval_cached = -0x7fffffff;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_get_history(qg_handle *h, int t0, int n, double *rho01_out)
+{
+  if(!h || (n > 0 && !rho01_out)) return qg_fail(QG_ERR_INVALID_ARG, "qg_get_history: NULL argument");
+  if(n < 0 || n > h->W || t0 < -kWindow)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_get_history: need -22 <= t0 and 0 <= n <= %d", h->W);
+  QG_CUDA(cudaSetDevice(h->device));
+  StepArgs a = h->step_args(true);
+  for(int k = 0; k < n; ++k) {
+    launch_ring_read(a, t0 + k, h->d_io, h->stream);
+    QG_TRY(download_io(h, rho01_out + (size_t)k * h->n * 2));
+  }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_get_info(const qg_handle *h, qg_info *info)
+{
+  if(!h || !info) return qg_fail(QG_ERR_INVALID_ARG, "qg_get_info: NULL argument");
+  std::memset(info, 0, sizeof *info);
+  info->n = h->n;
+  info->max_delay = h->max_delay;
+  info->ring_depth = h->W;
+  info->num_pairs = h->P;
+  info->near_pairs = h->near_pairs;
+  info->coef_mode = QG_COEF_TABLE;
+  info->precision = QG_PREC_FP64;
+  info->fused_step = h->fused ? 1 : 0;
+  info->device_bytes = h->bytes;
+  info->table_build_ms = h->table_ms;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t *bytes)
+{
+  if(!p || !bytes || n < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_footprint: bad argument");
+  const int nT = (n + kTile - 1) / kTile, n_pad = nT * kTile;
+  const long long nblk = (long long)nT * (nT + 1) / 2;
+  const int q = p->interpolation_order;
+  const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
+  const int W = std::max(md + q + 2, 8);
+  size_t b = table_bytes(nblk, q);
+  b += sizeof(double2) * (size_t)n_pad * (W + kRingMirror);
+  b += sizeof(double2) * (size_t)kPcDepth * 4 * n_pad;
+  b += sizeof(double2) * (size_t)nT * n_pad;
+  b += sizeof(double2) * (size_t)n_pad * 8;
+  b += sizeof(double) * (size_t)n_pad * 9 + sizeof(int) * (size_t)n_pad * 2;
+  const long long K = std::max<long long>(1, std::min<long long>(256, (32ll << 20) / (32ll * n)));
+  b += sizeof(double2) * (size_t)(2 * K * n * 2) + sizeof(double2) * (size_t)n;  // trajectory + io staging
+  *bytes = b;
+  return QG_OK;
+}
+
+extern "C" void *qg_stream(qg_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+extern "C" qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *launches)
+{
+  if(!h) return qg_fail(QG_ERR_INVALID_ARG, "qg_kernel_time: NULL handle");
+  if(pair_ms) *pair_ms = h->pair_ms;
+  if(launches) *launches = h->pair_launches;
+  if(reset) {
+    h->pair_ms = 0;
+    h->pair_launches = 0;
+  }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
+{
+  if(!h || !key) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: NULL argument");
+  if(!std::strcmp(key, "graph")) {
+    h->use_graph = value != 0;
+  } else if(!std::strcmp(key, "profile")) {
+    h->profile = value != 0;
+  } else if(!std::strcmp(key, "reset")) {
+    return reset_state(h);
+  } else {
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: unknown key '%s'", key);
+  }
+  return QG_OK;
+}

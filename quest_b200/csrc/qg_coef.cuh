@@ -1,0 +1,155 @@
+// Per-pair retarded-interaction coefficients on the device, following the
+// reference's table build operation by operation:
+//   separation / norm / split_double   history_interaction.cpp:29-35, 88-97
+//   UniformLagrangeSet::calculate_weights   lagrange_set.cpp:17-41
+//   spatial dyads                      green_function.h:32-55
+//   RotatingDyadic::coefficients       rotating_green_function.cpp:3-24
+//   Dyadic::coefficients (lab frame)   green_function.cpp:3-20
+//   d_obs . (M d_src)                  history_interaction.cpp:40-43
+// Included by translation units compiled with -fmad=false, so each multiply
+// and add rounds separately as in the reference's x86-64 build.
+#pragma once
+
+#include "qg_internal.h"
+
+namespace qg {
+
+// lagrange_set.cpp:17-41; w[k][i] for derivative k = 0..2, node i = 0..q.
+template <int Q>
+__device__ __forceinline__ void lagrange_weights_ref(double x, double dt, double (&w)[3][Q + 1])
+{
+#pragma unroll
+  for(int b = 0; b <= Q; ++b) {
+    double d0 = 1, d1 = 0, d2 = 0;
+#pragma unroll
+    for(int m = 0; m <= Q; ++m) {
+      if(m == b) continue;
+      d0 *= (x - m) / (double)(b - m);
+      d1 -= 1 / (x - m);
+      d2 -= pow(x - m, -2.0);
+    }
+    w[0][b] = d0;
+    w[1][b] = w[0][b] * d1;
+    w[2][b] = w[0][b] * d2 + (w[1][b] * w[1][b]) / w[0][b];
+  }
+  const double inv_dt = 1.0 / dt;  // gcc folds pow(dt, -1) to 1/dt
+  const double inv_dt2 = pow(dt, -2.0);
+#pragma unroll
+  for(int i = 0; i <= Q; ++i) {
+    w[1][i] *= inv_dt;
+    w[2][i] *= inv_dt2;
+  }
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b)
+{
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s)
+{
+  return make_double2(a.x * s, a.y * s);
+}
+
+// d_obs . (M d_src) with Eigen's left-to-right sums over 3-vectors.
+__device__ __forceinline__ double2 contract3(const double (&dobs)[3], const double2 (&M)[9],
+                                             const double (&dsrc)[3])
+{
+  double2 v[3];
+#pragma unroll
+  for(int r = 0; r < 3; ++r) {
+    double2 acc = cscale(M[3 * r + 0], dsrc[0]);
+    acc = cadd(acc, cscale(M[3 * r + 1], dsrc[1]));
+    acc = cadd(acc, cscale(M[3 * r + 2], dsrc[2]));
+    v[r] = acc;
+  }
+  double2 out = cscale(v[0], dobs[0]);
+  out = cadd(out, cscale(v[1], dobs[1]));
+  out = cadd(out, cscale(v[2], dobs[2]));
+  return out;
+}
+
+// Floor delay and q+1 coefficients of the pair (src = larger user index,
+// obs = smaller), exactly the quantities build_coefficient_table stores.
+template <int Q>
+__device__ __forceinline__ int pair_coef_ref(const double (&psrc)[3], const double (&pobs)[3],
+                                             const double (&dsrc)[3], const double (&dobs)[3],
+                                             const CoefParams &p, double2 (&coef)[Q + 1])
+{
+  double dr[3];
+#pragma unroll
+  for(int k = 0; k < 3; ++k) dr[k] = pobs[k] - psrc[k];
+  const double sq = (dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2];
+  const double nrm = sqrt(sq);
+  double idelay;
+  const double frac = modf(nrm / (p.c0 * p.dt), &idelay);
+  const int fd = (int)idelay;
+
+  double w[3][Q + 1];
+  lagrange_weights_ref<Q>(frac, p.dt, w);
+
+  // spatial dyads (green_function.h:32-40)
+  double dy[3][9];
+  const double c2 = p.c0 * p.c0;       // pow(c, 2)
+  const double n3 = pow(nrm, 3.0);     // pow(|r|, 3)
+#pragma unroll
+  for(int r = 0; r < 3; ++r) {
+#pragma unroll
+    for(int k = 0; k < 3; ++k) {
+      const double rhat = (dr[r] * dr[k]) / sq;
+      const double id = (r == k) ? 1.0 : 0.0;
+      const double i3 = id - 3 * rhat;
+      const double i1 = id - rhat;
+      dy[0][3 * r + k] = (i3 * c2) / n3;
+      dy[1][3 * r + k] = (i3 * p.c0) / sq;
+      dy[2][3 * r + k] = i1 / nrm;
+    }
+  }
+  const double A = p.mu0 / (4 * M_PI * p.hbar);
+
+  if(p.frame == 0) {
+    const double om = p.omega;
+    const double y = (-om * nrm) / p.c0;
+    double sn, cs;
+    sincos(y, &sn, &cs);
+    const double2 s = make_double2(-A * cs, -A * sn);
+    const double om2 = om * om;
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) {
+      const double w0 = w[0][i], w1 = w[1][i], w2 = w[2][i];
+      const double2 t1 = make_double2(w1, om * w0);
+      const double2 t2 = make_double2(w2 - om2 * w0, (2.0 * om) * w1);
+      double2 M[9];
+#pragma unroll
+      for(int e = 0; e < 9; ++e) {
+        const double2 a = make_double2(dy[0][e] * w0, 0.0);
+        const double2 b = cmul(make_double2(dy[1][e], 0.0), t1);
+        const double2 c = cmul(make_double2(dy[2][e], 0.0), t2);
+        M[e] = cmul(s, cadd(cadd(a, b), c));
+      }
+      coef[i] = contract3(dobs, M, dsrc);
+    }
+  } else {
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) {
+      double2 M[9];
+#pragma unroll
+      for(int e = 0; e < 9; ++e) {
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for(int term = 0; term < 3; ++term) {
+          const double2 t = make_double2((A * dy[term][e]) * w[term][i], (A * 0.0) * w[term][i]);
+          acc = cadd(acc, t);
+        }
+        M[e] = acc;
+      }
+      coef[i] = contract3(dobs, M, dsrc);
+    }
+  }
+  return fd;
+}
+
+}  // namespace qg

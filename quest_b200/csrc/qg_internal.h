@@ -1,0 +1,114 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <vector_types.h>  // double2
+
+#include "../../include/quest_gpu.h"
+
+// Records the message for qg_last_error() on this thread and returns code.
+qg_status qg_fail(qg_status code, const char *fmt, ...);
+
+namespace qg {
+
+constexpr int kWindow = 22;      // History's negative-time extent (main.cpp:30)
+constexpr int kCorrectorSteps = 10;  // NUM_CORRECTOR_STEPS (integrator.cpp:3)
+constexpr int kMaxOrder = 7;     // largest interpolation order built
+constexpr int kRingMirror = 8;   // slots mirrored past the ring end (>= q+1)
+constexpr int kTile = 64;        // dots per table tile
+constexpr int kTilePairs = kTile * kTile;
+constexpr int kPcDepth = 23;     // PC ring: 22 past steps + the current one
+constexpr int kStepBlock = 128;  // threads per block of the dot-step kernel
+constexpr int kBadNone = 0x7fffffff;
+
+// Weights as passed to kernels (copy of qg_weights).
+struct PCW {
+  int n_time;
+  double ps[64];
+  double cs[64];
+  double fc;
+};
+
+// Per-pair physics constants for coefficient kernels.
+struct CoefParams {
+  double c0, dt, mu0, hbar, omega;
+  int q;
+  int frame;
+};
+
+struct PulseParams {
+  double amp_pol[3];  // (amplitude / 2) * polarisation_k
+  double k[3];        // wavevector
+  double freq, delay, width;
+};
+
+// Arguments of the table-build kernel.
+struct TableArgs {
+  const double *pos;   // [n_pad][3] internal order
+  const double *dip;   // [n_pad][3]
+  const int *user;     // internal -> user index, -1 for padding
+  int n, n_pad, nT;
+  long long nblk;
+  int *delay;          // [nblk][kTilePairs]
+  double2 *coef;       // [nblk][q+1][kTilePairs]
+  int *max_delay;      // atomicMax
+  unsigned long long *near_count;
+  CoefParams cp;
+};
+
+// Arguments of the pair-sum (sweep) kernel over the FP64 table.
+struct SweepArgs {
+  const int *delay;
+  const double2 *coef;
+  const double2 *ring;  // [n_pad][stride]: prefactor(rho01) by time slot
+  double2 *partial;     // [nT][n_pad]
+  int n_pad, nT, W, stride, q, frame;
+  long long nblk;
+  const int *d_step;
+  const int *d_bad;
+};
+
+// Arguments of the per-dot step kernels.
+struct StepArgs {
+  int n, n_pad, nT, W, stride, q, frame;
+  double dt, laser_freq, hbar;
+  PulseParams pulse;
+  const double *pos;     // [n_pad][3] internal order
+  const double *dip;     // [n_pad][3]
+  const double *freq, *t1, *t2;
+  const int *slot_dot;   // slot -> internal index (-1 empty)
+  const int *user;       // internal -> user
+  const double2 *partial;
+  double2 *pcr;          // [kPcDepth][4][n_pad]
+  double2 *ring;         // [n_pad][stride] rho01 by step slot
+  // current-step coupling: CSR by slot (fused: partner = local slot in the
+  // block; general: partner = internal index)
+  const int *near_ptr;
+  const int *near_idx;
+  const double2 *near_coef;
+  // general path scratch
+  double2 *scratch;      // [n_pad][8]: past field, pulse, H (2 complex), cur rho x2
+  double2 *traj;         // [k][n][2] user order or null
+  const int *traj_t0;
+  int *d_step, *d_done, *d_bad;
+  PCW w;
+};
+
+// Launchers (defined in the .cu files).
+void launch_table_build(const TableArgs &a, int q, void *stream);
+void launch_near_extract(const int *delay, const double2 *coef, long long nblk, int nT,
+                         int q, int *out_pairs /*[cap][2] internal a,b*/, double2 *out_coef,
+                         unsigned long long *counter, unsigned long long cap, void *stream);
+void launch_sweep_table(const SweepArgs &a, void *stream);
+void launch_step_fused(const StepArgs &a, int nblocks, void *stream);
+void launch_step_general(const StepArgs &a, int phase, void *stream);
+void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream);
+void launch_pulse_field(const StepArgs &a, int step, double2 *out_user, void *stream);
+void launch_set_int(int *p, int v, void *stream);
+void launch_init_state(const StepArgs &a, void *stream);
+void launch_ring_write(const StepArgs &a, int t, const double2 *rho01_user, void *stream);
+void launch_ring_read(const StepArgs &a, int t, double2 *rho01_user, void *stream);
+
+}  // namespace qg

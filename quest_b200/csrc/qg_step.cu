@@ -1,0 +1,366 @@
+// Per-dot work of one time step: the integrator, the pulse and the Bloch
+// right-hand side.
+//
+//   predictor            reference src/integrator.cpp:142-154
+//   corrector            integrator.cpp:156-169
+//   evaluator            integrator.cpp:171-185 (field = (0 + pulse) + history)
+//   PulseInteraction     src/interactions/pulse_interaction.cpp:9-20,
+//                        src/pulse.cpp:15-20, src/math_utils.cpp:27-30
+//   liouville_rhs        src/quantum_dot.cpp:10-19
+//   all_finite           integrator.cpp:187-198
+//
+// The strictly-past part of the history field comes from the sweep kernel's
+// partial sums.  The (delay 0, tap 0) terms, which read the current step's
+// iterate, are re-evaluated in each of the 11 evaluations from a near list.
+//
+// Two forms.  The fused kernel runs predictor, 11 evaluations and 10
+// corrections in one launch: every connected group of dots coupled at delay
+// 0 is placed inside one thread block, so a __syncthreads between
+// iterations is the only synchronisation needed.  The general form (used when
+// such a group is larger than a block, e.g. when c0*dt exceeds the dot
+// spacing and every pair has delay 0) runs one launch per evaluation.
+//
+// Per-dot state in HBM:
+//   pcr[slot][k][dot]   k = rho00, rho01, drho00, drho01 for the last 23
+//                       steps (slot = t mod 23): the integrator's window
+//   ring[dot][slot]     rho01 by step (slot = t mod W, first kRingMirror
+//                       slots mirrored after W-1), read by the sweep
+//
+// Compiled with -fmad=false: the predictor, corrector and right-hand side
+// round each operation as the reference does.
+#include <cuda_runtime.h>
+
+#include "qg_coef.cuh"
+
+namespace qg {
+
+__device__ __forceinline__ int pc_slot(int t) { return ((t % kPcDepth) + kPcDepth) % kPcDepth; }
+
+__device__ __forceinline__ double2 prefactor(double2 r, int frame)
+{
+  // rotating frame: rho01 (rotating_green_function.h:17-21);
+  // lab frame: 2 Re rho01 (green_function.h:23-27)
+  return frame == 0 ? r : make_double2(2 * r.x, 0.0);
+}
+
+__device__ __forceinline__ void liouville(double2 r0, double2 r1, double2 om, double t1, double t2,
+                                          double det, double2 &m0, double2 &m1)
+{
+  const double2 r1c = make_double2(r1.x, -r1.y), omc = make_double2(om.x, -om.y);
+  const double2 mi = make_double2(-0.0, -1.0);  // -iu
+  const double2 u = cmul(om, r1c), v = cmul(omc, r1);
+  m0 = cmul(mi, make_double2(u.x - v.x, u.y - v.y));
+  m0.x = m0.x - (r0.x - 1.0) / t1;
+  m0.y = m0.y - r0.y / t1;
+  const double2 one_m = make_double2(1.0 - 2.0 * r0.x, -(2.0 * r0.y));
+  const double2 aa = cmul(om, one_m);
+  const double2 ab = make_double2(aa.x + r1.x * det, aa.y + r1.y * det);
+  m1 = cmul(mi, ab);
+  m1.x = m1.x - r1.x / t2;
+  m1.y = m1.y - r1.y / t2;
+}
+
+__device__ __forceinline__ double pulse_rabi(const StepArgs &a, int idx, int t)
+{
+  const double *p = a.pos + 3 * idx;
+  const PulseParams &P = a.pulse;
+  const double kr = (P.k[0] * p[0] + P.k[1] * p[1]) + P.k[2] * p[2];
+  const double time = t * a.dt;
+  const double arg = kr - P.freq * (time - P.delay);
+  const double x = arg / P.width;
+  const double g = exp(-(x * x) / 2);
+  const double *d = a.dip + 3 * idx;
+  const double e0 = P.amp_pol[0] * g, e1 = P.amp_pol[1] * g, e2 = P.amp_pol[2] * g;
+  return ((e0 * d[0] + e1 * d[1]) + e2 * d[2]) / a.hbar;
+}
+
+// Predictor value P and corrector base H (the history part of the
+// corrector sum) from the 22-step window.
+__device__ __forceinline__ void pc_window(const StepArgs &a, int idx, int t, double2 (&P)[2],
+                                          double2 (&H)[2])
+{
+  P[0] = P[1] = H[0] = H[1] = make_double2(0.0, 0.0);
+  const int nt = a.w.n_time;
+  const double dt = a.dt;
+  for(int h = 0; h < nt; ++h) {
+    const int s = pc_slot(t - nt + h);
+    const double2 *base = a.pcr + (long long)s * 4 * a.n_pad + idx;
+    const double2 x0 = base[0], x1 = base[a.n_pad], y0 = base[2 * a.n_pad], y1 = base[3 * a.n_pad];
+    const double p0 = a.w.ps[h], p1 = a.w.ps[nt + h];
+    const double c0 = a.w.cs[h], c1 = a.w.cs[nt + h];
+    P[0].x += x0.x * p0 + (y0.x * p1) * dt;
+    P[0].y += x0.y * p0 + (y0.y * p1) * dt;
+    P[1].x += x1.x * p0 + (y1.x * p1) * dt;
+    P[1].y += x1.y * p0 + (y1.y * p1) * dt;
+    H[0].x += x0.x * c0 + (y0.x * c1) * dt;
+    H[0].y += x0.y * c0 + (y0.y * c1) * dt;
+    H[1].x += x1.x * c0 + (y1.x * c1) * dt;
+    H[1].y += x1.y * c0 + (y1.y * c1) * dt;
+  }
+}
+
+__device__ __forceinline__ double2 past_field(const StepArgs &a, int idx)
+{
+  double2 f = make_double2(0.0, 0.0);
+  for(int k = 0; k < a.nT; ++k) {
+    const double2 v = a.partial[(long long)k * a.n_pad + idx];
+    f.x += v.x;
+    f.y += v.y;
+  }
+  return f;
+}
+
+__device__ __forceinline__ void corrector(const StepArgs &a, const double2 (&dr)[2],
+                                          const double2 (&H)[2], double2 (&r)[2])
+{
+  const double fc = a.w.fc, dt = a.dt;
+#pragma unroll
+  for(int c = 0; c < 2; ++c) {
+    r[c].x = (fc * dr[c].x) * dt + H[c].x;
+    r[c].y = (fc * dr[c].y) * dt + H[c].y;
+  }
+}
+
+__device__ __forceinline__ bool finite4(double2 a, double2 b)
+{
+  return isfinite(a.x) && isfinite(a.y) && isfinite(b.x) && isfinite(b.y);
+}
+
+// Stores the step's final state: PC window, rho01 ring, trajectory row,
+// and the non-finite flag.
+__device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, const double2 (&r)[2],
+                                           const double2 (&dr)[2])
+{
+  double2 *base = a.pcr + (long long)pc_slot(t) * 4 * a.n_pad + idx;
+  base[0] = r[0];
+  base[a.n_pad] = r[1];
+  base[2 * a.n_pad] = dr[0];
+  base[3 * a.n_pad] = dr[1];
+  const int slot = t % a.W;
+  double2 *ring = a.ring + (long long)idx * a.stride;
+  ring[slot] = r[1];
+  if(slot < kRingMirror) ring[a.W + slot] = r[1];
+  if(a.traj) {
+    const int row = t - *a.traj_t0;
+    double2 *tr = a.traj + ((long long)row * a.n + a.user[idx]) * 2;
+    tr[0] = r[0];
+    tr[1] = r[1];
+  }
+  if(!finite4(r[0], r[1]) || !finite4(dr[0], dr[1])) atomicMin(a.d_bad, t);
+}
+
+__device__ __forceinline__ void advance_step(const StepArgs &a, int t)
+{
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd((unsigned *)a.d_done, 1u);
+    if(prev == gridDim.x - 1) {
+      *a.d_done = 0;
+      __threadfence();
+      atomicExch(a.d_step, t + 1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kStepBlock) step_fused_kernel(StepArgs a)
+{
+  __shared__ double2 cur[kStepBlock];
+  const int slot = blockIdx.x * kStepBlock + threadIdx.x;
+  const int idx = a.slot_dot[slot];
+  const int t = *a.d_step;
+  const bool live = idx >= 0 && *a.d_bad >= t;
+  const int nb0 = a.near_ptr[blockIdx.x * kStepBlock];
+  const bool block_near = a.near_ptr[(blockIdx.x + 1) * kStepBlock] > nb0;
+
+  double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
+  double det = 0, t1 = 1, t2 = 1, pul = 0;
+  if(live) {
+    pc_window(a, idx, t, P, H);
+    past = past_field(a, idx);
+    pul = pulse_rabi(a, idx, t);
+    det = a.laser_freq - a.freq[idx];
+    t1 = a.t1[idx];
+    t2 = a.t2[idx];
+    r[0] = P[0];
+    r[1] = P[1];
+  }
+  const int e0 = a.near_ptr[slot], e1 = a.near_ptr[slot + 1];
+  for(int it = 0; it <= kCorrectorSteps; ++it) {
+    if(it > 0 && live) corrector(a, dr, H, r);
+    double2 nf = make_double2(0.0, 0.0);
+    if(block_near) {
+      __syncthreads();
+      cur[threadIdx.x] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
+      __syncthreads();
+      for(int e = e0; e < e1; ++e) {
+        const double2 c = a.near_coef[e];
+        const double2 v = cmul(cur[a.near_idx[e]], c);
+        nf.x += v.x;
+        nf.y += v.y;
+      }
+    }
+    if(live) {
+      const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
+      liouville(r[0], r[1], om, t1, t2, det, dr[0], dr[1]);
+    }
+  }
+  if(live) finish_dot(a, idx, t, r, dr);
+  advance_step(a, t);
+}
+
+// General form, one launch per phase: phase 0 predicts, phases 1..11 are the
+// 11 evaluations (each followed by a correction except the last).
+// scratch[idx*8 + k]: 0 past field, 1 pulse, 2-3 H, 4-5 rho (even
+// iterations), 6-7 rho (odd iterations).
+__global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, int phase)
+{
+  const int idx = blockIdx.x * kStepBlock + threadIdx.x;
+  const int t = *a.d_step;
+  const bool live = idx < a.n && *a.d_bad >= t;
+  double2 *sc = a.scratch + (long long)idx * 8;
+  if(phase == 0) {
+    if(live) {
+      double2 P[2], H[2];
+      pc_window(a, idx, t, P, H);
+      sc[0] = past_field(a, idx);
+      sc[1] = make_double2(pulse_rabi(a, idx, t), 0.0);
+      sc[2] = H[0];
+      sc[3] = H[1];
+      sc[4] = P[0];
+      sc[5] = P[1];
+    }
+    return;
+  }
+  const int it = phase - 1;
+  const int rd = (it & 1) ? 6 : 4, wr = (it & 1) ? 4 : 6;
+  if(live) {
+    double2 r[2] = {sc[rd], sc[rd + 1]};
+    double2 nf = make_double2(0.0, 0.0);
+    for(int e = a.near_ptr[idx]; e < a.near_ptr[idx + 1]; ++e) {
+      const int b = a.near_idx[e];
+      const double2 v = cmul(prefactor(a.scratch[(long long)b * 8 + rd + 1], a.frame), a.near_coef[e]);
+      nf.x += v.x;
+      nf.y += v.y;
+    }
+    const double2 past = sc[0];
+    const double pul = sc[1].x;
+    const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
+    double2 dr[2];
+    liouville(r[0], r[1], om, a.t1[idx], a.t2[idx], a.laser_freq - a.freq[idx], dr[0], dr[1]);
+    if(it < kCorrectorSteps) {
+      const double2 H[2] = {sc[2], sc[3]};
+      corrector(a, dr, H, r);
+      sc[wr] = r[0];
+      sc[wr + 1] = r[1];
+    } else {
+      finish_dot(a, idx, t, r, dr);
+    }
+  }
+  if(it == kCorrectorSteps) advance_step(a, t);
+}
+
+void launch_step_fused(const StepArgs &a, int nblocks, void *stream)
+{
+  step_fused_kernel<<<nblocks, kStepBlock, 0, (cudaStream_t)stream>>>(a);
+}
+
+void launch_step_general(const StepArgs &a, int phase, void *stream)
+{
+  const int nblocks = (a.n + kStepBlock - 1) / kStepBlock;
+  step_general_kernel<<<nblocks, kStepBlock, 0, (cudaStream_t)stream>>>(a, phase);
+}
+
+// HistoryInteraction::evaluate at an explicit step: past partial sums plus
+// the delay-0 tap-0 terms read from the ring at `step`, in user order.
+__global__ void eval_field_kernel(StepArgs a, const int *d_eval_step, double2 *out)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= a.n) return;
+  const int step = *d_eval_step;
+  const int slot = ((step % a.W) + a.W) % a.W;
+  double2 f = past_field(a, idx);
+  for(int e = a.near_ptr[idx]; e < a.near_ptr[idx + 1]; ++e) {
+    const int b = a.near_idx[e];
+    const double2 v = cmul(prefactor(a.ring[(long long)b * a.stride + slot], a.frame), a.near_coef[e]);
+    f.x += v.x;
+    f.y += v.y;
+  }
+  out[a.user[idx]] = f;
+}
+
+void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream)
+{
+  eval_field_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, d_eval_step, out_user);
+}
+
+__global__ void pulse_field_kernel(StepArgs a, int step, double2 *out)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= a.n) return;
+  out[a.user[idx]] = make_double2(pulse_rabi(a, idx, step), 0.0);
+}
+
+void launch_pulse_field(const StepArgs &a, int step, double2 *out_user, void *stream)
+{
+  pulse_field_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, step, out_user);
+}
+
+__global__ void set_int_kernel(int *p, int v) { *p = v; }
+
+void launch_set_int(int *p, int v, void *stream)
+{
+  set_int_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(p, v);
+}
+
+// main.cpp:30-36: rho = (1, 0) and rho-dot = 0 in every PC slot (steps
+// -22..0); the ring (rho01 = 0 at t <= 0) is zeroed by the caller.
+__global__ void init_state_kernel(StepArgs a)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)kPcDepth * a.n_pad;
+  if(i >= total) return;
+  const long long s = i / a.n_pad, d = i % a.n_pad;
+  double2 *base = a.pcr + s * 4 * a.n_pad + d;
+  base[0] = make_double2(1.0, 0.0);
+  base[a.n_pad] = make_double2(0.0, 0.0);
+  base[2 * a.n_pad] = make_double2(0.0, 0.0);
+  base[3 * a.n_pad] = make_double2(0.0, 0.0);
+}
+
+void launch_init_state(const StepArgs &a, void *stream)
+{
+  const long long total = (long long)kPcDepth * a.n_pad;
+  init_state_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
+}
+
+__global__ void ring_write_kernel(StepArgs a, int t, const double2 *rho01_user)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= a.n) return;
+  const int slot = ((t % a.W) + a.W) % a.W;
+  const double2 v = rho01_user[a.user[idx]];
+  double2 *ring = a.ring + (long long)idx * a.stride;
+  ring[slot] = v;
+  if(slot < kRingMirror) ring[a.W + slot] = v;
+}
+
+void launch_ring_write(const StepArgs &a, int t, const double2 *rho01_user, void *stream)
+{
+  ring_write_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
+}
+
+__global__ void ring_read_kernel(StepArgs a, int t, double2 *rho01_user)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= a.n) return;
+  const int slot = ((t % a.W) + a.W) % a.W;
+  rho01_user[a.user[idx]] = a.ring[(long long)idx * a.stride + slot];
+}
+
+void launch_ring_read(const StepArgs &a, int t, double2 *rho01_user, void *stream)
+{
+  ring_read_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
+}
+
+}  // namespace qg

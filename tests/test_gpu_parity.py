@@ -1,0 +1,253 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Tolerance: max |rho_gpu - rho_oracle| / max |rho_oracle|, per component
+(rho00 and rho01 separately), must be <= 1e-10 for the FP64 path.  The GPU
+sums the pair terms in a different order than the reference (once per step,
+tile by tile), so bitwise equality is not expected; the per-pair terms
+cancel strongly (individual taps are ~1e3 times the field), which is what
+sets the size of the difference.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from quest_b200 import capi, inputs as I
+from tests.conftest import GOLDEN, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def gpu_run(dots, pulse, c, weights, steps=None, **kw):
+    steps = c.num_timesteps if steps is None else steps
+    with capi.Simulation(dots, pulse, c, weights=weights, **kw) as sim:
+        rho = sim.run(steps)
+        info = sim.info()
+    return rho, info
+
+
+def assert_parity(ref_hist, rho, tol=TOL):
+    ref = O.rho_trajectory(ref_hist)[: rho.shape[0]]
+    e00 = rel_err(ref[..., 0], rho[..., 0])
+    e01 = rel_err(ref[..., 1], rho[..., 1])
+    assert e00 <= tol and e01 <= tol, (e00, e01)
+    return e00, e01
+
+
+def load_example(n=None, steps=None):
+    c, n_cfg, _, _ = I.read_input_cfg(os.path.join(GOLDEN, "example_input.cfg"))
+    n = n_cfg if n is None else n
+    dots = I.read_dots_cfg(os.path.join(GOLDEN, "example_dots.cfg"), n)
+    pulse = I.read_pulse_cfg(os.path.join(GOLDEN, "example_pulse.cfg"))
+    if steps is not None:
+        c.num_timesteps = steps
+    return dots, pulse, c
+
+
+def test_small_against_faithful_oracle(golden_weights, oracle_weights):
+    wl = I.plain_small(n=60, steps=400, pulse_delay=0.2)
+    hist, bad = O.run_faithful(wl.dots, wl.pulse, wl.constants, oracle_weights, 400)
+    assert bad is None
+    rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    assert info["fused_step"] == 1
+    assert_parity(hist, rho)
+    assert np.abs(rho[..., 1]).max() > 1e-6
+
+
+def test_plain_small_delay_half(golden_weights, oracle_weights):
+    """N=200, 0.2 cube, 2000 steps, order 5, pulse delay 0.5 (the stated delay
+    5 never reaches the dots before t = 2)."""
+    wl = I.plain_small(n=200, steps=2000, pulse_delay=0.5)
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 2000)
+    assert bad is None
+    rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    assert_parity(hist, rho)
+
+
+def test_plain_small_as_stated_stays_in_ground_state(golden_weights, oracle_weights):
+    wl = I.plain_small(n=200, steps=2000, pulse_delay=5.0)
+    rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    hist, _ = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 2000)
+    ref = O.rho_trajectory(hist)
+    np.testing.assert_allclose(rho[..., 0], ref[..., 0], rtol=0, atol=1e-13)
+    assert np.abs(rho[..., 1]).max() < 1e-13
+    assert np.abs(rho[..., 0] - 1).max() < 1e-12
+
+
+def test_reference_example_two_dots(golden_weights, oracle_weights):
+    """examples/ verbatim: N=2, order 3, 4000 steps, the pair at delay 0."""
+    dots, pulse, c = load_example()
+    hist, bad = O.run_faithful(dots, pulse, c, oracle_weights, c.num_timesteps)
+    assert bad is None
+    rho, info = gpu_run(dots, pulse, c, golden_weights)
+    assert info["near_pairs"] == 1 and info["fused_step"] == 1
+    assert_parity(hist, rho)
+
+
+def test_reference_example_all_pairs_near(golden_weights, oracle_weights):
+    """examples/ with 256 dots: every pair at delay 0, coupled in every
+    corrector iteration; the group exceeds one block, so the general
+    (one launch per evaluation) form runs."""
+    dots, pulse, c = load_example(n=256, steps=1150)
+    hist, bad = O.run_fast(dots, pulse, c, oracle_weights, 1150)
+    assert bad is None
+    rho, info = gpu_run(dots, pulse, c, golden_weights)
+    assert info["fused_step"] == 0 and info["near_pairs"] == 256 * 255 // 2
+    assert_parity(hist, rho)
+
+
+def test_small_near_groups_fused(golden_weights, oracle_weights):
+    """A few delay-0 pairs in an otherwise retarded system: the fused kernel
+    with groups packed into blocks."""
+    wl = I.plain_small(n=300, steps=500, pulse_delay=0.15)
+    wl.constants.dt = 2e-3  # c dt = 2e-3: a handful of pairs closer than that
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 500)
+    assert bad is None
+    rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    assert info["near_pairs"] > 0 and info["fused_step"] == 1
+    assert_parity(hist, rho)
+
+
+@pytest.mark.parametrize("q", [1, 3, 7])
+def test_interpolation_orders(golden_weights, oracle_weights, q):
+    wl = I.plain_small(n=90, steps=300, pulse_delay=0.15)
+    wl.constants.interpolation_order = q
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 300)
+    assert bad is None
+    rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    assert_parity(hist, rho)
+
+
+def test_lab_frame(golden_weights, oracle_weights):
+    """GreenFunction::Dyadic (green_function.cpp:3-20) with prefactor 2 Re rho01."""
+    wl = I.plain_small(n=64, steps=300, pulse_delay=0.15)
+    wl.constants.frame = 1
+    hist, bad = O.run_faithful(wl.dots, wl.pulse, wl.constants, oracle_weights, 300)
+    assert bad is None
+    rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    assert_parity(hist, rho)
+
+
+def test_default_weights_are_the_golden_ones(oracle_weights):
+    wl = I.plain_small(n=40, steps=200, pulse_delay=0.1)
+    hist, _ = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 200)
+    rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, None)
+    assert_parity(hist, rho)
+
+
+def test_history_evaluate_matches_reference_sum(golden_weights):
+    """HistoryInteraction::evaluate on an arbitrary history, all steps."""
+    wl = I.plain_small(n=150, steps=400)
+    c = wl.constants
+    n = wl.n
+    rng = np.random.default_rng(5)
+    T = 400
+    hist = np.zeros((n, T + O.WINDOW, 2, 2), dtype=np.complex128)
+    hist[:, :, 0, 1] = rng.normal(size=(n, T + O.WINDOW)) + 1j * rng.normal(size=(n, T + O.WINDOW))
+    delays, coefs = O.build_table(wl.dots, c)
+    with capi.Simulation(wl.dots, wl.pulse, c, weights=golden_weights) as sim:
+        W = sim.info()["ring_depth"]
+        for step in [0, 5, 60, 250, 399]:
+            lo = max(-O.WINDOW, step - W + 1)
+            sim.set_history(lo, hist[:, lo + O.WINDOW: step + O.WINDOW, 0, 1].T)
+            got = sim.history_evaluate(step, hist[:, step + O.WINDOW, 0, 1])
+            ref = O.history_evaluate(wl.dots, c, delays, coefs, hist, step)
+            assert rel_err(ref, got) < 1e-12, step
+            # a second call at the same step re-uses the past sum
+            got2 = sim.history_evaluate(step, hist[:, step + O.WINDOW, 0, 1] * 0.5)
+            hist2 = hist.copy()
+            hist2[:, step + O.WINDOW, 0, 1] *= 0.5
+            ref2 = O.history_evaluate(wl.dots, c, delays, coefs, hist2, step)
+            assert rel_err(ref2, got2) < 1e-12, step
+
+
+def test_pulse_evaluate(golden_weights):
+    wl = I.plain_small(n=50, steps=10, pulse_delay=0.0)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        for step in [0, 3, 9]:
+            np.testing.assert_array_equal(sim.pulse_evaluate(step),
+                                          O.pulse_evaluate(wl.dots, wl.pulse, wl.constants, step))
+
+
+def test_run_in_pieces_equals_one_run(golden_weights):
+    wl = I.plain_small(n=100, steps=600, pulse_delay=0.1)
+    a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        parts = [sim.run(k) for k in (1, 99, 300, 200)]
+        assert sim.next_step == 600
+    np.testing.assert_array_equal(a, np.concatenate(parts))
+
+
+def test_deterministic(golden_weights):
+    wl = I.plain_small(n=333, steps=300, pulse_delay=0.1)
+    a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    b, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_graph_and_direct_launches_agree(golden_weights):
+    wl = I.plain_small(n=100, steps=200, pulse_delay=0.1)
+    a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        sim.set_option("graph", 0)
+        b = sim.run(100)
+        sim.set_option("profile", 1)
+        c = sim.run(100)
+        ms, launches = sim.kernel_time()
+    np.testing.assert_array_equal(a, np.concatenate([b, c]))
+    assert launches == 100 and ms > 0
+
+
+def test_coincident_dots_raise_at_step_zero(golden_weights):
+    dots = I.make_dots(5, 0.1, 3)
+    dots[3, :3] = dots[1, :3]
+    c = I.Constants(num_timesteps=10)
+    with capi.Simulation(dots, I.make_pulse(delay=0.0), c, weights=golden_weights) as sim:
+        with pytest.raises(capi.NonFiniteError) as e:
+            sim.run(10)
+    assert e.value.step == 0
+    assert "unbounded history values at or before step 0" in str(e.value)
+
+
+def test_integer_delay_raises_where_the_reference_does(golden_weights, oracle_weights):
+    c = I.Constants(c0=1.0, dt=0.125, num_timesteps=40)
+    dots = np.array([[0.0, 0, 0, 200, 10, 10, 0, 0, 2e-3],
+                     [5.0, 0, 0, 200, 10, 10, 0, 0, 2e-3]])
+    _, bad = O.run_faithful(dots, I.make_pulse(delay=0.0), c, oracle_weights, 40)
+    with capi.Simulation(dots, I.make_pulse(delay=0.0), c, weights=golden_weights) as sim:
+        with pytest.raises(capi.NonFiniteError) as e:
+            sim.run(40)
+    assert e.value.step == bad == 19
+
+
+def test_steps_past_the_end_are_rejected(golden_weights):
+    wl = I.plain_small(n=10, steps=20)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        sim.run(15, record=False)
+        with pytest.raises(capi.QuestError) as e:
+            sim.run(6)
+        assert e.value.code == capi.QG_ERR_INVALID_ARG
+
+
+def test_single_dot_and_ragged_sizes(golden_weights, oracle_weights):
+    for n in [1, 2, 63, 64, 65, 129]:
+        wl = I.plain_small(n=n, steps=120, pulse_delay=0.06)
+        hist, _ = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 120)
+        rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+        assert_parity(hist, rho)
+
+
+@pytest.mark.slow
+def test_fp64_table_n4096_truncated(golden_weights, oracle_weights):
+    """The N=4096 FP64-table workload over 700 steps (past the largest delay,
+    346), with the pulse moved to t = 0.3 so it is inside the window."""
+    wl = I.plain_table(n=4096, steps=700, pulse_delay=0.3)
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 700)
+    assert bad is None
+    rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    assert info["max_delay"] >= 300
+    e = assert_parity(hist, rho)
+    print("N=4096 rel err rho00 %.3e rho01 %.3e" % e)
