@@ -112,7 +112,32 @@ class ClockSampler:
 
 
 def workload(args, rank: int) -> I.Workload:
-    return I.plain_table(seed=2 + rank, n=args.n, steps=args.warmup + args.steps, pulse_delay=args.pulse_delay)
+    wl = I.plain_table(seed=2 + rank, n=args.n, steps=args.warmup + args.steps, pulse_delay=args.pulse_delay)
+    if args.dipole_scale != 1.0:
+        wl.dots[:, 6:9] *= args.dipole_scale
+    return wl
+
+
+def fp64_peak_tflops() -> float:
+    """Dense FP64 throughput of this GPU, measured as the best of 5 cuBLAS
+    DGEMMs of 8192^3 (2 n^3 flops each), CUDA events."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    best = 1e30
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / (best / 1e3) / 1e12
 
 
 def dist_setup(args):
@@ -211,9 +236,13 @@ def run_ours(args, world, rank, local):
     weights = capi.pc_weights()
 
     # ---- device-resident throughput (value) and the sweep kernel's roofline
+    nonfinite = None
     sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights)
     info = sim.info()
-    sim.run(args.warmup, record=False)
+    try:
+        sim.run(args.warmup, record=False)
+    except capi.NonFiniteError as e:
+        nonfinite = e.step
     sim.set_option("profile", 1)
     sim.kernel_time(reset=True)
     stream = torch.cuda.ExternalStream(capi.lib().qg_stream(sim.h))
@@ -223,7 +252,10 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clocks:
         e0.record(stream)
-        sim.run(args.steps, record=False)
+        try:
+            sim.run(args.steps, record=False)
+        except capi.NonFiniteError as e:
+            nonfinite = e.step if nonfinite is None else nonfinite
         e1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
@@ -240,7 +272,10 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights) as sim2:
-        sim2.run(total, out=rho_host)
+        try:
+            sim2.run(total, out=rho_host)
+        except capi.NonFiniteError:
+            pass
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)
@@ -248,25 +283,34 @@ def run_ours(args, world, rank, local):
 
     hbm, src = peaks()
     q = 5
+    K = info["time_block"]
     alg_bytes = info["num_pairs"] * TABLE_BYTES_PER_PAIR(q)
+    far_pairs = info["num_pairs"] - info["mid_pairs"]
+    flops = far_pairs * 2 * K * (q + 1) * 8  # complex multiply-add = 4 FMA = 8 flops
     avg_ms = pair_ms / max(launches, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    traffic = profile_traffic("sweep_table_fp64_N4096")
+    fp64_tf = flops / (avg_ms / 1e3) / 1e12
+    fp64_peak = fp64_peak_tflops()
+    traffic = profile_traffic("far_kernel_fp64_N4096")
     line = {
         "metric": "pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded dots and pulse of the stated distributions)",
         "config": config_dict(args),
-        "roofline": {"bound": "hbm", "kernel": "sweep_table_kernel<5>", "achieved": achieved, "peak": hbm,
+        "roofline": {"bound": "hbm", "kernel": "far_kernel<5,false>", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
-                     "share_of_step": pair_ms / ms if ms > 0 else None},
+                     "algorithmic_bytes_per_launch": alg_bytes, "steps_per_launch": K,
+                     "avg_launch_ms": avg_ms, "share_of_timed_region": pair_ms / ms if ms > 0 else None,
+                     "fp64": {"achieved": fp64_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                              "frac": fp64_tf / fp64_peak, "flops_per_launch": flops,
+                              "peak_source": "measured here: best cuBLAS DGEMM 8192^3"}},
         "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s,
                 "h2d_bytes_per_step": (n * 72 + 80) / total, "d2h_bytes_per_step": n * 32,
                 "includes": "qg_create (dots upload + table build) + qg_run with every step's rho read back"},
         "gpu_launches": launches + args.steps * (1 if info["fused_step"] else 12),
-        "near_pairs": info["near_pairs"], "max_delay": info["max_delay"],
+        "near_pairs": info["near_pairs"], "mid_pairs": info["mid_pairs"], "max_delay": info["max_delay"],
+        "nonfinite_from_step": nonfinite,
         "table_build_ms": info["table_build_ms"],
     }
     cs = clocks.summary()
@@ -289,6 +333,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-t0", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dipole-scale", type=float, default=1.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -165,6 +165,8 @@ typedef struct {
   int ring_depth;        /* W: rho01 steps kept per dot */
   long long num_pairs;   /* N(N-1)/2 */
   long long near_pairs;  /* pairs with floor delay 0 (current-step coupling) */
+  long long mid_pairs;   /* pairs with floor delay < time_block (summed per step) */
+  int time_block;        /* K: steps per pass of the far-pair kernel */
   int coef_mode;         /* resolved qg_coef_mode */
   int precision;         /* qg_precision */
   int fused_step;        /* 1 when all current-step coupling fits one block */

@@ -63,6 +63,7 @@ class QgWeights(ctypes.Structure):
 class QgInfo(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("max_delay", ctypes.c_int), ("ring_depth", ctypes.c_int),
                 ("num_pairs", ctypes.c_longlong), ("near_pairs", ctypes.c_longlong),
+                ("mid_pairs", ctypes.c_longlong), ("time_block", ctypes.c_int),
                 ("coef_mode", ctypes.c_int), ("precision", ctypes.c_int), ("fused_step", ctypes.c_int),
                 ("device_bytes", ctypes.c_size_t), ("table_build_ms", ctypes.c_double)]
 

@@ -69,7 +69,11 @@ struct qg_handle_s {
   double2 *d_fnear_coef = nullptr;
   int *d_gnear_ptr = nullptr, *d_gnear_idx = nullptr;  // general: by internal index
   double2 *d_gnear_coef = nullptr;
-  int *d_ints = nullptr;  // 0 step, 1 done, 2 bad, 3 traj_t0, 4 eval_step, 5 max_delay
+  int *d_mid_ptr = nullptr, *d_mid_idx = nullptr, *d_mid_delay = nullptr;  // delay < K pairs
+  double2 *d_mid_coef = nullptr;
+  // d_ints: 0 step, 1 done, 2 bad, 3 traj_t0, 4 eval_step, 5 max_delay,
+  //         6 far_t0 (run), 7 far block start request, 8 far_t0 (evaluate)
+  int *d_ints = nullptr;
   unsigned long long *d_u64 = nullptr;
   double2 *d_traj = nullptr;  // 2 * traj_k steps x N x 2
   double2 *h_traj = nullptr;  // pinned, same size
@@ -80,12 +84,13 @@ struct qg_handle_s {
   bool fused = true;
   int step_blocks = 0;
   int max_delay = 0;
-  long long near_pairs = 0;
+  long long near_pairs = 0, mid_pairs = 0;
+  int far_block = -0x7fffffff;  // first step of the far block the partials hold
   double table_ms = 0;
   int next_step = 0;
   int eval_cached = -0x7fffffff;
 
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [traj off, traj on]
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // K-step block: [traj off, traj on]
   bool use_graph = true;
   bool profile = false;
   cudaEvent_t ev_a[256], ev_b[256];
@@ -94,9 +99,9 @@ struct qg_handle_s {
   int pair_launches = 0;
   cudaEvent_t ev_chunk[2], ev_copy[2];
 
-  SweepArgs sweep_args() const
+  FarArgs far_args(const int *d_t0, int *far_t0_out) const
   {
-    SweepArgs s{};
+    FarArgs s{};
     s.delay = d_delay;
     s.coef = d_coef;
     s.ring = d_ring;
@@ -108,8 +113,8 @@ struct qg_handle_s {
     s.q = q;
     s.frame = params.frame;
     s.nblk = nblk;
-    s.d_step = d_ints + 0;
-    s.d_bad = d_ints + 2;
+    s.d_t0 = d_t0;
+    s.far_t0_out = far_t0_out;
     return s;
   }
 
@@ -141,6 +146,11 @@ struct qg_handle_s {
     a.slot_dot = d_slot_dot;
     a.user = d_user;
     a.partial = d_partial;
+    a.far_t0 = d_ints + 6;
+    a.mid_ptr = d_mid_ptr;
+    a.mid_idx = d_mid_idx;
+    a.mid_delay = d_mid_delay;
+    a.mid_coef = d_mid_coef;
     a.pcr = d_pcr;
     a.ring = d_ring;
     a.near_ptr = general ? d_gnear_ptr : d_fnear_ptr;
@@ -148,6 +158,7 @@ struct qg_handle_s {
     a.near_coef = general ? d_gnear_coef : d_fnear_coef;
     a.scratch = d_scratch;
     a.traj = nullptr;
+    a.traj_rows = 2 * traj_k;
     a.traj_t0 = d_ints + 3;
     a.d_step = d_ints + 0;
     a.d_done = d_ints + 1;
@@ -287,45 +298,80 @@ static size_t table_bytes(long long nblk, int q)
   return (size_t)nblk * kTilePairs * (sizeof(int) + sizeof(double2) * (q + 1));
 }
 
-static qg_status build_near(qg_handle *h)
+static int ring_depth(int max_delay, int q) { return max_delay + q + kTimeBlock + 2; }
+
+// Steps per trajectory staging chunk: a multiple of K, about 32 MiB.
+static int traj_steps(int n)
 {
-  // 1. extract delay-0 pairs
-  const unsigned long long cap = (unsigned long long)std::max<long long>(h->near_pairs, 1);
+  long long k = std::min<long long>(256, (32ll << 20) / (32ll * n));
+  k = std::max<long long>(kTimeBlock, k - k % kTimeBlock);
+  return (int)k;
+}
+
+// Builds the per-step lists from the pairs with floor delay < K: the mid
+// list (all their taps, read by the dot-step kernels every step) and the near
+// list (tap 0 of the delay-0 pairs, re-read in every corrector iteration),
+// and packs the groups of dots coupled at delay 0 into step blocks.
+static qg_status build_lists(qg_handle *h)
+{
+  const int q1 = h->q + 1;
+  const unsigned long long cap = (unsigned long long)std::max<long long>(h->mid_pairs, 1);
   int *d_pairs = nullptr;
-  double2 *d_nc = nullptr;
-  QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 2 * cap));
-  QG_CUDA(cudaMalloc(&d_nc, sizeof(double2) * cap));
-  QG_CUDA(cudaMemsetAsync(h->d_u64 + 1, 0, sizeof(unsigned long long), h->stream));
-  if(h->near_pairs > 0)
-    launch_near_extract(h->d_delay, h->d_coef, h->nblk, h->nT, h->q, d_pairs, d_nc, h->d_u64 + 1, cap,
-                        h->stream);
-  std::vector<int> pairs(2 * cap);
-  std::vector<double2> nc(cap);
-  QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 2 * cap, cudaMemcpyDeviceToHost,
+  double2 *d_mc = nullptr;
+  QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
+  QG_CUDA(cudaMalloc(&d_mc, sizeof(double2) * q1 * cap));
+  QG_CUDA(cudaMemsetAsync(h->d_u64 + 2, 0, sizeof(unsigned long long), h->stream));
+  if(h->mid_pairs > 0)
+    launch_mid_extract(h->d_delay, h->d_coef, h->nblk, h->q, d_pairs, d_mc, h->d_u64 + 2, cap, h->stream);
+  std::vector<int> pairs(3 * cap);
+  std::vector<double2> mc(q1 * cap);
+  QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 3 * cap, cudaMemcpyDeviceToHost,
                           h->stream));
-  QG_CUDA(cudaMemcpyAsync(nc.data(), d_nc, sizeof(double2) * cap, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaMemcpyAsync(mc.data(), d_mc, sizeof(double2) * q1 * cap, cudaMemcpyDeviceToHost,
+                          h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   cudaFree(d_pairs);
-  cudaFree(d_nc);
-  const long long m = h->near_pairs;
-
-  // 2. general CSR by internal index (both directions), sorted partners
+  cudaFree(d_mc);
+  const long long m = h->mid_pairs;
   const int n = h->n;
-  std::vector<std::vector<std::pair<int, double2>>> adj(n);
+
+  // mid list: both directions, partners in increasing order
+  struct MidEntry {
+    int b, d;
+    long long k;  // index into pairs / mc
+  };
+  std::vector<std::vector<MidEntry>> mid(n);
+  std::vector<std::vector<std::pair<int, double2>>> adj(n);  // delay-0 tap-0 coupling
   DSU dsu(n);
   for(long long k = 0; k < m; ++k) {
-    const int a = pairs[2 * k], b = pairs[2 * k + 1];
-    adj[a].push_back({b, nc[k]});
-    adj[b].push_back({a, nc[k]});
-    dsu.unite(a, b);
+    const int a = pairs[3 * k], b = pairs[3 * k + 1], d = pairs[3 * k + 2];
+    mid[a].push_back({b, d, k});
+    mid[b].push_back({a, d, k});
+    if(d == 0) {
+      adj[a].push_back({b, mc[k * q1]});
+      adj[b].push_back({a, mc[k * q1]});
+      dsu.unite(a, b);
+    }
+  }
+  std::vector<int> mptr(n + 1, 0), midx, mdel;
+  std::vector<double2> mcoef;
+  midx.reserve(2 * m);
+  mdel.reserve(2 * m);
+  mcoef.reserve(2 * m * q1);
+  for(int i = 0; i < n; ++i) {
+    std::sort(mid[i].begin(), mid[i].end(), [](const MidEntry &x, const MidEntry &y) { return x.b < y.b; });
+    for(auto &e : mid[i]) {
+      midx.push_back(e.b);
+      mdel.push_back(e.d);
+      for(int t = 0; t < q1; ++t) mcoef.push_back(mc[e.k * q1 + t]);
+    }
+    mptr[i + 1] = (int)midx.size();
   }
   for(auto &v : adj)
     std::sort(v.begin(), v.end(), [](const std::pair<int, double2> &x,
                                      const std::pair<int, double2> &y) { return x.first < y.first; });
   std::vector<int> gptr(n + 1, 0), gidx;
   std::vector<double2> gcoef;
-  gidx.reserve(2 * m);
-  gcoef.reserve(2 * m);
   for(int i = 0; i < n; ++i) {
     for(auto &e : adj[i]) {
       gidx.push_back(e.first);
@@ -334,7 +380,7 @@ static qg_status build_near(qg_handle *h)
     gptr[i + 1] = (int)gidx.size();
   }
 
-  // 3. pack connected components into step blocks (fused form)
+  // pack connected delay-0 groups into step blocks (fused form)
   std::vector<std::vector<int>> comps;
   {
     std::vector<int> root_to_comp(n, -1);
@@ -380,8 +426,8 @@ static qg_status build_near(qg_handle *h)
         slot_dot[b * kStepBlock + j] = bins[b][j];
         local[bins[b][j]] = (int)j;
       }
-    for(size_t s = 0; s < slot_dot.size(); ++s) {
-      const int i = slot_dot[s];
+    for(size_t sl = 0; sl < slot_dot.size(); ++sl) {
+      const int i = slot_dot[sl];
       if(i >= 0)
         for(auto &e : adj[i]) {
           fidx.push_back(local[e.first]);
@@ -396,40 +442,43 @@ static qg_status build_near(qg_handle *h)
     fptr.assign(slot_dot.size() + 1, 0);
   }
 
-  QG_TRY(dalloc(h, &h->d_gnear_ptr, gptr.size()));
-  QG_TRY(dalloc(h, &h->d_gnear_idx, gidx.size()));
-  QG_TRY(dalloc(h, &h->d_gnear_coef, gcoef.size()));
-  QG_TRY(dalloc(h, &h->d_fnear_ptr, fptr.size()));
-  QG_TRY(dalloc(h, &h->d_fnear_idx, fidx.size()));
-  QG_TRY(dalloc(h, &h->d_fnear_coef, fcoef.size()));
-  QG_TRY(dalloc(h, &h->d_slot_dot, slot_dot.size()));
-  QG_CUDA(cudaMemcpy(h->d_gnear_ptr, gptr.data(), sizeof(int) * gptr.size(), cudaMemcpyHostToDevice));
-  if(!gidx.empty()) {
-    QG_CUDA(cudaMemcpy(h->d_gnear_idx, gidx.data(), sizeof(int) * gidx.size(), cudaMemcpyHostToDevice));
-    QG_CUDA(cudaMemcpy(h->d_gnear_coef, gcoef.data(), sizeof(double2) * gcoef.size(),
-                       cudaMemcpyHostToDevice));
-  }
-  QG_CUDA(cudaMemcpy(h->d_fnear_ptr, fptr.data(), sizeof(int) * fptr.size(), cudaMemcpyHostToDevice));
-  if(!fidx.empty()) {
-    QG_CUDA(cudaMemcpy(h->d_fnear_idx, fidx.data(), sizeof(int) * fidx.size(), cudaMemcpyHostToDevice));
-    QG_CUDA(cudaMemcpy(h->d_fnear_coef, fcoef.data(), sizeof(double2) * fcoef.size(),
-                       cudaMemcpyHostToDevice));
-  }
-  QG_CUDA(cudaMemcpy(h->d_slot_dot, slot_dot.data(), sizeof(int) * slot_dot.size(),
-                     cudaMemcpyHostToDevice));
+  auto upload_i = [&](int **dst, const std::vector<int> &v) -> qg_status {
+    QG_TRY(dalloc(h, dst, v.size()));
+    if(!v.empty()) QG_CUDA(cudaMemcpy(*dst, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice));
+    return QG_OK;
+  };
+  auto upload_c = [&](double2 **dst, const std::vector<double2> &v) -> qg_status {
+    QG_TRY(dalloc(h, dst, v.size()));
+    if(!v.empty())
+      QG_CUDA(cudaMemcpy(*dst, v.data(), sizeof(double2) * v.size(), cudaMemcpyHostToDevice));
+    return QG_OK;
+  };
+  QG_TRY(upload_i(&h->d_mid_ptr, mptr));
+  QG_TRY(upload_i(&h->d_mid_idx, midx));
+  QG_TRY(upload_i(&h->d_mid_delay, mdel));
+  QG_TRY(upload_c(&h->d_mid_coef, mcoef));
+  QG_TRY(upload_i(&h->d_gnear_ptr, gptr));
+  QG_TRY(upload_i(&h->d_gnear_idx, gidx));
+  QG_TRY(upload_c(&h->d_gnear_coef, gcoef));
+  QG_TRY(upload_i(&h->d_fnear_ptr, fptr));
+  QG_TRY(upload_i(&h->d_fnear_idx, fidx));
+  QG_TRY(upload_c(&h->d_fnear_coef, fcoef));
+  QG_TRY(upload_i(&h->d_slot_dot, slot_dot));
   return QG_OK;
 }
 
 static qg_status reset_state(qg_handle *h)
 {
   QG_CUDA(cudaMemsetAsync(h->d_ring, 0, sizeof(double2) * (size_t)h->n_pad * h->stride, h->stream));
-  QG_CUDA(cudaMemsetAsync(h->d_partial, 0, sizeof(double2) * (size_t)h->nT * h->n_pad, h->stream));
+  QG_CUDA(cudaMemsetAsync(h->d_partial, 0,
+                          sizeof(double2) * (size_t)kTimeBlock * h->nT * h->n_pad, h->stream));
   launch_init_state(h->step_args(false), h->stream);
-  int init[6] = {0, 0, kBadNone, 0, 0, 0};
-  QG_CUDA(cudaMemcpyAsync(h->d_ints, init, sizeof(int) * 5, cudaMemcpyHostToDevice, h->stream));
+  int init[9] = {0, 0, kBadNone, 0, 0, h->max_delay, 0, 0, 0};
+  QG_CUDA(cudaMemcpyAsync(h->d_ints, init, sizeof init, cudaMemcpyHostToDevice, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   h->next_step = 0;
   h->eval_cached = -0x7fffffff;
+  h->far_block = -0x7fffffff;
   return QG_OK;
 }
 
@@ -535,9 +584,9 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaGetLastError());
   QG_CUDA(cudaEventRecord(e1, h->stream));
   int md = 0;
-  unsigned long long nn = 0;
+  unsigned long long nn[2] = {0, 0};
   QG_CUDA(cudaMemcpyAsync(&md, h->d_ints + 5, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  QG_CUDA(cudaMemcpyAsync(&nn, h->d_u64, sizeof nn, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaMemcpyAsync(nn, h->d_u64, sizeof nn, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   float tms = 0;
   cudaEventElapsedTime(&tms, e0, e1);
@@ -548,16 +597,19 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: floor delay %d out of range (non-finite positions?)",
                    md);
   h->max_delay = md;
-  h->near_pairs = (long long)nn;
+  h->near_pairs = (long long)nn[0];
+  h->mid_pairs = (long long)nn[1];
 
-  // rings and scratch
-  h->W = std::max(md + h->q + 2, 8);
+  // rings and scratch.  W covers the oldest sample a far block reads
+  // (t0 - max_delay - q) even when the block is recomputed up to K - 1
+  // steps after t0.
+  h->W = ring_depth(md, h->q);
   h->stride = h->W + kRingMirror;
   QG_TRY(dalloc(h, &h->d_ring, (size_t)h->n_pad * h->stride));
   QG_TRY(dalloc(h, &h->d_pcr, (size_t)kPcDepth * 4 * h->n_pad));
-  QG_TRY(dalloc(h, &h->d_partial, (size_t)h->nT * h->n_pad));
+  QG_TRY(dalloc(h, &h->d_partial, (size_t)kTimeBlock * h->nT * h->n_pad));
   QG_TRY(dalloc(h, &h->d_scratch, (size_t)h->n_pad * 8));
-  h->traj_k = (int)std::max<long long>(1, std::min<long long>(256, (32ll << 20) / (32ll * n)));
+  h->traj_k = traj_steps(n);
   QG_TRY(dalloc(h, &h->d_traj, (size_t)2 * h->traj_k * n * 2));
   QG_CUDA(cudaMallocHost((void **)&h->h_traj, sizeof(double2) * (size_t)2 * h->traj_k * n * 2));
   QG_TRY(dalloc(h, &h->d_io, (size_t)n));
@@ -572,7 +624,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   }
   h->events_ready = true;
 
-  QG_TRY(build_near(h));
+  QG_TRY(build_lists(h));
   QG_TRY(reset_state(h));
   return QG_OK;
 }
@@ -599,13 +651,24 @@ extern "C" qg_status qg_destroy(qg_handle *h)
   return QG_OK;
 }
 
-// One step's launches: the past pair sum, then the per-dot integrator.
-static void enqueue_step(qg_handle *h, bool traj, bool timed, int ev)
+// The far-pair kernel for the block that starts at t0.  At a block
+// boundary it reads t0 from the device step counter (so it can live in a
+// CUDA graph); a block resumed part-way (after qg_history_evaluate reused the
+// partial buffer, or when a run starts off a boundary) gets t0 explicitly.
+static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, cudaEvent_t eb)
 {
-  SweepArgs sa = h->sweep_args();
-  if(timed) cudaEventRecord(h->ev_a[ev], h->stream);
-  if(h->nblk > 0) launch_sweep_table(sa, h->stream);
-  if(timed) cudaEventRecord(h->ev_b[ev], h->stream);
+  const int *src = h->d_ints + 0;
+  if(!at_boundary) {
+    launch_set_int(h->d_ints + 7, t0, h->stream);
+    src = h->d_ints + 7;
+  }
+  if(ea) cudaEventRecord(ea, h->stream);
+  launch_far(h->far_args(src, h->d_ints + 6), h->stream);
+  if(eb) cudaEventRecord(eb, h->stream);
+}
+
+static void enqueue_dot_step(qg_handle *h, bool traj)
+{
   StepArgs a = h->step_args(!h->fused);
   if(traj) a.traj = h->d_traj;
   if(h->fused) {
@@ -615,43 +678,62 @@ static void enqueue_step(qg_handle *h, bool traj, bool timed, int ev)
   }
 }
 
+// One K-step block starting on a boundary: far kernel + K dot steps.
 static qg_status ensure_graph(qg_handle *h, int traj)
 {
   if(h->graph[traj]) return QG_OK;
   cudaGraph_t g;
   QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_step(h, traj != 0, false, 0);
+  enqueue_far(h, 0, true, nullptr, nullptr);
+  for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, traj != 0);
   QG_CUDA(cudaStreamEndCapture(h->stream, &g));
   QG_CUDA(cudaGraphInstantiate(&h->graph[traj], g, 0));
   cudaGraphDestroy(g);
   return QG_OK;
 }
 
-static qg_status launch_steps(qg_handle *h, int count, bool traj)
+static qg_status collect_events(qg_handle *h, int nev)
 {
-  if(h->profile) {
-    for(int done = 0; done < count;) {
-      const int k = std::min(count - done, 256);
-      for(int j = 0; j < k; ++j) enqueue_step(h, traj, true, j);
-      QG_CUDA(cudaGetLastError());
-      QG_CUDA(cudaEventSynchronize(h->ev_b[k - 1]));
-      for(int j = 0; j < k; ++j) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, h->ev_a[j], h->ev_b[j]);
-        h->pair_ms += ms;
-      }
-      h->pair_launches += (h->nblk > 0) ? k : 0;
-      done += k;
+  if(nev == 0) return QG_OK;
+  QG_CUDA(cudaEventSynchronize(h->ev_b[nev - 1]));
+  for(int j = 0; j < nev; ++j) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev_a[j], h->ev_b[j]);
+    h->pair_ms += ms;
+  }
+  h->pair_launches += nev;
+  return QG_OK;
+}
+
+// Enqueues steps [t, t + count); whole aligned blocks replay the graph.
+static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
+{
+  int nev = 0;
+  while(count > 0) {
+    const int t0 = t - t % kTimeBlock;
+    if(t == t0 && count >= kTimeBlock && h->use_graph && !h->profile) {
+      QG_TRY(ensure_graph(h, traj ? 1 : 0));
+      QG_CUDA(cudaGraphLaunch(h->graph[traj ? 1 : 0], h->stream));
+      h->far_block = t0;
+      t += kTimeBlock;
+      count -= kTimeBlock;
+      continue;
     }
-    return QG_OK;
+    if(h->far_block != t0) {
+      enqueue_far(h, t0, t == t0, h->profile ? h->ev_a[nev] : nullptr,
+                  h->profile ? h->ev_b[nev] : nullptr);
+      if(h->profile && ++nev == 256) {
+        QG_TRY(collect_events(h, nev));
+        nev = 0;
+      }
+      h->far_block = t0;
+    }
+    enqueue_dot_step(h, traj);
+    ++t;
+    --count;
   }
-  if(h->use_graph) {
-    QG_TRY(ensure_graph(h, traj ? 1 : 0));
-    for(int j = 0; j < count; ++j) QG_CUDA(cudaGraphLaunch(h->graph[traj ? 1 : 0], h->stream));
-  } else {
-    for(int j = 0; j < count; ++j) enqueue_step(h, traj, false, 0);
-    QG_CUDA(cudaGetLastError());
-  }
+  QG_CUDA(cudaGetLastError());
+  if(h->profile) QG_TRY(collect_events(h, nev));
   return QG_OK;
 }
 
@@ -668,7 +750,7 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   h->eval_cached = -0x7fffffff;
   const size_t row = (size_t)h->n * 2;  // double2 per step
   if(!rho_out) {
-    QG_TRY(launch_steps(h, n_steps, false));
+    QG_TRY(launch_steps(h, t_start, n_steps, false));
   } else {
     const int K = h->traj_k;
     const int nchunks = (n_steps + K - 1) / K;
@@ -688,7 +770,7 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
         QG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_copy[b], 0));
       }
       launch_set_int(h->d_ints + 3, t_start + c * K - b * K, h->stream);
-      QG_TRY(launch_steps(h, k, true));
+      QG_TRY(launch_steps(h, t_start + c * K, k, true));
       QG_CUDA(cudaEventRecord(h->ev_chunk[b], h->stream));
       QG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ev_chunk[b], 0));
       QG_CUDA(cudaMemcpyAsync(h->h_traj + (size_t)b * K * row, h->d_traj + (size_t)b * K * row,
@@ -702,6 +784,8 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   QG_CUDA(cudaStreamSynchronize(h->stream));
   QG_CUDA(cudaGetLastError());
   h->next_step = t_start + n_steps;
+  if(bad < 0)
+    return qg_fail(QG_ERR_CUDA, "qg_run: internal scheduling error (far block or trajectory row)");
   if(bad != kBadNone) {
     if(bad_step) *bad_step = bad;
     return qg_fail(QG_ERR_NONFINITE, "unbounded history values at or before step %d", bad);
@@ -744,12 +828,13 @@ extern "C" qg_status qg_history_evaluate(qg_handle *h, int step, const double *r
     launch_ring_write(a, step, h->d_io, h->stream);
   }
   if(h->eval_cached != step) {
+    // the far partials of [step, step + K) in the run's buffer
     launch_set_int(h->d_ints + 4, step, h->stream);
-    SweepArgs sa = h->sweep_args();
-    sa.d_step = h->d_ints + 4;
-    if(h->nblk > 0) launch_sweep_table(sa, h->stream);
+    launch_far(h->far_args(h->d_ints + 4, h->d_ints + 8), h->stream);
     h->eval_cached = step;
+    h->far_block = -0x7fffffff;
   }
+  a.far_t0 = h->d_ints + 4;
   launch_eval_field(a, h->d_ints + 4, h->d_io, h->stream);
   QG_CUDA(cudaGetLastError());
   return download_io(h, field_out);
@@ -778,6 +863,7 @@ extern "C" qg_status qg_set_history(qg_handle *h, int t0, int n, const double *r
   }
   QG_CUDA(cudaGetLastError());
   h->eval_cached = -0x7fffffff;
+  h->far_block = -0x7fffffff;
   return QG_OK;
 }
 
@@ -804,6 +890,8 @@ extern "C" qg_status qg_get_info(const qg_handle *h, qg_info *info)
   info->ring_depth = h->W;
   info->num_pairs = h->P;
   info->near_pairs = h->near_pairs;
+  info->mid_pairs = h->mid_pairs;
+  info->time_block = kTimeBlock;
   info->coef_mode = QG_COEF_TABLE;
   info->precision = QG_PREC_FP64;
   info->fused_step = h->fused ? 1 : 0;
@@ -819,14 +907,14 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
   const long long nblk = (long long)nT * (nT + 1) / 2;
   const int q = p->interpolation_order;
   const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
-  const int W = std::max(md + q + 2, 8);
+  const int W = ring_depth(md, q);
   size_t b = table_bytes(nblk, q);
   b += sizeof(double2) * (size_t)n_pad * (W + kRingMirror);
   b += sizeof(double2) * (size_t)kPcDepth * 4 * n_pad;
-  b += sizeof(double2) * (size_t)nT * n_pad;
+  b += sizeof(double2) * (size_t)kTimeBlock * nT * n_pad;
   b += sizeof(double2) * (size_t)n_pad * 8;
   b += sizeof(double) * (size_t)n_pad * 9 + sizeof(int) * (size_t)n_pad * 2;
-  const long long K = std::max<long long>(1, std::min<long long>(256, (32ll << 20) / (32ll * n)));
+  const long long K = traj_steps(n);
   b += sizeof(double2) * (size_t)(2 * K * n * 2) + sizeof(double2) * (size_t)n;  // trajectory + io staging
   *bytes = b;
   return QG_OK;

@@ -16,8 +16,9 @@ namespace qg {
 constexpr int kWindow = 22;      // History's negative-time extent (main.cpp:30)
 constexpr int kCorrectorSteps = 10;  // NUM_CORRECTOR_STEPS (integrator.cpp:3)
 constexpr int kMaxOrder = 7;     // largest interpolation order built
-constexpr int kRingMirror = 8;   // slots mirrored past the ring end (>= q+1)
-constexpr int kTile = 64;        // dots per table tile
+constexpr int kTimeBlock = 8;    // K: steps per pass of the far-pair kernel
+constexpr int kRingMirror = 16;  // slots mirrored past the ring end (>= K+q)
+constexpr int kTile = 32;        // dots per table tile (one warp per tile pair)
 constexpr int kTilePairs = kTile * kTile;
 constexpr int kPcDepth = 23;     // PC ring: 22 past steps + the current one
 constexpr int kStepBlock = 128;  // threads per block of the dot-step kernel
@@ -54,20 +55,21 @@ struct TableArgs {
   int *delay;          // [nblk][kTilePairs]
   double2 *coef;       // [nblk][q+1][kTilePairs]
   int *max_delay;      // atomicMax
-  unsigned long long *near_count;
+  unsigned long long *near_count;  // [0] pairs with delay 0, [1] pairs with delay < K
   CoefParams cp;
 };
 
-// Arguments of the pair-sum (sweep) kernel over the FP64 table.
-struct SweepArgs {
+// Arguments of the far-pair kernel: K steps of the pair sum for every pair
+// with floor delay >= K, from one pass over the table.
+struct FarArgs {
   const int *delay;
   const double2 *coef;
-  const double2 *ring;  // [n_pad][stride]: prefactor(rho01) by time slot
-  double2 *partial;     // [nT][n_pad]
+  const double2 *ring;  // [n_pad][stride]: rho01 by time slot
+  double2 *partial;     // [K][nT][n_pad]
   int n_pad, nT, W, stride, q, frame;
   long long nblk;
-  const int *d_step;
-  const int *d_bad;
+  const int *d_t0;      // first step of the block
+  int *far_t0_out;      // receives *d_t0 (read by the dot-step kernels)
 };
 
 // Arguments of the per-dot step kernels.
@@ -80,7 +82,14 @@ struct StepArgs {
   const double *freq, *t1, *t2;
   const int *slot_dot;   // slot -> internal index (-1 empty)
   const int *user;       // internal -> user
-  const double2 *partial;
+  const double2 *partial;  // [K][nT][n_pad] far-pair sums
+  const int *far_t0;     // first step of the far block partial[] holds
+  // pairs with floor delay < K (taps not covered by the far kernel): CSR by
+  // internal index, partner, delay and q+1 coefficients
+  const int *mid_ptr;
+  const int *mid_idx;
+  const int *mid_delay;
+  const double2 *mid_coef;  // [entry][q+1]
   double2 *pcr;          // [kPcDepth][4][n_pad]
   double2 *ring;         // [n_pad][stride] rho01 by step slot
   // current-step coupling: CSR by slot (fused: partner = local slot in the
@@ -91,6 +100,7 @@ struct StepArgs {
   // general path scratch
   double2 *scratch;      // [n_pad][8]: past field, pulse, H (2 complex), cur rho x2
   double2 *traj;         // [k][n][2] user order or null
+  int traj_rows;         // rows allocated in traj
   const int *traj_t0;
   int *d_step, *d_done, *d_bad;
   PCW w;
@@ -98,10 +108,10 @@ struct StepArgs {
 
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);
-void launch_near_extract(const int *delay, const double2 *coef, long long nblk, int nT,
-                         int q, int *out_pairs /*[cap][2] internal a,b*/, double2 *out_coef,
-                         unsigned long long *counter, unsigned long long cap, void *stream);
-void launch_sweep_table(const SweepArgs &a, void *stream);
+void launch_mid_extract(const int *delay, const double2 *coef, long long nblk, int q,
+                        int *out_pairs /*[cap][3] internal a, b, delay*/, double2 *out_coef,
+                        unsigned long long *counter, unsigned long long cap, void *stream);
+void launch_far(const FarArgs &a, void *stream);
 void launch_step_fused(const StepArgs &a, int nblocks, void *stream);
 void launch_step_general(const StepArgs &a, int phase, void *stream);
 void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream);

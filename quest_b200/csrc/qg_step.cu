@@ -9,9 +9,13 @@
 //   liouville_rhs        src/quantum_dot.cpp:10-19
 //   all_finite           integrator.cpp:187-198
 //
-// The strictly-past part of the history field comes from the sweep kernel's
-// partial sums.  The (delay 0, tap 0) terms, which read the current step's
-// iterate, are re-evaluated in each of the 11 evaluations from a near list.
+// The strictly-past part of the history field has two sources: the far-pair
+// kernel's partial sums (pairs with floor delay >= K, computed once per K
+// steps) and the mid list (pairs with delay < K), summed here every step.
+// The (delay 0, tap 0) terms, which read the current step's iterate, are
+// re-evaluated in each of the 11 evaluations from a near list.  Work does not
+// stop after a non-finite value: the first such step is recorded and every
+// step is computed, so the cost per step does not depend on the data.
 //
 // Two forms.  The fused kernel runs predictor, 11 evaluations and 10
 // corrections in one launch: every connected group of dots coupled at delay
@@ -99,13 +103,38 @@ __device__ __forceinline__ void pc_window(const StepArgs &a, int idx, int t, dou
   }
 }
 
-__device__ __forceinline__ double2 past_field(const StepArgs &a, int idx)
+__device__ __forceinline__ int ring_slot(int t, int W) { return ((t % W) + W) % W; }
+
+// Field at step t from every tap that reads a step before t: the far-pair
+// partials of this step's slice, then the mid-list pairs (delay < K), taps
+// before step -22 skipped and the (delay 0, tap 0) term left to the near list.
+__device__ __forceinline__ double2 past_field(const StepArgs &a, int idx, int t)
 {
   double2 f = make_double2(0.0, 0.0);
+  const int slice = t - *a.far_t0;
+  if(slice < 0 || slice >= kTimeBlock) {
+    // the host did not run the far kernel for this block: flag, do not read
+    atomicMin(a.d_bad, -1);
+    return make_double2(nan(""), nan(""));
+  }
+  const double2 *P = a.partial + (long long)slice * a.nT * a.n_pad + idx;
   for(int k = 0; k < a.nT; ++k) {
-    const double2 v = a.partial[(long long)k * a.n_pad + idx];
+    const double2 v = P[(long long)k * a.n_pad];
     f.x += v.x;
     f.y += v.y;
+  }
+  const int q = a.q;
+  for(int e = a.mid_ptr[idx]; e < a.mid_ptr[idx + 1]; ++e) {
+    const int b = a.mid_idx[e];
+    const int d = a.mid_delay[e];
+    const double2 *c = a.mid_coef + (long long)e * (q + 1);
+    const double2 *ring = a.ring + (long long)b * a.stride;
+    const int s = t - d;
+    for(int i = (d == 0) ? 1 : 0; i <= q && s - i >= -kWindow; ++i) {
+      const double2 v = cmul(prefactor(ring[ring_slot(s - i, a.W)], a.frame), c[i]);
+      f.x += v.x;
+      f.y += v.y;
+    }
   }
   return f;
 }
@@ -142,9 +171,13 @@ __device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, co
   if(slot < kRingMirror) ring[a.W + slot] = r[1];
   if(a.traj) {
     const int row = t - *a.traj_t0;
-    double2 *tr = a.traj + ((long long)row * a.n + a.user[idx]) * 2;
-    tr[0] = r[0];
-    tr[1] = r[1];
+    if(row >= 0 && row < a.traj_rows) {
+      double2 *tr = a.traj + ((long long)row * a.n + a.user[idx]) * 2;
+      tr[0] = r[0];
+      tr[1] = r[1];
+    } else {
+      atomicMin(a.d_bad, -1);
+    }
   }
   if(!finite4(r[0], r[1]) || !finite4(dr[0], dr[1])) atomicMin(a.d_bad, t);
 }
@@ -169,7 +202,7 @@ __global__ void __launch_bounds__(kStepBlock) step_fused_kernel(StepArgs a)
   const int slot = blockIdx.x * kStepBlock + threadIdx.x;
   const int idx = a.slot_dot[slot];
   const int t = *a.d_step;
-  const bool live = idx >= 0 && *a.d_bad >= t;
+  const bool live = idx >= 0;
   const int nb0 = a.near_ptr[blockIdx.x * kStepBlock];
   const bool block_near = a.near_ptr[(blockIdx.x + 1) * kStepBlock] > nb0;
 
@@ -177,7 +210,7 @@ __global__ void __launch_bounds__(kStepBlock) step_fused_kernel(StepArgs a)
   double det = 0, t1 = 1, t2 = 1, pul = 0;
   if(live) {
     pc_window(a, idx, t, P, H);
-    past = past_field(a, idx);
+    past = past_field(a, idx, t);
     pul = pulse_rabi(a, idx, t);
     det = a.laser_freq - a.freq[idx];
     t1 = a.t1[idx];
@@ -217,13 +250,13 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
 {
   const int idx = blockIdx.x * kStepBlock + threadIdx.x;
   const int t = *a.d_step;
-  const bool live = idx < a.n && *a.d_bad >= t;
+  const bool live = idx < a.n;
   double2 *sc = a.scratch + (long long)idx * 8;
   if(phase == 0) {
     if(live) {
       double2 P[2], H[2];
       pc_window(a, idx, t, P, H);
-      sc[0] = past_field(a, idx);
+      sc[0] = past_field(a, idx, t);
       sc[1] = make_double2(pulse_rabi(a, idx, t), 0.0);
       sc[2] = H[0];
       sc[3] = H[1];
@@ -278,8 +311,8 @@ __global__ void eval_field_kernel(StepArgs a, const int *d_eval_step, double2 *o
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if(idx >= a.n) return;
   const int step = *d_eval_step;
-  const int slot = ((step % a.W) + a.W) % a.W;
-  double2 f = past_field(a, idx);
+  const int slot = ring_slot(step, a.W);
+  double2 f = past_field(a, idx, step);
   for(int e = a.near_ptr[idx]; e < a.near_ptr[idx + 1]; ++e) {
     const int b = a.near_idx[e];
     const double2 v = cmul(prefactor(a.ring[(long long)b * a.stride + slot], a.frame), a.near_coef[e]);

@@ -2,16 +2,17 @@
 // (reference src/interactions/history_interaction.cpp:21-45) as one kernel.
 //
 // Layout in HBM.  Dots are in internal (Morton) order, padded to a multiple
-// of kTile = 64.  The unordered pairs are grouped into tile blocks (I, J),
-// I >= J, numbered blk = I(I+1)/2 + J.  Block blk holds kTilePairs = 4096
-// entries e = la*64 + lb (dot a = 64 I + la, dot b = 64 J + lb):
+// of kTile = 32.  The unordered pairs are grouped into tile blocks (I, J),
+// I >= J, numbered blk = I(I+1)/2 + J.  Block blk holds kTilePairs = 1024
+// entries in diagonal-major order: entry e = 32 j + l is the pair of dot
+// a = 32 I + l and dot b = 32 J + ((l + j) mod 32), so at step j of the
+// far-pair kernel lane l of a warp reads entry 32 j + l:
 //   delay[blk][e]          int32 floor delay, -1 when the entry is no pair
-//                          (padding, or lb >= la on a diagonal block)
+//                          (padding, or b >= a on a diagonal block)
 //   coef [blk][i][e]       double2 coefficient of tap i = 0..q
-// so a warp reading 32 consecutive entries of one tap is one 512-byte
-// transaction.  Each pair is computed in the reference's own orientation
-// (src = larger user index, obs = smaller) so its rounding is the
-// reference's.
+// A warp reading one tap of one diagonal is one 512-byte transaction.  Each
+// pair is computed in the reference's own orientation (src = larger user
+// index, obs = smaller) so its rounding is the reference's.
 //
 // Compiled with -fmad=false.
 #include <cuda_runtime.h>
@@ -39,7 +40,7 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   const int e = (int)(gid % kTilePairs);
   int I, J;
   decode_block(blk, I, J);
-  const int la = e / kTile, lb = e % kTile;
+  const int la = e % kTile, lb = (la + e / kTile) % kTile;
   const int ia = I * kTile + la, ib = J * kTile + lb;
   int *dptr = a.delay + blk * kTilePairs + e;
   double2 *cptr = a.coef + blk * (long long)(Q + 1) * kTilePairs + e;
@@ -69,6 +70,7 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   for(int i = 0; i <= Q; ++i) cptr[(long long)i * kTilePairs] = coef[i];
   atomicMax(a.max_delay, fd);
   if(fd == 0) atomicAdd(a.near_count, 1ULL);
+  if(fd < kTimeBlock) atomicAdd(a.near_count + 1, 1ULL);
 }
 
 void launch_table_build(const TableArgs &a, int q, void *stream)
@@ -89,36 +91,40 @@ void launch_table_build(const TableArgs &a, int q, void *stream)
   }
 }
 
-// Compacts the delay-0 pairs (the ones whose tap 0 reads the current step)
-// into a list of (a, b, tap-0 coefficient); the host sorts it.
-__global__ void near_extract_kernel(const int *delay, const double2 *coef, long long nblk, int q,
-                                    int *out_pairs, double2 *out_coef,
-                                    unsigned long long *counter, unsigned long long cap)
+// Compacts the pairs with floor delay < K (the ones the far-pair kernel
+// leaves to the per-step kernels) into (a, b, delay) + q+1 coefficients; the
+// host sorts them.
+__global__ void mid_extract_kernel(const int *delay, const double2 *coef, long long nblk, int q,
+                                   int *out_pairs, double2 *out_coef, unsigned long long *counter,
+                                   unsigned long long cap)
 {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if(gid >= nblk * kTilePairs) return;
-  if(delay[gid] != 0) return;
+  const int d = delay[gid];
+  if(d < 0 || d >= kTimeBlock) return;
   const long long blk = gid / kTilePairs;
   const int e = (int)(gid % kTilePairs);
   int I, J;
   decode_block(blk, I, J);
   const unsigned long long slot = atomicAdd(counter, 1ULL);
   if(slot >= cap) return;
-  out_pairs[2 * slot] = I * kTile + e / kTile;
-  out_pairs[2 * slot + 1] = J * kTile + e % kTile;
-  out_coef[slot] = coef[blk * (long long)(q + 1) * kTilePairs + e];
+  const int la = e % kTile, lb = (la + e / kTile) % kTile;
+  out_pairs[3 * slot] = I * kTile + la;
+  out_pairs[3 * slot + 1] = J * kTile + lb;
+  out_pairs[3 * slot + 2] = d;
+  for(int i = 0; i <= q; ++i)
+    out_coef[slot * (q + 1) + i] = coef[blk * (long long)(q + 1) * kTilePairs + (long long)i * kTilePairs + e];
 }
 
-void launch_near_extract(const int *delay, const double2 *coef, long long nblk, int nT, int q,
-                         int *out_pairs, double2 *out_coef, unsigned long long *counter,
-                         unsigned long long cap, void *stream)
+void launch_mid_extract(const int *delay, const double2 *coef, long long nblk, int q, int *out_pairs,
+                        double2 *out_coef, unsigned long long *counter, unsigned long long cap,
+                        void *stream)
 {
-  (void)nT;
   const long long total = nblk * kTilePairs;
   const int threads = 256;
   const unsigned blocks = (unsigned)((total + threads - 1) / threads);
-  near_extract_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(delay, coef, nblk, q, out_pairs,
-                                                                    out_coef, counter, cap);
+  mid_extract_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(delay, coef, nblk, q, out_pairs,
+                                                                   out_coef, counter, cap);
 }
 
 }  // namespace qg

@@ -1,11 +1,19 @@
 """GPU parity: the CUDA path through the C ABI against the CPU oracle.
 
 Tolerance: max |rho_gpu - rho_oracle| / max |rho_oracle|, per component
-(rho00 and rho01 separately), must be <= 1e-10 for the FP64 path.  The GPU
-sums the pair terms in a different order than the reference (once per step,
-tile by tile), so bitwise equality is not expected; the per-pair terms
-cancel strongly (individual taps are ~1e3 times the field), which is what
-sets the size of the difference.
+(rho00 and rho01 separately), must be <= 1e-10 for the FP64 path.
+
+The GPU sums the pair terms in a different order than the reference (far
+pairs K steps at a time, tile by tile), so bitwise equality is not expected.
+With interpolation order 5 or 7 the reference's scheme amplifies
+rounding-level differences exponentially once the dots are excited (about x10
+every 25 steps at dt = 1e-3 in a 0.2 cube): two summation orders of the
+oracle itself drift apart the same way, and the run eventually overflows.
+Each test therefore stops at a horizon where the oracle's own sensitivity to
+summation order (1 vs 7 threads) is at most ~1e-12, so the 1e-10 bound
+measures the GPU path and not the instability.  Orders 1 and 3 and the lab
+frame are stable and are compared over their whole runs.  The step at which
+the overflow happens is compared separately.
 """
 import os
 
@@ -48,8 +56,8 @@ def load_example(n=None, steps=None):
 
 
 def test_small_against_faithful_oracle(golden_weights, oracle_weights):
-    wl = I.plain_small(n=60, steps=400, pulse_delay=0.2)
-    hist, bad = O.run_faithful(wl.dots, wl.pulse, wl.constants, oracle_weights, 400)
+    wl = I.plain_small(n=60, steps=350, pulse_delay=0.2)
+    hist, bad = O.run_faithful(wl.dots, wl.pulse, wl.constants, oracle_weights, 350)
     assert bad is None
     rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     assert info["fused_step"] == 1
@@ -58,13 +66,27 @@ def test_small_against_faithful_oracle(golden_weights, oracle_weights):
 
 
 def test_plain_small_delay_half(golden_weights, oracle_weights):
-    """N=200, 0.2 cube, 2000 steps, order 5, pulse delay 0.5 (the stated delay
-    5 never reaches the dots before t = 2)."""
-    wl = I.plain_small(n=200, steps=2000, pulse_delay=0.5)
-    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 2000)
+    """N=200, 0.2 cube, order 5, pulse delay 0.5 (the stated delay 5 never
+    reaches the dots before t = 2), compared until step 520."""
+    wl = I.plain_small(n=200, steps=520, pulse_delay=0.5)
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 520)
     assert bad is None
     rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     assert_parity(hist, rho)
+
+
+def test_plain_small_overflows_where_the_oracle_does(golden_weights, oracle_weights):
+    """The same run continued: the reference's scheme overflows about 400
+    steps after the pulse and throws std::domain_error; the GPU path reports
+    the first non-finite step within the oracle's own spread (802 with one
+    and with seven threads, 803 with eight)."""
+    wl = I.plain_small(n=200, steps=900, pulse_delay=0.5)
+    _, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 900)
+    assert bad is not None and 700 < bad < 900
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        with pytest.raises(capi.NonFiniteError) as e:
+            sim.run(900)
+    assert abs(e.value.step - bad) <= 2, (e.value.step, bad)
 
 
 def test_plain_small_as_stated_stays_in_ground_state(golden_weights, oracle_weights):
@@ -99,23 +121,37 @@ def test_reference_example_all_pairs_near(golden_weights, oracle_weights):
     assert_parity(hist, rho)
 
 
+def near_group_workload(steps=400):
+    """N=300 with 12 planted pairs and one triple closer than c dt (delay 0),
+    dipoles 2e-4 (weak enough that order 5 stays stable with them)."""
+    wl = I.plain_small(n=300, steps=steps, pulse_delay=0.15)
+    d = wl.dots
+    d[:, 8] = 2e-4
+    rng = np.random.default_rng(1)
+    for k in range(12):
+        v = rng.normal(size=3)
+        d[2 * k + 1, :3] = d[2 * k, :3] + 8e-4 * v / np.linalg.norm(v)
+    d[30, :3] = d[28, :3] + 8e-4 * np.array([0, 1.0, 0])
+    d[29, :3] = d[28, :3] + 8e-4 * np.array([1.0, 0, 0])
+    return wl
+
+
 def test_small_near_groups_fused(golden_weights, oracle_weights):
-    """A few delay-0 pairs in an otherwise retarded system: the fused kernel
-    with groups packed into blocks."""
-    wl = I.plain_small(n=300, steps=500, pulse_delay=0.15)
-    wl.constants.dt = 2e-3  # c dt = 2e-3: a handful of pairs closer than that
-    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 500)
+    """Delay-0 pairs in an otherwise retarded system: the fused kernel with
+    the coupled groups packed into blocks, iterated with the correctors."""
+    wl = near_group_workload()
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 400)
     assert bad is None
     rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
-    assert info["near_pairs"] > 0 and info["fused_step"] == 1
+    assert info["near_pairs"] >= 14 and info["fused_step"] == 1
     assert_parity(hist, rho)
 
 
-@pytest.mark.parametrize("q", [1, 3, 7])
-def test_interpolation_orders(golden_weights, oracle_weights, q):
-    wl = I.plain_small(n=90, steps=300, pulse_delay=0.15)
+@pytest.mark.parametrize("q,steps", [(1, 300), (3, 300), (7, 200)])
+def test_interpolation_orders(golden_weights, oracle_weights, q, steps):
+    wl = I.plain_small(n=90, steps=steps, pulse_delay=0.15)
     wl.constants.interpolation_order = q
-    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 300)
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, steps)
     assert bad is None
     rho, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     assert_parity(hist, rho)
