@@ -64,7 +64,9 @@ struct qg_handle_s {
   double2 *d_coef = nullptr;
   double2 *d_ring = nullptr;
   int W = 0, stride = 0;
-  double2 *d_pcr = nullptr, *d_partial = nullptr, *d_scratch = nullptr;
+  double2 *d_pcr = nullptr, *d_partial = nullptr, *d_field = nullptr, *d_scratch = nullptr;
+  unsigned *d_tile_done = nullptr;
+  int nG = 0;
   int *d_fnear_ptr = nullptr, *d_fnear_idx = nullptr;  // fused: by slot, local partner
   double2 *d_fnear_coef = nullptr;
   int *d_gnear_ptr = nullptr, *d_gnear_idx = nullptr;  // general: by internal index
@@ -83,6 +85,7 @@ struct qg_handle_s {
 
   bool fused = true;
   int step_blocks = 0;
+  int step_bs = kStepBlock;  // threads per block of the fused step kernel
   int max_delay = 0;
   long long near_pairs = 0, mid_pairs = 0;
   int far_block = -0x7fffffff;  // first step of the far block the partials hold
@@ -106,13 +109,15 @@ struct qg_handle_s {
     s.coef = d_coef;
     s.ring = d_ring;
     s.partial = d_partial;
+    s.field = d_field;
+    s.tile_done = d_tile_done;
     s.n_pad = n_pad;
     s.nT = nT;
+    s.nG = nG;
     s.W = W;
     s.stride = stride;
     s.q = q;
     s.frame = params.frame;
-    s.nblk = nblk;
     s.d_t0 = d_t0;
     s.far_t0_out = far_t0_out;
     return s;
@@ -145,7 +150,7 @@ struct qg_handle_s {
     a.t2 = d_t2;
     a.slot_dot = d_slot_dot;
     a.user = d_user;
-    a.partial = d_partial;
+    a.far_field = d_field;
     a.far_t0 = d_ints + 6;
     a.mid_ptr = d_mid_ptr;
     a.mid_idx = d_mid_idx;
@@ -293,9 +298,10 @@ static qg_status validate(const qg_dot *dots, int n, const qg_pulse *pulse, cons
   return QG_OK;
 }
 
-static size_t table_bytes(long long nblk, int q)
+// Ordered tile pairs: every unordered pair is stored twice.
+static size_t table_bytes(int nT, int q)
 {
-  return (size_t)nblk * kTilePairs * (sizeof(int) + sizeof(double2) * (q + 1));
+  return (size_t)nT * nT * kTilePairs * (sizeof(int) + sizeof(double2) * (q + 1));
 }
 
 static int ring_depth(int max_delay, int q) { return max_delay + q + kTimeBlock + 2; }
@@ -322,7 +328,7 @@ static qg_status build_lists(qg_handle *h)
   QG_CUDA(cudaMalloc(&d_mc, sizeof(double2) * q1 * cap));
   QG_CUDA(cudaMemsetAsync(h->d_u64 + 2, 0, sizeof(unsigned long long), h->stream));
   if(h->mid_pairs > 0)
-    launch_mid_extract(h->d_delay, h->d_coef, h->nblk, h->q, d_pairs, d_mc, h->d_u64 + 2, cap, h->stream);
+    launch_mid_extract(h->d_delay, h->d_coef, h->nT, h->q, d_pairs, d_mc, h->d_u64 + 2, cap, h->stream);
   std::vector<int> pairs(3 * cap);
   std::vector<double2> mc(q1 * cap);
   QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 3 * cap, cudaMemcpyDeviceToHost,
@@ -397,6 +403,9 @@ static qg_status build_lists(qg_handle *h)
   size_t largest = 0;
   for(auto &c : comps) largest = std::max(largest, c.size());
   h->fused = largest <= (size_t)kStepBlock;
+  // small blocks spread a few thousand dots over more SMs
+  h->step_bs = largest <= 32 ? 32 : kStepBlock;
+  const size_t BS = (size_t)h->step_bs;
   std::vector<int> slot_dot;
   std::vector<int> fptr(1, 0), fidx;
   std::vector<double2> fcoef;
@@ -407,23 +416,23 @@ static qg_status build_lists(qg_handle *h)
     for(auto &c : comps) {
       size_t b = 0;
       for(; b < bins.size(); ++b)
-        if(bins[b].size() + c.size() <= (size_t)kStepBlock) break;
+        if(bins[b].size() + c.size() <= BS) break;
       if(b == bins.size()) bins.emplace_back();
       bins[b].insert(bins[b].end(), c.begin(), c.end());
     }
     size_t fill = 0;
     for(int i = 0; i < n; ++i) {
       if(!adj[i].empty()) continue;
-      while(fill < bins.size() && bins[fill].size() >= (size_t)kStepBlock) ++fill;
+      while(fill < bins.size() && bins[fill].size() >= BS) ++fill;
       if(fill == bins.size()) bins.emplace_back();
       bins[fill].push_back(i);
     }
     h->step_blocks = (int)bins.size();
-    slot_dot.assign((size_t)h->step_blocks * kStepBlock, -1);
+    slot_dot.assign((size_t)h->step_blocks * BS, -1);
     std::vector<int> local(n, -1);
     for(size_t b = 0; b < bins.size(); ++b)
       for(size_t j = 0; j < bins[b].size(); ++j) {
-        slot_dot[b * kStepBlock + j] = bins[b][j];
+        slot_dot[b * BS + j] = bins[b][j];
         local[bins[b][j]] = (int)j;
       }
     for(size_t sl = 0; sl < slot_dot.size(); ++sl) {
@@ -471,7 +480,9 @@ static qg_status reset_state(qg_handle *h)
 {
   QG_CUDA(cudaMemsetAsync(h->d_ring, 0, sizeof(double2) * (size_t)h->n_pad * h->stride, h->stream));
   QG_CUDA(cudaMemsetAsync(h->d_partial, 0,
-                          sizeof(double2) * (size_t)kTimeBlock * h->nT * h->n_pad, h->stream));
+                          sizeof(double2) * (size_t)kTimeBlock * h->nG * h->n_pad, h->stream));
+  QG_CUDA(cudaMemsetAsync(h->d_field, 0, sizeof(double2) * (size_t)kTimeBlock * h->n_pad, h->stream));
+  QG_CUDA(cudaMemsetAsync(h->d_tile_done, 0, sizeof(unsigned) * (size_t)h->nT, h->stream));
   launch_init_state(h->step_args(false), h->stream);
   int init[9] = {0, 0, kBadNone, 0, 0, h->max_delay, 0, 0, 0};
   QG_CUDA(cudaMemcpyAsync(h->d_ints, init, sizeof init, cudaMemcpyHostToDevice, h->stream));
@@ -495,6 +506,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   h->pulse = *pulse;
   h->nT = (n + kTile - 1) / kTile;
   h->n_pad = h->nT * kTile;
+  h->nG = (h->nT + kTileGroup - 1) / kTileGroup;
   h->nblk = (long long)h->nT * (h->nT + 1) / 2;
   h->P = (long long)n * (n - 1) / 2;
 
@@ -550,13 +562,13 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaMemset(h->d_u64, 0, sizeof(unsigned long long) * 4));
 
   // coefficient table
-  const size_t tb = table_bytes(h->nblk, h->q);
+  const size_t tb = table_bytes(h->nT, h->q);
   size_t free_b = 0, total_b = 0;
   QG_CUDA(cudaMemGetInfo(&free_b, &total_b));
   if(tb > free_b * 0.9)
     return qg_fail(QG_ERR_OOM, "qg_create: coefficient table needs %zu bytes, %zu free", tb, free_b);
-  QG_TRY(dalloc(h, &h->d_delay, (size_t)h->nblk * kTilePairs));
-  QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nblk * kTilePairs * (h->q + 1)));
+  QG_TRY(dalloc(h, &h->d_delay, (size_t)h->nT * h->nT * kTilePairs));
+  QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nT * h->nT * kTilePairs * (h->q + 1)));
   TableArgs ta{};
   ta.pos = h->d_pos;
   ta.dip = h->d_dip;
@@ -607,7 +619,9 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   h->stride = h->W + kRingMirror;
   QG_TRY(dalloc(h, &h->d_ring, (size_t)h->n_pad * h->stride));
   QG_TRY(dalloc(h, &h->d_pcr, (size_t)kPcDepth * 4 * h->n_pad));
-  QG_TRY(dalloc(h, &h->d_partial, (size_t)kTimeBlock * h->nT * h->n_pad));
+  QG_TRY(dalloc(h, &h->d_partial, (size_t)kTimeBlock * h->nG * h->n_pad));
+  QG_TRY(dalloc(h, &h->d_field, (size_t)kTimeBlock * h->n_pad));
+  QG_TRY(dalloc(h, &h->d_tile_done, (size_t)h->nT));
   QG_TRY(dalloc(h, &h->d_scratch, (size_t)h->n_pad * 8));
   h->traj_k = traj_steps(n);
   QG_TRY(dalloc(h, &h->d_traj, (size_t)2 * h->traj_k * n * 2));
@@ -672,7 +686,7 @@ static void enqueue_dot_step(qg_handle *h, bool traj)
   StepArgs a = h->step_args(!h->fused);
   if(traj) a.traj = h->d_traj;
   if(h->fused) {
-    launch_step_fused(a, h->step_blocks, h->stream);
+    launch_step_fused(a, h->step_blocks, h->step_bs, h->stream);
   } else {
     for(int ph = 0; ph <= kCorrectorSteps + 1; ++ph) launch_step_general(a, ph, h->stream);
   }
@@ -904,14 +918,14 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
 {
   if(!p || !bytes || n < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_footprint: bad argument");
   const int nT = (n + kTile - 1) / kTile, n_pad = nT * kTile;
-  const long long nblk = (long long)nT * (nT + 1) / 2;
+  const int nG = (nT + kTileGroup - 1) / kTileGroup;
   const int q = p->interpolation_order;
   const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
   const int W = ring_depth(md, q);
-  size_t b = table_bytes(nblk, q);
+  size_t b = table_bytes(nT, q);
   b += sizeof(double2) * (size_t)n_pad * (W + kRingMirror);
   b += sizeof(double2) * (size_t)kPcDepth * 4 * n_pad;
-  b += sizeof(double2) * (size_t)kTimeBlock * nT * n_pad;
+  b += sizeof(double2) * (size_t)kTimeBlock * (nG + 1) * n_pad + sizeof(unsigned) * nT;
   b += sizeof(double2) * (size_t)n_pad * 8;
   b += sizeof(double) * (size_t)n_pad * 9 + sizeof(int) * (size_t)n_pad * 2;
   const long long K = traj_steps(n);

@@ -13,20 +13,20 @@
 // d < K (a few per thousand at the benchmark sizes) are summed per step by
 // the dot-step kernel from a compact list.
 //
-// Per pair and direction the K steps read one window of K + q consecutive
-// history samples, held in registers, and form a K-output, (q+1)-tap
-// convolution with the pair's coefficients: 2 K (q+1) complex
-// multiply-adds per pair per pass, each coefficient read from HBM once per K
-// steps.
+// Per ordered pair the K steps read one window of K + q consecutive history
+// samples of the source and form a K-output, (q+1)-tap convolution with the
+// pair's coefficients: K (q+1) complex multiply-adds per ordered pair per
+// pass, each coefficient read from HBM once per K steps.  The window is
+// consumed one sample at a time (each sample feeds up to q+1 outputs), so
+// only the K accumulators and the q+1 coefficients stay in registers.
 //
-// Schedule.  One warp owns one 32 x 32 tile block (I, J) and walks it in 32
-// diagonal steps: at step j lane l takes the pair (a = 32 I + l,
-// b = 32 J + (l + j) mod 32).  The row sums (field of a) stay in lane l's
-// registers; the column sums (field of b) move one lane down after every
-// step, so after 32 steps lane l holds the complete column l.  No reduction
-// trees, no atomics: each (dot, partner tile, step) partial is written once,
-// and the dot-step kernel adds the partials in a fixed order, so results are
-// deterministic.
+// Schedule.  One warp owns a target tile I (lane l = dot 32 I + l) and a
+// group of kTileGroup source tiles.  At each step all 32 lanes take the same
+// source b, so their windows, at the 32 different delays d(a_l, b), fall in
+// one short stretch of b's history row: a handful of cache lines per load
+// instead of 32.  The sums over the group are written as partials; the last
+// warp of a target tile (completion counter) adds the nG partials in a fixed
+// order, so the result does not depend on scheduling.
 //
 // The rho01 ring holds rho01 by time slot (slot = t mod W) with the first
 // kRingMirror slots repeated after slot W-1, so every window is contiguous.
@@ -38,15 +38,6 @@
 #include "qg_internal.h"
 
 namespace qg {
-
-__device__ __forceinline__ void decode_block_f(long long blk, int &I, int &J)
-{
-  long long r = (long long)((sqrt(8.0 * (double)blk + 1.0) - 1.0) * 0.5);
-  while(r * (r + 1) / 2 > blk) --r;
-  while((r + 1) * (r + 2) / 2 <= blk) ++r;
-  I = (int)r;
-  J = (int)(blk - r * (r + 1) / 2);
-}
 
 __device__ __forceinline__ void cfma(double2 &acc, double2 c, double2 r)
 {
@@ -63,26 +54,29 @@ __device__ __forceinline__ double2 ring_pref(const double2 *p)
   return LAB ? make_double2(2 * r.x, 0.0) : r;
 }
 
+// acc[k] += sum_i c[i] * w[k + Q - i] over the window w[m] = ring[slot0 + m],
+// m = 0 .. K+Q-1, whose first sample is step tau0.  Samples before step -22
+// are skipped (their taps are skipped by the reference).
 template <int Q, bool LAB>
-__device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int tau0, bool full,
+__device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int tau0,
                                             const double2 (&c)[Q + 1], double2 (&acc)[kTimeBlock])
 {
   constexpr int K = kTimeBlock;
-  double2 w[K + Q];
+  if(tau0 >= -kWindow) {
 #pragma unroll
-  for(int m = 0; m < K + Q; ++m) w[m] = ring_pref<LAB>(ring + slot0 + m);
-  if(full) {
+    for(int m = 0; m < K + Q; ++m) {
+      const double2 w = ring_pref<LAB>(ring + slot0 + m);
 #pragma unroll
-    for(int k = 0; k < K; ++k)
-#pragma unroll
-      for(int i = 0; i <= Q; ++i) cfma(acc[k], c[i], w[k + Q - i]);
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfma(acc[k], c[k + Q - m], w);
+    }
   } else {
-    // early steps: taps before step -22 are skipped, as the reference does
 #pragma unroll
-    for(int k = 0; k < K; ++k)
+    for(int m = 0; m < K + Q; ++m) {
+      if(tau0 + m < -kWindow) continue;
+      const double2 w = ring_pref<LAB>(ring + slot0 + m);
 #pragma unroll
-      for(int i = 0; i <= Q; ++i)
-        if(tau0 + k + Q - i >= -kWindow) cfma(acc[k], c[i], w[k + Q - i]);
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfma(acc[k], c[k + Q - m], w);
+    }
   }
 }
 
@@ -91,72 +85,78 @@ __global__ void __launch_bounds__(128) far_kernel(FarArgs a)
 {
   constexpr int K = kTimeBlock;
   const int lane = threadIdx.x & 31;
-  const long long blk = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
-  if(blk >= a.nblk) return;  // uniform per warp
-  int I, J;
-  decode_block_f(blk, I, J);
+  const int task = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if(task >= a.nT * a.nG) return;  // uniform per warp
+  const int I = task / a.nG, g = task % a.nG;
+  const int J0 = g * kTileGroup;
+  const int nJ = min(kTileGroup, a.nT - J0);
   const int t0 = *a.d_t0;
-  if(blk == 0 && lane == 0) *a.far_t0_out = t0;
+  if(task == 0 && lane == 0) *a.far_t0_out = t0;
   const int W = a.W;
   const int ia = I * kTile + lane;
-  const double2 *ring_a = a.ring + (long long)ia * a.stride;
-  const int *bd = a.delay + blk * kTilePairs;
-  const double2 *bc = a.coef + blk * (long long)(Q + 1) * kTilePairs;
 
-  double2 racc[K], cacc[K];
+  double2 acc[K];
 #pragma unroll
-  for(int k = 0; k < K; ++k) racc[k] = cacc[k] = make_double2(0.0, 0.0);
+  for(int k = 0; k < K; ++k) acc[k] = make_double2(0.0, 0.0);
 
-  int dn = __ldg(bd + lane);
+  const long long tile0 = (long long)I * a.nT + J0;
+  const int iters = nJ * kTile;
+  // software prefetch of the next source's delay and coefficients
+  int dn = __ldg(a.delay + tile0 * kTilePairs + lane);
   double2 cn[Q + 1];
 #pragma unroll
-  for(int i = 0; i <= Q; ++i) cn[i] = __ldg(bc + i * kTilePairs + lane);
-
-  for(int j = 0; j < kTile; ++j) {
+  for(int i = 0; i <= Q; ++i) cn[i] = __ldg(a.coef + (tile0 * (Q + 1) + i) * kTilePairs + lane);
+  for(int it = 0; it < iters; ++it) {
     const int d = dn;
     double2 c[Q + 1];
 #pragma unroll
     for(int i = 0; i <= Q; ++i) c[i] = cn[i];
-    if(j + 1 < kTile) {
-      const int e = (j + 1) * kTile + lane;
-      dn = __ldg(bd + e);
+    if(it + 1 < iters) {
+      const long long tile = tile0 + (it + 1) / kTile;
+      const int e = ((it + 1) % kTile) * kTile + lane;
+      dn = __ldg(a.delay + tile * kTilePairs + e);
 #pragma unroll
-      for(int i = 0; i <= Q; ++i) cn[i] = __ldg(bc + i * kTilePairs + e);
+      for(int i = 0; i <= Q; ++i) cn[i] = __ldg(a.coef + (tile * (Q + 1) + i) * kTilePairs + e);
     }
     if(d >= K) {
-      const int ib = J * kTile + ((lane + j) & (kTile - 1));
+      const int ib = (J0 + it / kTile) * kTile + (it % kTile);
       const int tau0 = t0 - d - Q;
       int slot0 = tau0 % W;
       if(slot0 < 0) slot0 += W;
-      const bool full = tau0 >= -kWindow;
-      window_conv<Q, LAB>(a.ring + (long long)ib * a.stride, slot0, tau0, full, c, racc);
-      window_conv<Q, LAB>(ring_a, slot0, tau0, full, c, cacc);
-    }
-    const int src = (lane + 1) & (kTile - 1);
-#pragma unroll
-    for(int k = 0; k < K; ++k) {
-      cacc[k].x = __shfl_sync(0xffffffffu, cacc[k].x, src);
-      cacc[k].y = __shfl_sync(0xffffffffu, cacc[k].y, src);
+      window_conv<Q, LAB>(a.ring + (long long)ib * a.stride, slot0, tau0, c, acc);
     }
   }
 
-  const long long slice = (long long)a.nT * a.n_pad;
+  const long long gslice = (long long)a.nG * a.n_pad;
 #pragma unroll
-  for(int k = 0; k < K; ++k) {
-    double2 *P = a.partial + k * slice;
-    if(I == J) {
-      P[(long long)I * a.n_pad + ia] = make_double2(racc[k].x + cacc[k].x, racc[k].y + cacc[k].y);
-    } else {
-      P[(long long)J * a.n_pad + ia] = racc[k];
-      P[(long long)I * a.n_pad + J * kTile + lane] = cacc[k];
+  for(int k = 0; k < K; ++k) a.partial[k * gslice + (long long)g * a.n_pad + ia] = acc[k];
+
+  // the last warp of this target tile adds the nG partials in order
+  __threadfence();
+  unsigned prev = 0;
+  if(lane == 0) prev = atomicAdd(a.tile_done + I, 1u);
+  prev = __shfl_sync(0xffffffffu, prev, 0);
+  if(prev == (unsigned)(a.nG - 1)) {
+    __threadfence();
+#pragma unroll 1
+    for(int k = 0; k < K; ++k) {
+      double2 f = make_double2(0.0, 0.0);
+      const double2 *P = a.partial + k * gslice + ia;
+      for(int gg = 0; gg < a.nG; ++gg) {
+        const double2 v = __ldcg(P + (long long)gg * a.n_pad);
+        f.x += v.x;
+        f.y += v.y;
+      }
+      a.field[(long long)k * a.n_pad + ia] = f;
     }
+    if(lane == 0) a.tile_done[I] = 0;
   }
 }
 
 template <bool LAB>
 static void launch_far_frame(const FarArgs &a, cudaStream_t s)
 {
-  const unsigned blocks = (unsigned)((a.nblk + 3) / 4);
+  const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
   switch(a.q) {
     case 1: far_kernel<1, LAB><<<blocks, 128, 0, s>>>(a); break;
     case 2: far_kernel<2, LAB><<<blocks, 128, 0, s>>>(a); break;
@@ -171,7 +171,7 @@ static void launch_far_frame(const FarArgs &a, cudaStream_t s)
 
 void launch_far(const FarArgs &a, void *stream)
 {
-  if(a.nblk <= 0) return;
+  if(a.nT <= 0) return;
   if(a.frame == 0)
     launch_far_frame<false>(a, (cudaStream_t)stream);
   else

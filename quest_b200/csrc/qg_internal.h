@@ -16,10 +16,11 @@ namespace qg {
 constexpr int kWindow = 22;      // History's negative-time extent (main.cpp:30)
 constexpr int kCorrectorSteps = 10;  // NUM_CORRECTOR_STEPS (integrator.cpp:3)
 constexpr int kMaxOrder = 7;     // largest interpolation order built
-constexpr int kTimeBlock = 8;    // K: steps per pass of the far-pair kernel
-constexpr int kRingMirror = 16;  // slots mirrored past the ring end (>= K+q)
-constexpr int kTile = 32;        // dots per table tile (one warp per tile pair)
+constexpr int kTimeBlock = 16;   // K: steps per pass of the far-pair kernel
+constexpr int kRingMirror = 24;  // slots mirrored past the ring end (>= K+q)
+constexpr int kTile = 32;        // dots per table tile (a warp's 32 targets)
 constexpr int kTilePairs = kTile * kTile;
+constexpr int kTileGroup = 4;    // source tiles one warp sums before writing
 constexpr int kPcDepth = 23;     // PC ring: 22 past steps + the current one
 constexpr int kStepBlock = 128;  // threads per block of the dot-step kernel
 constexpr int kBadNone = 0x7fffffff;
@@ -52,8 +53,8 @@ struct TableArgs {
   const int *user;     // internal -> user index, -1 for padding
   int n, n_pad, nT;
   long long nblk;
-  int *delay;          // [nblk][kTilePairs]
-  double2 *coef;       // [nblk][q+1][kTilePairs]
+  int *delay;          // [nT][nT][kTilePairs]
+  double2 *coef;       // [nT][nT][q+1][kTilePairs]
   int *max_delay;      // atomicMax
   unsigned long long *near_count;  // [0] pairs with delay 0, [1] pairs with delay < K
   CoefParams cp;
@@ -62,12 +63,13 @@ struct TableArgs {
 // Arguments of the far-pair kernel: K steps of the pair sum for every pair
 // with floor delay >= K, from one pass over the table.
 struct FarArgs {
-  const int *delay;
-  const double2 *coef;
+  const int *delay;     // [nT][nT][kTilePairs] ordered tile pairs
+  const double2 *coef;  // [nT][nT][q+1][kTilePairs]
   const double2 *ring;  // [n_pad][stride]: rho01 by time slot
-  double2 *partial;     // [K][nT][n_pad]
-  int n_pad, nT, W, stride, q, frame;
-  long long nblk;
+  double2 *partial;     // [K][nG][n_pad] per source-tile group
+  double2 *field;       // [K][n_pad] far-pair field
+  unsigned *tile_done;  // [nT] completion counters (zero between launches)
+  int n_pad, nT, nG, W, stride, q, frame;
   const int *d_t0;      // first step of the block
   int *far_t0_out;      // receives *d_t0 (read by the dot-step kernels)
 };
@@ -82,8 +84,8 @@ struct StepArgs {
   const double *freq, *t1, *t2;
   const int *slot_dot;   // slot -> internal index (-1 empty)
   const int *user;       // internal -> user
-  const double2 *partial;  // [K][nT][n_pad] far-pair sums
-  const int *far_t0;     // first step of the far block partial[] holds
+  const double2 *far_field;  // [K][n_pad] far-pair field of the current block
+  const int *far_t0;     // first step of the far block far_field holds
   // pairs with floor delay < K (taps not covered by the far kernel): CSR by
   // internal index, partner, delay and q+1 coefficients
   const int *mid_ptr;
@@ -108,11 +110,11 @@ struct StepArgs {
 
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);
-void launch_mid_extract(const int *delay, const double2 *coef, long long nblk, int q,
+void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q,
                         int *out_pairs /*[cap][3] internal a, b, delay*/, double2 *out_coef,
                         unsigned long long *counter, unsigned long long cap, void *stream);
 void launch_far(const FarArgs &a, void *stream);
-void launch_step_fused(const StepArgs &a, int nblocks, void *stream);
+void launch_step_fused(const StepArgs &a, int nblocks, int block_size, void *stream);
 void launch_step_general(const StepArgs &a, int phase, void *stream);
 void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream);
 void launch_pulse_field(const StepArgs &a, int step, double2 *out_user, void *stream);

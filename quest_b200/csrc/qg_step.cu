@@ -79,14 +79,17 @@ __device__ __forceinline__ double pulse_rabi(const StepArgs &a, int idx, int t)
 }
 
 // Predictor value P and corrector base H (the history part of the
-// corrector sum) from the 22-step window.
+// corrector sum) from the n_time-step window (NT > 0: compile-time width,
+// loop unrolled so the window's loads are all in flight together).
+template <int NT>
 __device__ __forceinline__ void pc_window(const StepArgs &a, int idx, int t, double2 (&P)[2],
                                           double2 (&H)[2])
 {
   P[0] = P[1] = H[0] = H[1] = make_double2(0.0, 0.0);
-  const int nt = a.w.n_time;
+  const int nt = NT > 0 ? NT : a.w.n_time;
   const double dt = a.dt;
-  for(int h = 0; h < nt; ++h) {
+#pragma unroll
+  for(int h = 0; h < (NT > 0 ? NT : a.w.n_time); ++h) {
     const int s = pc_slot(t - nt + h);
     const double2 *base = a.pcr + (long long)s * 4 * a.n_pad + idx;
     const double2 x0 = base[0], x1 = base[a.n_pad], y0 = base[2 * a.n_pad], y1 = base[3 * a.n_pad];
@@ -106,23 +109,17 @@ __device__ __forceinline__ void pc_window(const StepArgs &a, int idx, int t, dou
 __device__ __forceinline__ int ring_slot(int t, int W) { return ((t % W) + W) % W; }
 
 // Field at step t from every tap that reads a step before t: the far-pair
-// partials of this step's slice, then the mid-list pairs (delay < K), taps
+// field of this step's slice, then the mid-list pairs (delay < K), taps
 // before step -22 skipped and the (delay 0, tap 0) term left to the near list.
 __device__ __forceinline__ double2 past_field(const StepArgs &a, int idx, int t)
 {
-  double2 f = make_double2(0.0, 0.0);
   const int slice = t - *a.far_t0;
   if(slice < 0 || slice >= kTimeBlock) {
     // the host did not run the far kernel for this block: flag, do not read
     atomicMin(a.d_bad, -1);
     return make_double2(nan(""), nan(""));
   }
-  const double2 *P = a.partial + (long long)slice * a.nT * a.n_pad + idx;
-  for(int k = 0; k < a.nT; ++k) {
-    const double2 v = P[(long long)k * a.n_pad];
-    f.x += v.x;
-    f.y += v.y;
-  }
+  double2 f = a.far_field[(long long)slice * a.n_pad + idx];
   const int q = a.q;
   for(int e = a.mid_ptr[idx]; e < a.mid_ptr[idx + 1]; ++e) {
     const int b = a.mid_idx[e];
@@ -196,20 +193,21 @@ __device__ __forceinline__ void advance_step(const StepArgs &a, int t)
   }
 }
 
-__global__ void __launch_bounds__(kStepBlock) step_fused_kernel(StepArgs a)
+template <int BS, int NT>
+__global__ void __launch_bounds__(BS) step_fused_kernel(StepArgs a)
 {
-  __shared__ double2 cur[kStepBlock];
-  const int slot = blockIdx.x * kStepBlock + threadIdx.x;
+  __shared__ double2 cur[BS];
+  const int slot = blockIdx.x * BS + threadIdx.x;
   const int idx = a.slot_dot[slot];
   const int t = *a.d_step;
   const bool live = idx >= 0;
-  const int nb0 = a.near_ptr[blockIdx.x * kStepBlock];
-  const bool block_near = a.near_ptr[(blockIdx.x + 1) * kStepBlock] > nb0;
+  const int nb0 = a.near_ptr[blockIdx.x * BS];
+  const bool block_near = a.near_ptr[(blockIdx.x + 1) * BS] > nb0;
 
   double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
   double det = 0, t1 = 1, t2 = 1, pul = 0;
   if(live) {
-    pc_window(a, idx, t, P, H);
+    pc_window<NT>(a, idx, t, P, H);
     past = past_field(a, idx, t);
     pul = pulse_rabi(a, idx, t);
     det = a.laser_freq - a.freq[idx];
@@ -255,7 +253,10 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
   if(phase == 0) {
     if(live) {
       double2 P[2], H[2];
-      pc_window(a, idx, t, P, H);
+      if(a.w.n_time == 22)
+        pc_window<22>(a, idx, t, P, H);
+      else
+        pc_window<0>(a, idx, t, P, H);
       sc[0] = past_field(a, idx, t);
       sc[1] = make_double2(pulse_rabi(a, idx, t), 0.0);
       sc[2] = H[0];
@@ -293,9 +294,21 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
   if(it == kCorrectorSteps) advance_step(a, t);
 }
 
-void launch_step_fused(const StepArgs &a, int nblocks, void *stream)
+void launch_step_fused(const StepArgs &a, int nblocks, int block_size, void *stream)
 {
-  step_fused_kernel<<<nblocks, kStepBlock, 0, (cudaStream_t)stream>>>(a);
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool w22 = a.w.n_time == 22;
+  if(block_size == 32) {
+    if(w22)
+      step_fused_kernel<32, 22><<<nblocks, 32, 0, s>>>(a);
+    else
+      step_fused_kernel<32, 0><<<nblocks, 32, 0, s>>>(a);
+  } else {
+    if(w22)
+      step_fused_kernel<kStepBlock, 22><<<nblocks, kStepBlock, 0, s>>>(a);
+    else
+      step_fused_kernel<kStepBlock, 0><<<nblocks, kStepBlock, 0, s>>>(a);
+  }
 }
 
 void launch_step_general(const StepArgs &a, int phase, void *stream)

@@ -2,17 +2,18 @@
 // (reference src/interactions/history_interaction.cpp:21-45) as one kernel.
 //
 // Layout in HBM.  Dots are in internal (Morton) order, padded to a multiple
-// of kTile = 32.  The unordered pairs are grouped into tile blocks (I, J),
-// I >= J, numbered blk = I(I+1)/2 + J.  Block blk holds kTilePairs = 1024
-// entries in diagonal-major order: entry e = 32 j + l is the pair of dot
-// a = 32 I + l and dot b = 32 J + ((l + j) mod 32), so at step j of the
-// far-pair kernel lane l of a warp reads entry 32 j + l:
-//   delay[blk][e]          int32 floor delay, -1 when the entry is no pair
-//                          (padding, or b >= a on a diagonal block)
-//   coef [blk][i][e]       double2 coefficient of tap i = 0..q
-// A warp reading one tap of one diagonal is one 512-byte transaction.  Each
-// pair is computed in the reference's own orientation (src = larger user
-// index, obs = smaller) so its rounding is the reference's.
+// of kTile = 32.  The table is stored for ordered tile pairs: tile (I, J)
+// holds the 32 x 32 pairs with target a = 32 I + l and source b = 32 J + j
+// at entry e = 32 j + l, so the 32 lanes of a warp (one per target) read one
+// source's entries as one coalesced transaction:
+//   delay[I][J][e]          int32 floor delay, -1 when the entry is no pair
+//                           (padding, or a == b)
+//   coef [I][J][i][e]       double2 coefficient of tap i = 0..q
+// Every unordered pair is computed once, in the reference's own orientation
+// (src = larger user index, obs = smaller, so its rounding is the
+// reference's), and written to both (I, J) and (J, I).  The two copies
+// double the table's size; in exchange the far-pair kernel reads windows of
+// one source row per warp step instead of 32.
 //
 // Compiled with -fmad=false.
 #include <cuda_runtime.h>
@@ -39,16 +40,22 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   const long long blk = gid / kTilePairs;
   const int e = (int)(gid % kTilePairs);
   int I, J;
-  decode_block(blk, I, J);
-  const int la = e % kTile, lb = (la + e / kTile) % kTile;
+  decode_block(blk, I, J);  // I >= J
+  const int la = e / kTile, lb = e % kTile;
+  if(I == J && la < lb) return;  // written by the (lb, la) thread
   const int ia = I * kTile + la, ib = J * kTile + lb;
-  int *dptr = a.delay + blk * kTilePairs + e;
-  double2 *cptr = a.coef + blk * (long long)(Q + 1) * kTilePairs + e;
-  const bool valid = ia < a.n && ib < a.n && !(I == J && lb >= la);
+  const long long T1 = (long long)I * a.nT + J, T2 = (long long)J * a.nT + I;
+  const int e1 = lb * kTile + la;  // in (I, J): target a, source b
+  const int e2 = la * kTile + lb;  // in (J, I): target b, source a
+  int *d1 = a.delay + T1 * kTilePairs + e1, *d2 = a.delay + T2 * kTilePairs + e2;
+  double2 *c1 = a.coef + T1 * (Q + 1) * kTilePairs + e1;
+  double2 *c2 = a.coef + T2 * (Q + 1) * kTilePairs + e2;
+  const bool valid = ia < a.n && ib < a.n && ia != ib;
   if(!valid) {
-    *dptr = -1;
+    *d1 = -1;
+    *d2 = -1;
 #pragma unroll
-    for(int i = 0; i <= Q; ++i) cptr[(long long)i * kTilePairs] = make_double2(0.0, 0.0);
+    for(int i = 0; i <= Q; ++i) c1[(long long)i * kTilePairs] = c2[(long long)i * kTilePairs] = make_double2(0.0, 0.0);
     return;
   }
   // reference orientation: src = row = larger user index, obs = col
@@ -65,9 +72,10 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   }
   double2 coef[Q + 1];
   const int fd = pair_coef_ref<Q>(ps, po, ds, dob, a.cp, coef);
-  *dptr = fd;
+  *d1 = fd;
+  *d2 = fd;
 #pragma unroll
-  for(int i = 0; i <= Q; ++i) cptr[(long long)i * kTilePairs] = coef[i];
+  for(int i = 0; i <= Q; ++i) c1[(long long)i * kTilePairs] = c2[(long long)i * kTilePairs] = coef[i];
   atomicMax(a.max_delay, fd);
   if(fd == 0) atomicAdd(a.near_count, 1ULL);
   if(fd < kTimeBlock) atomicAdd(a.near_count + 1, 1ULL);
@@ -92,38 +100,39 @@ void launch_table_build(const TableArgs &a, int q, void *stream)
 }
 
 // Compacts the pairs with floor delay < K (the ones the far-pair kernel
-// leaves to the per-step kernels) into (a, b, delay) + q+1 coefficients; the
+// leaves to the per-step kernels) into (a, b, delay) + q+1 coefficients, each
+// unordered pair once (tiles I >= J, and a > b inside a diagonal tile); the
 // host sorts them.
-__global__ void mid_extract_kernel(const int *delay, const double2 *coef, long long nblk, int q,
+__global__ void mid_extract_kernel(const int *delay, const double2 *coef, int nT, int q,
                                    int *out_pairs, double2 *out_coef, unsigned long long *counter,
                                    unsigned long long cap)
 {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if(gid >= nblk * kTilePairs) return;
+  if(gid >= (long long)nT * nT * kTilePairs) return;
+  const long long tile = gid / kTilePairs;
+  const int I = (int)(tile / nT), J = (int)(tile % nT);
+  const int e = (int)(gid % kTilePairs);
+  const int l = e % kTile, j = e / kTile;  // target lane, source index
+  if(I < J || (I == J && l <= j)) return;
   const int d = delay[gid];
   if(d < 0 || d >= kTimeBlock) return;
-  const long long blk = gid / kTilePairs;
-  const int e = (int)(gid % kTilePairs);
-  int I, J;
-  decode_block(blk, I, J);
   const unsigned long long slot = atomicAdd(counter, 1ULL);
   if(slot >= cap) return;
-  const int la = e % kTile, lb = (la + e / kTile) % kTile;
-  out_pairs[3 * slot] = I * kTile + la;
-  out_pairs[3 * slot + 1] = J * kTile + lb;
+  out_pairs[3 * slot] = I * kTile + l;
+  out_pairs[3 * slot + 1] = J * kTile + j;
   out_pairs[3 * slot + 2] = d;
   for(int i = 0; i <= q; ++i)
-    out_coef[slot * (q + 1) + i] = coef[blk * (long long)(q + 1) * kTilePairs + (long long)i * kTilePairs + e];
+    out_coef[slot * (q + 1) + i] = coef[(tile * (q + 1) + i) * kTilePairs + e];
 }
 
-void launch_mid_extract(const int *delay, const double2 *coef, long long nblk, int q, int *out_pairs,
+void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q, int *out_pairs,
                         double2 *out_coef, unsigned long long *counter, unsigned long long cap,
                         void *stream)
 {
-  const long long total = nblk * kTilePairs;
+  const long long total = (long long)nT * nT * kTilePairs;
   const int threads = 256;
   const unsigned blocks = (unsigned)((total + threads - 1) / threads);
-  mid_extract_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(delay, coef, nblk, q, out_pairs,
+  mid_extract_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(delay, coef, nT, q, out_pairs,
                                                                    out_coef, counter, cap);
 }
 
