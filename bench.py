@@ -243,6 +243,7 @@ def run_ours(args, world, rank, local):
         sim.run(args.warmup, record=False)
     except capi.NonFiniteError as e:
         nonfinite = e.step
+    sim.set_option("far_variant", args.far_variant)
     sim.set_option("profile", 1)
     sim.kernel_time(reset=True)
     stream = torch.cuda.ExternalStream(capi.lib().qg_stream(sim.h))
@@ -260,7 +261,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
     barrier(world)
     ms = e0.elapsed_time(e1)
-    pair_ms, launches = sim.kernel_time()
+    pair_ms, launches, step_ms, step_launches = sim.kernel_times()
     sim.close()
     ms_max = max_over_ranks(ms, world)
     value = world * n * n * args.steps / (ms_max / 1e3)
@@ -304,6 +305,8 @@ def run_ours(args, world, rank, local):
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "steps_per_launch": K,
                      "avg_launch_ms": avg_ms, "share_of_timed_region": pair_ms / ms if ms > 0 else None,
+                     "step_kernels_ms_per_step": step_ms / max(step_launches, 1),
+                     "far_variant": args.far_variant,
                      "fp64": {"achieved": fp64_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                               "frac": fp64_tf / fp64_peak, "flops_per_launch": flops,
                               "peak_source": "measured here: best cuBLAS DGEMM 8192^3"}},
@@ -336,6 +339,7 @@ def main():
     ap.add_argument("--cpu-t0", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dipole-scale", type=float, default=1.0)
+    ap.add_argument("--far-variant", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

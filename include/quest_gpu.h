@@ -180,14 +180,17 @@ qg_status qg_get_info(const qg_handle *h, qg_info *info);
 qg_status qg_footprint(int n, const qg_params *params, double side, size_t *bytes);
 
 /* Timing hooks: the handle's cudaStream_t (as void*), and the device time in
- * milliseconds of the pair-sum kernel, accumulated over qg_run calls made
- * while the "profile" option is on. */
+ * milliseconds of the far-pair kernel and of the per-step kernels (each
+ * nullable), accumulated over qg_run calls made while the "profile" option
+ * is on. */
 void *qg_stream(qg_handle *h);
-qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *launches);
+qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_launches,
+                         double *step_ms, int *step_launches);
 
-/* Options: "graph" (1 = replay each step as a CUDA graph, default),
- * "profile" (1 = launch per step with CUDA events around the pair-sum
- * kernel), "reset" (restart the history at step 0, main.cpp:30-36). */
+/* Options: "graph" (1 = replay each K-step block as a CUDA graph, default),
+ * "profile" (1 = launch directly with CUDA events around every kernel),
+ * "far_variant" (0..2: resource shape of the far-pair kernel, same results),
+ * "reset" (restart the history at step 0, main.cpp:30-36). */
 qg_status qg_set_option(qg_handle *h, const char *key, int value);
 
 #ifdef __cplusplus

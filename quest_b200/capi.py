@@ -104,7 +104,7 @@ def lib():
                                    ctypes.POINTER(ctypes.c_size_t)]
         L.qg_stream.argtypes = [vp]
         L.qg_stream.restype = vp
-        L.qg_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip]
+        L.qg_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip, dp, ip]
         L.qg_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         _lib = L
     return _lib
@@ -254,10 +254,15 @@ class Simulation:
         _check(lib().qg_set_option(self.h, key.encode(), int(value)))
 
     def kernel_time(self, reset: bool = False) -> tuple[float, int]:
-        ms = ctypes.c_double()
-        n = ctypes.c_int()
-        _check(lib().qg_kernel_time(self.h, int(reset), ctypes.byref(ms), ctypes.byref(n)))
-        return ms.value, n.value
+        """(far-pair kernel ms, launches) accumulated in profile mode."""
+        return self.kernel_times(reset)[:2]
+
+    def kernel_times(self, reset: bool = False) -> tuple[float, int, float, int]:
+        """(far ms, far launches, per-step kernels ms, step launches)."""
+        ms, n, sms, sn = ctypes.c_double(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().qg_kernel_time(self.h, int(reset), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(sms),
+                                    ctypes.byref(sn)))
+        return ms.value, n.value, sms.value, sn.value
 
 
 def footprint(n: int, constants, side: float, precision=PREC_FP64, coef_mode=COEF_AUTO) -> int:

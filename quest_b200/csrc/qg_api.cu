@@ -95,11 +95,12 @@ struct qg_handle_s {
 
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // K-step block: [traj off, traj on]
   bool use_graph = true;
+  int far_variant = 2;
   bool profile = false;
-  cudaEvent_t ev_a[256], ev_b[256];
+  cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
   bool events_ready = false;
-  double pair_ms = 0;
-  int pair_launches = 0;
+  double pair_ms = 0, step_ms = 0;
+  int pair_launches = 0, step_launches = 0;
   cudaEvent_t ev_chunk[2], ev_copy[2];
 
   FarArgs far_args(const int *d_t0, int *far_t0_out) const
@@ -120,6 +121,7 @@ struct qg_handle_s {
     s.frame = params.frame;
     s.d_t0 = d_t0;
     s.far_t0_out = far_t0_out;
+    s.variant = far_variant;
     return s;
   }
 
@@ -207,6 +209,8 @@ static void destroy_handle(qg_handle *h)
     for(int i = 0; i < 256; ++i) {
       cudaEventDestroy(h->ev_a[i]);
       cudaEventDestroy(h->ev_b[i]);
+      cudaEventDestroy(h->ev_c[i]);
+      cudaEventDestroy(h->ev_d[i]);
     }
     for(int i = 0; i < 2; ++i) {
       cudaEventDestroy(h->ev_chunk[i]);
@@ -304,7 +308,12 @@ static size_t table_bytes(int nT, int q)
   return (size_t)nT * nT * kTilePairs * (sizeof(int) + sizeof(double2) * (q + 1));
 }
 
-static int ring_depth(int max_delay, int q) { return max_delay + q + kTimeBlock + 2; }
+// Even, so every ring row starts 32-byte aligned for paired-sample loads.
+static int ring_depth(int max_delay, int q)
+{
+  const int w = max_delay + q + kTimeBlock + 2;
+  return w + (w & 1);
+}
 
 // Steps per trajectory staging chunk: a multiple of K, about 32 MiB.
 static int traj_steps(int n)
@@ -631,6 +640,8 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   for(int i = 0; i < 256; ++i) {
     QG_CUDA(cudaEventCreate(&h->ev_a[i]));
     QG_CUDA(cudaEventCreate(&h->ev_b[i]));
+    QG_CUDA(cudaEventCreate(&h->ev_c[i]));
+    QG_CUDA(cudaEventCreate(&h->ev_d[i]));
   }
   for(int i = 0; i < 2; ++i) {
     QG_CUDA(cudaEventCreateWithFlags(&h->ev_chunk[i], cudaEventDisableTiming));
@@ -706,23 +717,33 @@ static qg_status ensure_graph(qg_handle *h, int traj)
   return QG_OK;
 }
 
-static qg_status collect_events(qg_handle *h, int nev)
+static qg_status collect_events(qg_handle *h, int nev, int nstep)
 {
-  if(nev == 0) return QG_OK;
-  QG_CUDA(cudaEventSynchronize(h->ev_b[nev - 1]));
-  for(int j = 0; j < nev; ++j) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, h->ev_a[j], h->ev_b[j]);
-    h->pair_ms += ms;
+  if(nev > 0) {
+    QG_CUDA(cudaEventSynchronize(h->ev_b[nev - 1]));
+    for(int j = 0; j < nev; ++j) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, h->ev_a[j], h->ev_b[j]);
+      h->pair_ms += ms;
+    }
+    h->pair_launches += nev;
   }
-  h->pair_launches += nev;
+  if(nstep > 0) {
+    QG_CUDA(cudaEventSynchronize(h->ev_d[nstep - 1]));
+    for(int j = 0; j < nstep; ++j) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, h->ev_c[j], h->ev_d[j]);
+      h->step_ms += ms;
+    }
+    h->step_launches += nstep;
+  }
   return QG_OK;
 }
 
 // Enqueues steps [t, t + count); whole aligned blocks replay the graph.
 static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
 {
-  int nev = 0;
+  int nev = 0, nstep = 0;
   while(count > 0) {
     const int t0 = t - t % kTimeBlock;
     if(t == t0 && count >= kTimeBlock && h->use_graph && !h->profile) {
@@ -736,18 +757,21 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
     if(h->far_block != t0) {
       enqueue_far(h, t0, t == t0, h->profile ? h->ev_a[nev] : nullptr,
                   h->profile ? h->ev_b[nev] : nullptr);
-      if(h->profile && ++nev == 256) {
-        QG_TRY(collect_events(h, nev));
-        nev = 0;
-      }
+      if(h->profile) ++nev;
       h->far_block = t0;
     }
+    if(h->profile) cudaEventRecord(h->ev_c[nstep], h->stream);
     enqueue_dot_step(h, traj);
+    if(h->profile) cudaEventRecord(h->ev_d[nstep++], h->stream);
+    if(h->profile && (nev == 256 || nstep == 256)) {
+      QG_TRY(collect_events(h, nev, nstep));
+      nev = nstep = 0;
+    }
     ++t;
     --count;
   }
   QG_CUDA(cudaGetLastError());
-  if(h->profile) QG_TRY(collect_events(h, nev));
+  if(h->profile) QG_TRY(collect_events(h, nev, nstep));
   return QG_OK;
 }
 
@@ -936,14 +960,17 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
 
 extern "C" void *qg_stream(qg_handle *h) { return h ? (void *)h->stream : nullptr; }
 
-extern "C" qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *launches)
+extern "C" qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_launches,
+                                    double *step_ms, int *step_launches)
 {
   if(!h) return qg_fail(QG_ERR_INVALID_ARG, "qg_kernel_time: NULL handle");
   if(pair_ms) *pair_ms = h->pair_ms;
-  if(launches) *launches = h->pair_launches;
+  if(pair_launches) *pair_launches = h->pair_launches;
+  if(step_ms) *step_ms = h->step_ms;
+  if(step_launches) *step_launches = h->step_launches;
   if(reset) {
-    h->pair_ms = 0;
-    h->pair_launches = 0;
+    h->pair_ms = h->step_ms = 0;
+    h->pair_launches = h->step_launches = 0;
   }
   return QG_OK;
 }
@@ -955,6 +982,14 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
     h->use_graph = value != 0;
   } else if(!std::strcmp(key, "profile")) {
     h->profile = value != 0;
+  } else if(!std::strcmp(key, "far_variant")) {
+    if(value < 0 || value > 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..2");
+    h->far_variant = value;
+    for(auto &g : h->graph)
+      if(g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
   } else if(!std::strcmp(key, "reset")) {
     return reset_state(h);
   } else {

@@ -80,12 +80,47 @@ __device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int 
   }
 }
 
-template <int Q, bool LAB>
-__global__ void __launch_bounds__(128) far_kernel(FarArgs a)
+// Same convolution reading two samples per 32-byte load (ld.global.nc.v4.f64).
+// The window starts at slot0; the loads start at the even slot below it
+// (rows are 32-byte aligned: even stride, even W), PAR = slot0 & 1.
+template <bool LAB>
+__device__ __forceinline__ void ld2(const double2 *p, double2 &x, double2 &y)
+{
+  double a0, a1, a2, a3;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a0), "=d"(a1), "=d"(a2), "=d"(a3) : "l"(p));
+  x = LAB ? make_double2(2 * a0, 0.0) : make_double2(a0, a1);
+  y = LAB ? make_double2(2 * a2, 0.0) : make_double2(a2, a3);
+}
+
+template <int Q, bool LAB, int PAR>
+__device__ __forceinline__ void window_conv2(const double2 *ring, int slot_even, int tau0,
+                                             const double2 (&c)[Q + 1], double2 (&acc)[kTimeBlock])
+{
+  constexpr int K = kTimeBlock;
+  constexpr int NV = (K + Q + PAR + 1) / 2;
+  const bool full = tau0 >= -kWindow;
+#pragma unroll
+  for(int v = 0; v < NV; ++v) {
+    double2 w2[2];
+    ld2<LAB>(ring + slot_even + 2 * v, w2[0], w2[1]);
+#pragma unroll
+    for(int e = 0; e < 2; ++e) {
+      const int m = 2 * v + e - PAR;
+      if(m < 0 || m >= K + Q) continue;
+      if(!full && tau0 + m < -kWindow) continue;
+#pragma unroll
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfma(acc[k], c[k + Q - m], w2[e]);
+    }
+  }
+}
+
+template <int Q, bool LAB, int VEC>
+__device__ __forceinline__ void far_body(const FarArgs &a)
 {
   constexpr int K = kTimeBlock;
   const int lane = threadIdx.x & 31;
   const int task = blockIdx.x * 4 + (threadIdx.x >> 5);
+  static_assert(VEC == 0 || VEC == 1, "VEC");
   if(task >= a.nT * a.nG) return;  // uniform per warp
   const int I = task / a.nG, g = task % a.nG;
   const int J0 = g * kTileGroup;
@@ -123,7 +158,15 @@ __global__ void __launch_bounds__(128) far_kernel(FarArgs a)
       const int tau0 = t0 - d - Q;
       int slot0 = tau0 % W;
       if(slot0 < 0) slot0 += W;
-      window_conv<Q, LAB>(a.ring + (long long)ib * a.stride, slot0, tau0, c, acc);
+      const double2 *row = a.ring + (long long)ib * a.stride;
+      if(VEC) {
+        if(slot0 & 1)
+          window_conv2<Q, LAB, 1>(row, slot0 - 1, tau0, c, acc);
+        else
+          window_conv2<Q, LAB, 0>(row, slot0, tau0, c, acc);
+      } else {
+        window_conv<Q, LAB>(row, slot0, tau0, c, acc);
+      }
     }
   }
 
@@ -153,18 +196,40 @@ __global__ void __launch_bounds__(128) far_kernel(FarArgs a)
   }
 }
 
+// Variants of the same kernel (identical arithmetic and results):
+//   far_kernel      3 blocks of 4 warps per SM, one sample per load
+//   far_kernel_r4   registers capped for 4 blocks per SM
+//   far_kernel_v2   capped, two samples per 32-byte load
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128) far_kernel(FarArgs a) { far_body<Q, LAB, 0>(a); }
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128, 4) far_kernel_r4(FarArgs a) { far_body<Q, LAB, 0>(a); }
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128, 4) far_kernel_v2(FarArgs a) { far_body<Q, LAB, 1>(a); }
+
+template <int Q, bool LAB>
+static void launch_far_q(const FarArgs &a, cudaStream_t s)
+{
+  const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
+  if(a.variant == 1)
+    far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
+  else if(a.variant == 2)
+    far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
+  else
+    far_kernel<Q, LAB><<<blocks, 128, 0, s>>>(a);
+}
+
 template <bool LAB>
 static void launch_far_frame(const FarArgs &a, cudaStream_t s)
 {
-  const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
   switch(a.q) {
-    case 1: far_kernel<1, LAB><<<blocks, 128, 0, s>>>(a); break;
-    case 2: far_kernel<2, LAB><<<blocks, 128, 0, s>>>(a); break;
-    case 3: far_kernel<3, LAB><<<blocks, 128, 0, s>>>(a); break;
-    case 4: far_kernel<4, LAB><<<blocks, 128, 0, s>>>(a); break;
-    case 5: far_kernel<5, LAB><<<blocks, 128, 0, s>>>(a); break;
-    case 6: far_kernel<6, LAB><<<blocks, 128, 0, s>>>(a); break;
-    case 7: far_kernel<7, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 1: launch_far_q<1, LAB>(a, s); break;
+    case 2: launch_far_q<2, LAB>(a, s); break;
+    case 3: launch_far_q<3, LAB>(a, s); break;
+    case 4: launch_far_q<4, LAB>(a, s); break;
+    case 5: launch_far_q<5, LAB>(a, s); break;
+    case 6: launch_far_q<6, LAB>(a, s); break;
+    case 7: launch_far_q<7, LAB>(a, s); break;
     default: break;
   }
 }

@@ -72,6 +72,7 @@ struct FarArgs {
   int n_pad, nT, nG, W, stride, q, frame;
   const int *d_t0;      // first step of the block
   int *far_t0_out;      // receives *d_t0 (read by the dot-step kernels)
+  int variant;          // kernel variant (same results), see qg_far.cu
 };
 
 // Arguments of the per-dot step kernels.

@@ -205,8 +205,10 @@ def test_pulse_evaluate(golden_weights):
     wl = I.plain_small(n=50, steps=10, pulse_delay=0.0)
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         for step in [0, 3, 9]:
-            np.testing.assert_array_equal(sim.pulse_evaluate(step),
-                                          O.pulse_evaluate(wl.dots, wl.pulse, wl.constants, step))
+            # same operations; CUDA's exp and glibc's differ by at most 1 ulp
+            np.testing.assert_allclose(sim.pulse_evaluate(step),
+                                       O.pulse_evaluate(wl.dots, wl.pulse, wl.constants, step),
+                                       rtol=4.5e-16, atol=0)
 
 
 def test_run_in_pieces_equals_one_run(golden_weights):
@@ -235,7 +237,20 @@ def test_graph_and_direct_launches_agree(golden_weights):
         c = sim.run(100)
         ms, launches = sim.kernel_time()
     np.testing.assert_array_equal(a, np.concatenate([b, c]))
-    assert launches == 100 and ms > 0
+    assert launches >= 6 and ms > 0  # one far-kernel launch per 16-step block
+
+
+def test_far_kernel_variants_agree_bitwise(golden_weights):
+    """The far-kernel variants differ only in register budget and load
+    width; their arithmetic, and so their results, are identical."""
+    wl = I.plain_small(n=300, steps=160, pulse_delay=0.06)
+    outs = []
+    for v in (0, 1, 2):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+            sim.set_option("far_variant", v)
+            outs.append(sim.run(160))
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
 
 
 def test_coincident_dots_raise_at_step_zero(golden_weights):
