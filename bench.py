@@ -339,7 +339,7 @@ def main():
     ap.add_argument("--cpu-t0", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dipole-scale", type=float, default=1.0)
-    ap.add_argument("--far-variant", type=int, default=2)
+    ap.add_argument("--far-variant", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

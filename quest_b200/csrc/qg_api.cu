@@ -95,7 +95,7 @@ struct qg_handle_s {
 
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // K-step block: [traj off, traj on]
   bool use_graph = true;
-  int far_variant = 2;
+  int far_variant = 0;
   bool profile = false;
   cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
   bool events_ready = false;
@@ -411,9 +411,10 @@ static qg_status build_lists(qg_handle *h)
   }
   size_t largest = 0;
   for(auto &c : comps) largest = std::max(largest, c.size());
-  h->fused = largest <= (size_t)kStepBlock;
-  // small blocks spread a few thousand dots over more SMs
-  h->step_bs = largest <= 32 ? 32 : kStepBlock;
+  // the fused step kernel holds 32 dots per block; larger groups coupled at
+  // delay 0 take the general (one launch per evaluation) form
+  h->fused = largest <= 32;
+  h->step_bs = 32;
   const size_t BS = (size_t)h->step_bs;
   std::vector<int> slot_dot;
   std::vector<int> fptr(1, 0), fidx;

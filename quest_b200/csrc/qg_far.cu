@@ -137,10 +137,12 @@ __device__ __forceinline__ void far_body(const FarArgs &a)
   const long long tile0 = (long long)I * a.nT + J0;
   const int iters = nJ * kTile;
   // software prefetch of the next source's delay and coefficients
-  int dn = __ldg(a.delay + tile0 * kTilePairs + lane);
+  // the table is streamed once per pass: evict-first loads keep the history
+  // ring and the per-step kernels' data resident in L2
+  int dn = __ldcs(a.delay + tile0 * kTilePairs + lane);
   double2 cn[Q + 1];
 #pragma unroll
-  for(int i = 0; i <= Q; ++i) cn[i] = __ldg(a.coef + (tile0 * (Q + 1) + i) * kTilePairs + lane);
+  for(int i = 0; i <= Q; ++i) cn[i] = __ldcs(a.coef + (tile0 * (Q + 1) + i) * kTilePairs + lane);
   for(int it = 0; it < iters; ++it) {
     const int d = dn;
     double2 c[Q + 1];
@@ -149,9 +151,9 @@ __device__ __forceinline__ void far_body(const FarArgs &a)
     if(it + 1 < iters) {
       const long long tile = tile0 + (it + 1) / kTile;
       const int e = ((it + 1) % kTile) * kTile + lane;
-      dn = __ldg(a.delay + tile * kTilePairs + e);
+      dn = __ldcs(a.delay + tile * kTilePairs + e);
 #pragma unroll
-      for(int i = 0; i <= Q; ++i) cn[i] = __ldg(a.coef + (tile * (Q + 1) + i) * kTilePairs + e);
+      for(int i = 0; i <= Q; ++i) cn[i] = __ldcs(a.coef + (tile * (Q + 1) + i) * kTilePairs + e);
     }
     if(d >= K) {
       const int ib = (J0 + it / kTile) * kTile + (it % kTile);

@@ -193,50 +193,144 @@ __device__ __forceinline__ void advance_step(const StepArgs &a, int t)
   }
 }
 
-template <int BS, int NT>
-__global__ void __launch_bounds__(BS) step_fused_kernel(StepArgs a)
+// The gathers of one step for one dot, split over kParts threads: part p
+// takes predictor/corrector window slots h = p, p + kParts, ... and mid-list
+// entries p, p + kParts, ...; results are combined in part order, so the
+// sums are deterministic.
+constexpr int kParts = 4;
+
+template <int NT>
+__device__ __forceinline__ void prep_part(const StepArgs &a, int idx, int t, int part,
+                                          double2 (&out)[5])
 {
+  double2 P0 = make_double2(0.0, 0.0), P1 = P0, H0 = P0, H1 = P0, M = P0;
+  const int nt = NT > 0 ? NT : a.w.n_time;
+  const double dt = a.dt;
+#pragma unroll
+  for(int h0 = 0; h0 < (NT > 0 ? NT : 32); h0 += kParts) {
+    const int h = h0 + part;
+    if(h < nt) {
+      const int s = pc_slot(t - nt + h);
+      const double2 *base = a.pcr + (long long)s * 4 * a.n_pad + idx;
+      const double2 x0 = base[0], x1 = base[a.n_pad], y0 = base[2 * a.n_pad], y1 = base[3 * a.n_pad];
+      const double p0 = a.w.ps[h], p1 = a.w.ps[nt + h];
+      const double c0 = a.w.cs[h], c1 = a.w.cs[nt + h];
+      P0.x += x0.x * p0 + (y0.x * p1) * dt;
+      P0.y += x0.y * p0 + (y0.y * p1) * dt;
+      P1.x += x1.x * p0 + (y1.x * p1) * dt;
+      P1.y += x1.y * p0 + (y1.y * p1) * dt;
+      H0.x += x0.x * c0 + (y0.x * c1) * dt;
+      H0.y += x0.y * c0 + (y0.y * c1) * dt;
+      H1.x += x1.x * c0 + (y1.x * c1) * dt;
+      H1.y += x1.y * c0 + (y1.y * c1) * dt;
+    }
+  }
+  // mid-list pairs (delay < K): taps before step -22 skipped, the
+  // (delay 0, tap 0) term left to the near list
+  const int q = a.q;
+  for(int e = a.mid_ptr[idx] + part; e < a.mid_ptr[idx + 1]; e += kParts) {
+    const int b = a.mid_idx[e];
+    const int d = a.mid_delay[e];
+    const double2 *c = a.mid_coef + (long long)e * (q + 1);
+    const double2 *ring = a.ring + (long long)b * a.stride;
+    const int s = t - d;
+    const int base = ring_slot(s - q, a.W);  // tap i at base + q - i (mirrored)
+#pragma unroll
+    for(int i = 0; i <= kMaxOrder; ++i) {
+      if(i <= q && s - i >= -kWindow && !(d == 0 && i == 0)) {
+        const double2 v = cmul(prefactor(ring[base + q - i], a.frame), c[i]);
+        M.x += v.x;
+        M.y += v.y;
+      }
+    }
+  }
+  out[0] = P0;
+  out[1] = P1;
+  out[2] = H0;
+  out[3] = H1;
+  out[4] = M;
+}
+
+// Fused step for 32 dots per block and kParts threads per dot: the gathers
+// in parallel, then warp 0 runs predictor, 11 evaluations and 10
+// corrections; dots coupled at delay 0 share the block and exchange their
+// iterates through shared memory after each correction.
+template <int NT>
+__global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a)
+{
+  constexpr int BS = 32;
+  __shared__ double2 red[kParts][5][BS];
   __shared__ double2 cur[BS];
-  const int slot = blockIdx.x * BS + threadIdx.x;
+  const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
+  const int slot = blockIdx.x * BS + lane;
   const int idx = a.slot_dot[slot];
   const int t = *a.d_step;
   const bool live = idx >= 0;
-  const int nb0 = a.near_ptr[blockIdx.x * BS];
-  const bool block_near = a.near_ptr[(blockIdx.x + 1) * BS] > nb0;
 
-  double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
-  double det = 0, t1 = 1, t2 = 1, pul = 0;
   if(live) {
-    pc_window<NT>(a, idx, t, P, H);
-    past = past_field(a, idx, t);
-    pul = pulse_rabi(a, idx, t);
-    det = a.laser_freq - a.freq[idx];
-    t1 = a.t1[idx];
-    t2 = a.t2[idx];
-    r[0] = P[0];
-    r[1] = P[1];
+    double2 out[5];
+    prep_part<NT>(a, idx, t, part, out);
+#pragma unroll
+    for(int k = 0; k < 5; ++k) red[part][k][lane] = out[k];
   }
-  const int e0 = a.near_ptr[slot], e1 = a.near_ptr[slot + 1];
-  for(int it = 0; it <= kCorrectorSteps; ++it) {
-    if(it > 0 && live) corrector(a, dr, H, r);
-    double2 nf = make_double2(0.0, 0.0);
-    if(block_near) {
-      __syncthreads();
-      cur[threadIdx.x] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
-      __syncthreads();
-      for(int e = e0; e < e1; ++e) {
-        const double2 c = a.near_coef[e];
-        const double2 v = cmul(cur[a.near_idx[e]], c);
-        nf.x += v.x;
-        nf.y += v.y;
+  __syncthreads();
+  if(part == 0) {
+    const int nb0 = a.near_ptr[blockIdx.x * BS];
+    const bool block_near = a.near_ptr[(blockIdx.x + 1) * BS] > nb0;
+    double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
+    double det = 0, t1 = 1, t2 = 1, pul = 0;
+    if(live) {
+      double2 sum[5];
+#pragma unroll
+      for(int k = 0; k < 5; ++k) {
+        sum[k] = red[0][k][lane];
+#pragma unroll
+        for(int p = 1; p < kParts; ++p) {
+          sum[k].x += red[p][k][lane].x;
+          sum[k].y += red[p][k][lane].y;
+        }
+      }
+      P[0] = sum[0];
+      P[1] = sum[1];
+      H[0] = sum[2];
+      H[1] = sum[3];
+      const int slice = t - *a.far_t0;
+      if(slice < 0 || slice >= kTimeBlock) {
+        atomicMin(a.d_bad, -1);  // far block not computed: flag, do not read
+        past = make_double2(nan(""), nan(""));
+      } else {
+        past = a.far_field[(long long)slice * a.n_pad + idx];
+        past.x += sum[4].x;
+        past.y += sum[4].y;
+      }
+      pul = pulse_rabi(a, idx, t);
+      det = a.laser_freq - a.freq[idx];
+      t1 = a.t1[idx];
+      t2 = a.t2[idx];
+      r[0] = P[0];
+      r[1] = P[1];
+    }
+    const int e0 = a.near_ptr[slot], e1 = a.near_ptr[slot + 1];
+    for(int it = 0; it <= kCorrectorSteps; ++it) {
+      if(it > 0 && live) corrector(a, dr, H, r);
+      double2 nf = make_double2(0.0, 0.0);
+      if(block_near) {
+        __syncwarp();
+        cur[lane] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
+        __syncwarp();
+        for(int e = e0; e < e1; ++e) {
+          const double2 v = cmul(cur[a.near_idx[e]], a.near_coef[e]);
+          nf.x += v.x;
+          nf.y += v.y;
+        }
+      }
+      if(live) {
+        const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
+        liouville(r[0], r[1], om, t1, t2, det, dr[0], dr[1]);
       }
     }
-    if(live) {
-      const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
-      liouville(r[0], r[1], om, t1, t2, det, dr[0], dr[1]);
-    }
+    if(live) finish_dot(a, idx, t, r, dr);
   }
-  if(live) finish_dot(a, idx, t, r, dr);
   advance_step(a, t);
 }
 
@@ -296,19 +390,12 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
 
 void launch_step_fused(const StepArgs &a, int nblocks, int block_size, void *stream)
 {
+  (void)block_size;  // 32 dots per block
   cudaStream_t s = (cudaStream_t)stream;
-  const bool w22 = a.w.n_time == 22;
-  if(block_size == 32) {
-    if(w22)
-      step_fused_kernel<32, 22><<<nblocks, 32, 0, s>>>(a);
-    else
-      step_fused_kernel<32, 0><<<nblocks, 32, 0, s>>>(a);
-  } else {
-    if(w22)
-      step_fused_kernel<kStepBlock, 22><<<nblocks, kStepBlock, 0, s>>>(a);
-    else
-      step_fused_kernel<kStepBlock, 0><<<nblocks, kStepBlock, 0, s>>>(a);
-  }
+  if(a.w.n_time == 22)
+    step_fused_kernel<22><<<nblocks, 32 * kParts, 0, s>>>(a);
+  else
+    step_fused_kernel<0><<<nblocks, 32 * kParts, 0, s>>>(a);
 }
 
 void launch_step_general(const StepArgs &a, int phase, void *stream)

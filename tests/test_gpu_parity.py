@@ -211,8 +211,16 @@ def test_pulse_evaluate(golden_weights):
                                        rtol=4.5e-16, atol=0)
 
 
+def stable_small(n, steps, pulse_delay):
+    """Order 3: stable over long runs (order 5 overflows a few hundred steps
+    after the pulse), for tests that compare whole runs with each other."""
+    wl = I.plain_small(n=n, steps=steps, pulse_delay=pulse_delay)
+    wl.constants.interpolation_order = 3
+    return wl
+
+
 def test_run_in_pieces_equals_one_run(golden_weights):
-    wl = I.plain_small(n=100, steps=600, pulse_delay=0.1)
+    wl = stable_small(100, 600, 0.1)
     a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         parts = [sim.run(k) for k in (1, 99, 300, 200)]
@@ -221,14 +229,14 @@ def test_run_in_pieces_equals_one_run(golden_weights):
 
 
 def test_deterministic(golden_weights):
-    wl = I.plain_small(n=333, steps=300, pulse_delay=0.1)
+    wl = stable_small(333, 300, 0.1)
     a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     b, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     np.testing.assert_array_equal(a, b)
 
 
 def test_graph_and_direct_launches_agree(golden_weights):
-    wl = I.plain_small(n=100, steps=200, pulse_delay=0.1)
+    wl = stable_small(100, 200, 0.1)
     a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         sim.set_option("graph", 0)
