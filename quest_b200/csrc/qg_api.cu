@@ -59,7 +59,7 @@ struct qg_handle_s {
   size_t bytes = 0;
 
   double *d_pos = nullptr, *d_dip = nullptr, *d_freq = nullptr, *d_t1 = nullptr, *d_t2 = nullptr;
-  int *d_user = nullptr, *d_slot_dot = nullptr;
+  int *d_user = nullptr;
   int *d_delay = nullptr;
   double2 *d_coef = nullptr;
   double2 *d_ring = nullptr;
@@ -85,7 +85,6 @@ struct qg_handle_s {
 
   bool fused = true;
   int step_blocks = 0;
-  int step_bs = kStepBlock;  // threads per block of the fused step kernel
   int max_delay = 0;
   long long near_pairs = 0, mid_pairs = 0;
   int far_block = -0x7fffffff;  // first step of the far block the partials hold
@@ -150,7 +149,6 @@ struct qg_handle_s {
     a.freq = d_freq;
     a.t1 = d_t1;
     a.t2 = d_t2;
-    a.slot_dot = d_slot_dot;
     a.user = d_user;
     a.far_field = d_field;
     a.far_t0 = d_ints + 6;
@@ -167,8 +165,7 @@ struct qg_handle_s {
     a.traj = nullptr;
     a.traj_rows = 2 * traj_k;
     a.traj_t0 = d_ints + 3;
-    a.d_step = d_ints + 0;
-    a.d_done = d_ints + 1;
+    a.d_next = d_ints + 0;
     a.d_bad = d_ints + 2;
     a.w = w;
     return a;
@@ -348,7 +345,7 @@ static qg_status build_lists(qg_handle *h)
   cudaFree(d_pairs);
   cudaFree(d_mc);
   const long long m = h->mid_pairs;
-  const int n = h->n;
+  const int n = h->n_pad;  // internal indices (padding holes have no pairs)
 
   // mid list: both directions, partners in increasing order
   struct MidEntry {
@@ -368,7 +365,7 @@ static qg_status build_lists(qg_handle *h)
       dsu.unite(a, b);
     }
   }
-  std::vector<int> mptr(n + 1, 0), midx, mdel;
+  std::vector<int> mptr(n + 1, 0), midx, mdel;  // n = n_pad here
   std::vector<double2> mcoef;
   midx.reserve(2 * m);
   mdel.reserve(2 * m);
@@ -395,71 +392,34 @@ static qg_status build_lists(qg_handle *h)
     gptr[i + 1] = (int)gidx.size();
   }
 
-  // pack connected delay-0 groups into step blocks (fused form)
-  std::vector<std::vector<int>> comps;
-  {
-    std::vector<int> root_to_comp(n, -1);
-    for(int i = 0; i < n; ++i) {
-      if(adj[i].empty()) continue;
-      const int r = dsu.find(i);
-      if(root_to_comp[r] < 0) {
-        root_to_comp[r] = (int)comps.size();
-        comps.emplace_back();
-      }
-      comps[root_to_comp[r]].push_back(i);
-    }
-  }
-  size_t largest = 0;
-  for(auto &c : comps) largest = std::max(largest, c.size());
-  // the fused step kernel holds 32 dots per block; larger groups coupled at
-  // delay 0 take the general (one launch per evaluation) form
-  h->fused = largest <= 32;
-  h->step_bs = 32;
-  const size_t BS = (size_t)h->step_bs;
-  std::vector<int> slot_dot;
+  // fused form: the dot order already places every delay-0 group inside one
+  // 32-dot block (see order_for_near_groups); partners are addressed by
+  // their position in the block
   std::vector<int> fptr(1, 0), fidx;
   std::vector<double2> fcoef;
+  const int np = h->n_pad;
   if(h->fused) {
-    std::sort(comps.begin(), comps.end(),
-              [](const std::vector<int> &x, const std::vector<int> &y) { return x.size() > y.size(); });
-    std::vector<std::vector<int>> bins;
-    for(auto &c : comps) {
-      size_t b = 0;
-      for(; b < bins.size(); ++b)
-        if(bins[b].size() + c.size() <= BS) break;
-      if(b == bins.size()) bins.emplace_back();
-      bins[b].insert(bins[b].end(), c.begin(), c.end());
-    }
-    size_t fill = 0;
-    for(int i = 0; i < n; ++i) {
-      if(!adj[i].empty()) continue;
-      while(fill < bins.size() && bins[fill].size() >= BS) ++fill;
-      if(fill == bins.size()) bins.emplace_back();
-      bins[fill].push_back(i);
-    }
-    h->step_blocks = (int)bins.size();
-    slot_dot.assign((size_t)h->step_blocks * BS, -1);
-    std::vector<int> local(n, -1);
-    for(size_t b = 0; b < bins.size(); ++b)
-      for(size_t j = 0; j < bins[b].size(); ++j) {
-        slot_dot[b * BS + j] = bins[b][j];
-        local[bins[b][j]] = (int)j;
-      }
-    for(size_t sl = 0; sl < slot_dot.size(); ++sl) {
-      const int i = slot_dot[sl];
-      if(i >= 0)
+    // every delay-0 partner must share the dot's 32-dot block
+    for(int i = 0; i < np && h->fused; ++i)
+      for(auto &e : adj[i])
+        if(e.first / 32 != i / 32) {
+          h->fused = false;
+          break;
+        }
+  }
+  if(h->fused) {
+    for(int i = 0; i < np; ++i) {
+      if(i < n)
         for(auto &e : adj[i]) {
-          fidx.push_back(local[e.first]);
+          fidx.push_back(e.first - (i / 32) * 32);
           fcoef.push_back(e.second);
         }
       fptr.push_back((int)fidx.size());
     }
   } else {
-    h->step_blocks = (n + kStepBlock - 1) / kStepBlock;
-    slot_dot.assign((size_t)h->step_blocks * kStepBlock, -1);
-    for(int i = 0; i < n; ++i) slot_dot[i] = i;
-    fptr.assign(slot_dot.size() + 1, 0);
+    fptr.assign(np + 1, 0);
   }
+  h->step_blocks = np / 32;
 
   auto upload_i = [&](int **dst, const std::vector<int> &v) -> qg_status {
     QG_TRY(dalloc(h, dst, v.size()));
@@ -482,7 +442,6 @@ static qg_status build_lists(qg_handle *h)
   QG_TRY(upload_i(&h->d_fnear_ptr, fptr));
   QG_TRY(upload_i(&h->d_fnear_idx, fidx));
   QG_TRY(upload_c(&h->d_fnear_coef, fcoef));
-  QG_TRY(upload_i(&h->d_slot_dot, slot_dot));
   return QG_OK;
 }
 
@@ -503,6 +462,101 @@ static qg_status reset_state(qg_handle *h)
   return QG_OK;
 }
 
+// Finds the pairs at floor delay 0 (one cheap kernel over all pairs) and
+// chooses the internal dot order: Morton order, with every connected group
+// of delay-0 pairs moved into one 32-dot block so the fused step kernel can
+// iterate the group with warp-level synchronisation only.  Groups larger
+// than 32 dots select the general step form and keep Morton order.
+static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const std::vector<int> &morton,
+                                       std::vector<int> &order)
+{
+  const int n = h->n;
+  const int np0 = ((n + kTile - 1) / kTile) * kTile;
+  std::vector<double> pos((size_t)np0 * 3, 0.0);
+  std::vector<int> user(np0, -1);
+  for(int i = 0; i < n; ++i) {
+    for(int k = 0; k < 3; ++k) pos[3 * i + k] = dots[morton[i]].pos[k];
+    user[i] = morton[i];
+  }
+  double *d_pos = nullptr;
+  int *d_user = nullptr, *d_pairs = nullptr;
+  unsigned long long *d_cnt = nullptr;
+  QG_CUDA(cudaMalloc(&d_pos, sizeof(double) * pos.size()));
+  QG_CUDA(cudaMalloc(&d_user, sizeof(int) * user.size()));
+  QG_CUDA(cudaMalloc(&d_cnt, sizeof(unsigned long long)));
+  QG_CUDA(cudaMemcpy(d_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpy(d_user, user.data(), sizeof(int) * user.size(), cudaMemcpyHostToDevice));
+  const double c0dt = h->params.c0 * h->params.dt;
+  unsigned long long cnt = 0;
+  for(int pass = 0; pass < 2; ++pass) {
+    const unsigned long long cap = pass == 0 ? 0 : std::max<unsigned long long>(cnt, 1);
+    if(pass == 1) QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 2 * cap));
+    QG_CUDA(cudaMemset(d_cnt, 0, sizeof(unsigned long long)));
+    launch_near_find(d_pos, d_user, np0, c0dt, d_pairs, d_cnt, cap, h->stream);
+    QG_CUDA(cudaGetLastError());
+    QG_CUDA(cudaMemcpyAsync(&cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
+    QG_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  std::vector<int> pairs(2 * std::max<unsigned long long>(cnt, 1));
+  if(cnt) QG_CUDA(cudaMemcpy(pairs.data(), d_pairs, sizeof(int) * 2 * cnt, cudaMemcpyDeviceToHost));
+  cudaFree(d_pos);
+  cudaFree(d_user);
+  cudaFree(d_cnt);
+  if(d_pairs) cudaFree(d_pairs);
+
+  // groups over Morton positions
+  DSU dsu(n);
+  std::vector<char> coupled(n, 0);
+  for(unsigned long long k = 0; k < cnt; ++k) {
+    dsu.unite(pairs[2 * k], pairs[2 * k + 1]);
+    coupled[pairs[2 * k]] = coupled[pairs[2 * k + 1]] = 1;
+  }
+  std::vector<std::vector<int>> comps;
+  {
+    std::vector<int> root_to_comp(n, -1);
+    for(int i = 0; i < n; ++i) {
+      if(!coupled[i]) continue;
+      const int r = dsu.find(i);
+      if(root_to_comp[r] < 0) {
+        root_to_comp[r] = (int)comps.size();
+        comps.emplace_back();
+      }
+      comps[root_to_comp[r]].push_back(i);
+    }
+  }
+  size_t largest = 0;
+  for(auto &c : comps) largest = std::max(largest, c.size());
+  h->fused = largest <= 32;
+  order.clear();
+  if(!h->fused || comps.empty()) {
+    for(int i = 0; i < n; ++i) order.push_back(morton[i]);
+    while(order.size() % kTile) order.push_back(-1);
+    return QG_OK;
+  }
+  std::sort(comps.begin(), comps.end(),
+            [](const std::vector<int> &x, const std::vector<int> &y) { return x.size() > y.size(); });
+  std::vector<std::vector<int>> bins;
+  for(auto &c : comps) {
+    size_t b = 0;
+    for(; b < bins.size(); ++b)
+      if(bins[b].size() + c.size() <= 32) break;
+    if(b == bins.size()) bins.emplace_back();
+    bins[b].insert(bins[b].end(), c.begin(), c.end());
+  }
+  size_t fill = 0;
+  for(int i = 0; i < n; ++i) {
+    if(coupled[i]) continue;
+    while(fill < bins.size() && bins[fill].size() >= 32) ++fill;
+    if(fill == bins.size()) bins.emplace_back();
+    bins[fill].push_back(i);
+  }
+  for(auto &b : bins) {
+    for(int i : b) order.push_back(morton[i]);
+    for(size_t j = b.size(); j < 32; ++j) order.push_back(-1);
+  }
+  return QG_OK;
+}
+
 static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, const qg_params *p,
                              const qg_weights *weights, qg_handle *h)
 {
@@ -514,10 +568,6 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   h->T = p->num_timesteps;
   h->params = *p;
   h->pulse = *pulse;
-  h->nT = (n + kTile - 1) / kTile;
-  h->n_pad = h->nT * kTile;
-  h->nG = (h->nT + kTileGroup - 1) / kTileGroup;
-  h->nblk = (long long)h->nT * (h->nT + 1) / 2;
   h->P = (long long)n * (n - 1) / 2;
 
   qg_weights wt;
@@ -538,13 +588,19 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   }
   h->w.fc = wt.future_coef;
 
-  // internal order
-  const std::vector<int> perm = morton_order(dots, n);
+  // internal order: Morton, delay-0 groups packed into 32-dot blocks
+  std::vector<int> order;
+  QG_TRY(order_for_near_groups(h, dots, morton_order(dots, n), order));
+  h->n_pad = (int)order.size();
+  h->nT = h->n_pad / kTile;
+  h->nG = (h->nT + kTileGroup - 1) / kTileGroup;
+  h->nblk = (long long)h->nT * (h->nT + 1) / 2;
   std::vector<double> pos((size_t)h->n_pad * 3, 0.0), dip((size_t)h->n_pad * 3, 0.0);
   std::vector<double> fr(h->n_pad, 0.0), t1(h->n_pad, 1.0), t2(h->n_pad, 1.0);
   std::vector<int> user(h->n_pad, -1);
-  for(int i = 0; i < n; ++i) {
-    const qg_dot &d = dots[perm[i]];
+  for(int i = 0; i < h->n_pad; ++i) {
+    if(order[i] < 0) continue;
+    const qg_dot &d = dots[order[i]];
     for(int k = 0; k < 3; ++k) {
       pos[3 * i + k] = d.pos[k];
       dip[3 * i + k] = d.dip[k];
@@ -552,7 +608,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
     fr[i] = d.freq;
     t1[i] = d.t1;
     t2[i] = d.t2;
-    user[i] = perm[i];
+    user[i] = order[i];
   }
   QG_TRY(dalloc(h, &h->d_pos, pos.size()));
   QG_TRY(dalloc(h, &h->d_dip, dip.size()));
@@ -683,6 +739,8 @@ extern "C" qg_status qg_destroy(qg_handle *h)
 // partial buffer, or when a run starts off a boundary) gets t0 explicitly.
 static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, cudaEvent_t eb)
 {
+  // at a boundary the previous block's last step kernel (or launch_steps)
+  // has stored t0 in d_ints[0]; that read keeps the launch graph-capturable
   const int *src = h->d_ints + 0;
   if(!at_boundary) {
     launch_set_int(h->d_ints + 7, t0, h->stream);
@@ -693,14 +751,14 @@ static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, 
   if(eb) cudaEventRecord(eb, h->stream);
 }
 
-static void enqueue_dot_step(qg_handle *h, bool traj)
+static void enqueue_dot_step(qg_handle *h, int k, bool traj)
 {
   StepArgs a = h->step_args(!h->fused);
   if(traj) a.traj = h->d_traj;
   if(h->fused) {
-    launch_step_fused(a, h->step_blocks, h->step_bs, h->stream);
+    launch_step_fused(a, k, h->step_blocks, h->stream);
   } else {
-    for(int ph = 0; ph <= kCorrectorSteps + 1; ++ph) launch_step_general(a, ph, h->stream);
+    for(int ph = 0; ph <= kCorrectorSteps + 1; ++ph) launch_step_general(a, k, ph, h->stream);
   }
 }
 
@@ -711,7 +769,7 @@ static qg_status ensure_graph(qg_handle *h, int traj)
   cudaGraph_t g;
   QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   enqueue_far(h, 0, true, nullptr, nullptr);
-  for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, traj != 0);
+  for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
   QG_CUDA(cudaStreamEndCapture(h->stream, &g));
   QG_CUDA(cudaGraphInstantiate(&h->graph[traj], g, 0));
   cudaGraphDestroy(g);
@@ -745,6 +803,7 @@ static qg_status collect_events(qg_handle *h, int nev, int nstep)
 static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
 {
   int nev = 0, nstep = 0;
+  if(count > 0 && t % kTimeBlock == 0) launch_set_int(h->d_ints + 0, t, h->stream);
   while(count > 0) {
     const int t0 = t - t % kTimeBlock;
     if(t == t0 && count >= kTimeBlock && h->use_graph && !h->profile) {
@@ -762,7 +821,7 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
       h->far_block = t0;
     }
     if(h->profile) cudaEventRecord(h->ev_c[nstep], h->stream);
-    enqueue_dot_step(h, traj);
+    enqueue_dot_step(h, t - t0, traj);
     if(h->profile) cudaEventRecord(h->ev_d[nstep++], h->stream);
     if(h->profile && (nev == 256 || nstep == 256)) {
       QG_TRY(collect_events(h, nev, nstep));

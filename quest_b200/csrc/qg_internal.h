@@ -83,8 +83,7 @@ struct StepArgs {
   const double *pos;     // [n_pad][3] internal order
   const double *dip;     // [n_pad][3]
   const double *freq, *t1, *t2;
-  const int *slot_dot;   // slot -> internal index (-1 empty)
-  const int *user;       // internal -> user
+  const int *user;       // internal -> user index, -1 for padding
   const double2 *far_field;  // [K][n_pad] far-pair field of the current block
   const int *far_t0;     // first step of the far block far_field holds
   // pairs with floor delay < K (taps not covered by the far kernel): CSR by
@@ -105,7 +104,9 @@ struct StepArgs {
   double2 *traj;         // [k][n][2] user order or null
   int traj_rows;         // rows allocated in traj
   const int *traj_t0;
-  int *d_step, *d_done, *d_bad;
+  int *d_next;           // first step of the next far block (set by the last
+                         // step kernel of a block, read by the far kernel)
+  int *d_bad;
   PCW w;
 };
 
@@ -115,8 +116,10 @@ void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q,
                         int *out_pairs /*[cap][3] internal a, b, delay*/, double2 *out_coef,
                         unsigned long long *counter, unsigned long long cap, void *stream);
 void launch_far(const FarArgs &a, void *stream);
-void launch_step_fused(const StepArgs &a, int nblocks, int block_size, void *stream);
-void launch_step_general(const StepArgs &a, int phase, void *stream);
+void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int *out_pairs,
+                      unsigned long long *counter, unsigned long long cap, void *stream);
+void launch_step_fused(const StepArgs &a, int k, int nblocks, void *stream);
+void launch_step_general(const StepArgs &a, int k, int phase, void *stream);
 void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream);
 void launch_pulse_field(const StepArgs &a, int step, double2 *out_user, void *stream);
 void launch_set_int(int *p, int v, void *stream);

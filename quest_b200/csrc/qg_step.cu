@@ -111,14 +111,8 @@ __device__ __forceinline__ int ring_slot(int t, int W) { return ((t % W) + W) % 
 // Field at step t from every tap that reads a step before t: the far-pair
 // field of this step's slice, then the mid-list pairs (delay < K), taps
 // before step -22 skipped and the (delay 0, tap 0) term left to the near list.
-__device__ __forceinline__ double2 past_field(const StepArgs &a, int idx, int t)
+__device__ __forceinline__ double2 past_field(const StepArgs &a, int idx, int t, int slice)
 {
-  const int slice = t - *a.far_t0;
-  if(slice < 0 || slice >= kTimeBlock) {
-    // the host did not run the far kernel for this block: flag, do not read
-    atomicMin(a.d_bad, -1);
-    return make_double2(nan(""), nan(""));
-  }
   double2 f = a.far_field[(long long)slice * a.n_pad + idx];
   const int q = a.q;
   for(int e = a.mid_ptr[idx]; e < a.mid_ptr[idx + 1]; ++e) {
@@ -179,18 +173,11 @@ __device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, co
   if(!finite4(r[0], r[1]) || !finite4(dr[0], dr[1])) atomicMin(a.d_bad, t);
 }
 
-__device__ __forceinline__ void advance_step(const StepArgs &a, int t)
+// The step index is the far block's first step plus the launch's offset k;
+// the last step of a block tells the next far-kernel launch where it starts.
+__device__ __forceinline__ void publish_next_block(const StepArgs &a, int k, int t)
 {
-  __syncthreads();
-  if(threadIdx.x == 0) {
-    __threadfence();
-    const unsigned prev = atomicAdd((unsigned *)a.d_done, 1u);
-    if(prev == gridDim.x - 1) {
-      *a.d_done = 0;
-      __threadfence();
-      atomicExch(a.d_step, t + 1);
-    }
-  }
+  if(k == kTimeBlock - 1 && blockIdx.x == 0 && threadIdx.x == 0) *a.d_next = t + 1;
 }
 
 // The gathers of one step for one dot, split over kParts threads: part p
@@ -256,53 +243,47 @@ __device__ __forceinline__ void prep_part(const StepArgs &a, int idx, int t, int
 // corrections; dots coupled at delay 0 share the block and exchange their
 // iterates through shared memory after each correction.
 template <int NT>
-__global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a)
+__global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int k)
 {
   constexpr int BS = 32;
   __shared__ double2 red[kParts][5][BS];
   __shared__ double2 cur[BS];
   const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
-  const int slot = blockIdx.x * BS + lane;
-  const int idx = a.slot_dot[slot];
-  const int t = *a.d_step;
-  const bool live = idx >= 0;
+  const int idx = blockIdx.x * BS + lane;
+  const int t = *a.far_t0 + k;
+  const bool live = a.user[idx] >= 0;
 
   if(live) {
     double2 out[5];
     prep_part<NT>(a, idx, t, part, out);
 #pragma unroll
-    for(int k = 0; k < 5; ++k) red[part][k][lane] = out[k];
+    for(int v = 0; v < 5; ++v) red[part][v][lane] = out[v];
   }
   __syncthreads();
   if(part == 0) {
     const int nb0 = a.near_ptr[blockIdx.x * BS];
     const bool block_near = a.near_ptr[(blockIdx.x + 1) * BS] > nb0;
+    const int slot = idx;
     double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
     double det = 0, t1 = 1, t2 = 1, pul = 0;
     if(live) {
       double2 sum[5];
 #pragma unroll
-      for(int k = 0; k < 5; ++k) {
-        sum[k] = red[0][k][lane];
+      for(int v = 0; v < 5; ++v) {
+        sum[v] = red[0][v][lane];
 #pragma unroll
         for(int p = 1; p < kParts; ++p) {
-          sum[k].x += red[p][k][lane].x;
-          sum[k].y += red[p][k][lane].y;
+          sum[v].x += red[p][v][lane].x;
+          sum[v].y += red[p][v][lane].y;
         }
       }
       P[0] = sum[0];
       P[1] = sum[1];
       H[0] = sum[2];
       H[1] = sum[3];
-      const int slice = t - *a.far_t0;
-      if(slice < 0 || slice >= kTimeBlock) {
-        atomicMin(a.d_bad, -1);  // far block not computed: flag, do not read
-        past = make_double2(nan(""), nan(""));
-      } else {
-        past = a.far_field[(long long)slice * a.n_pad + idx];
-        past.x += sum[4].x;
-        past.y += sum[4].y;
-      }
+      past = a.far_field[(long long)k * a.n_pad + idx];
+      past.x += sum[4].x;
+      past.y += sum[4].y;
       pul = pulse_rabi(a, idx, t);
       det = a.laser_freq - a.freq[idx];
       t1 = a.t1[idx];
@@ -331,18 +312,18 @@ __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a)
     }
     if(live) finish_dot(a, idx, t, r, dr);
   }
-  advance_step(a, t);
+  publish_next_block(a, k, t);
 }
 
 // General form, one launch per phase: phase 0 predicts, phases 1..11 are the
 // 11 evaluations (each followed by a correction except the last).
 // scratch[idx*8 + k]: 0 past field, 1 pulse, 2-3 H, 4-5 rho (even
 // iterations), 6-7 rho (odd iterations).
-__global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, int phase)
+__global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, int k, int phase)
 {
   const int idx = blockIdx.x * kStepBlock + threadIdx.x;
-  const int t = *a.d_step;
-  const bool live = idx < a.n;
+  const int t = *a.far_t0 + k;
+  const bool live = idx < a.n_pad && a.user[idx] >= 0;
   double2 *sc = a.scratch + (long long)idx * 8;
   if(phase == 0) {
     if(live) {
@@ -351,7 +332,7 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
         pc_window<22>(a, idx, t, P, H);
       else
         pc_window<0>(a, idx, t, P, H);
-      sc[0] = past_field(a, idx, t);
+      sc[0] = past_field(a, idx, t, k);
       sc[1] = make_double2(pulse_rabi(a, idx, t), 0.0);
       sc[2] = H[0];
       sc[3] = H[1];
@@ -385,23 +366,22 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
       finish_dot(a, idx, t, r, dr);
     }
   }
-  if(it == kCorrectorSteps) advance_step(a, t);
+  if(it == kCorrectorSteps) publish_next_block(a, k, t);
 }
 
-void launch_step_fused(const StepArgs &a, int nblocks, int block_size, void *stream)
+void launch_step_fused(const StepArgs &a, int k, int nblocks, void *stream)
 {
-  (void)block_size;  // 32 dots per block
   cudaStream_t s = (cudaStream_t)stream;
   if(a.w.n_time == 22)
-    step_fused_kernel<22><<<nblocks, 32 * kParts, 0, s>>>(a);
+    step_fused_kernel<22><<<nblocks, 32 * kParts, 0, s>>>(a, k);
   else
-    step_fused_kernel<0><<<nblocks, 32 * kParts, 0, s>>>(a);
+    step_fused_kernel<0><<<nblocks, 32 * kParts, 0, s>>>(a, k);
 }
 
-void launch_step_general(const StepArgs &a, int phase, void *stream)
+void launch_step_general(const StepArgs &a, int k, int phase, void *stream)
 {
-  const int nblocks = (a.n + kStepBlock - 1) / kStepBlock;
-  step_general_kernel<<<nblocks, kStepBlock, 0, (cudaStream_t)stream>>>(a, phase);
+  const int nblocks = (a.n_pad + kStepBlock - 1) / kStepBlock;
+  step_general_kernel<<<nblocks, kStepBlock, 0, (cudaStream_t)stream>>>(a, k, phase);
 }
 
 // HistoryInteraction::evaluate at an explicit step: past partial sums plus
@@ -409,10 +389,10 @@ void launch_step_general(const StepArgs &a, int phase, void *stream)
 __global__ void eval_field_kernel(StepArgs a, const int *d_eval_step, double2 *out)
 {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if(idx >= a.n) return;
+  if(idx >= a.n_pad || a.user[idx] < 0) return;
   const int step = *d_eval_step;
   const int slot = ring_slot(step, a.W);
-  double2 f = past_field(a, idx, step);
+  double2 f = past_field(a, idx, step, 0);
   for(int e = a.near_ptr[idx]; e < a.near_ptr[idx + 1]; ++e) {
     const int b = a.near_idx[e];
     const double2 v = cmul(prefactor(a.ring[(long long)b * a.stride + slot], a.frame), a.near_coef[e]);
@@ -424,19 +404,19 @@ __global__ void eval_field_kernel(StepArgs a, const int *d_eval_step, double2 *o
 
 void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream)
 {
-  eval_field_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, d_eval_step, out_user);
+  eval_field_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, d_eval_step, out_user);
 }
 
 __global__ void pulse_field_kernel(StepArgs a, int step, double2 *out)
 {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if(idx >= a.n) return;
+  if(idx >= a.n_pad || a.user[idx] < 0) return;
   out[a.user[idx]] = make_double2(pulse_rabi(a, idx, step), 0.0);
 }
 
 void launch_pulse_field(const StepArgs &a, int step, double2 *out_user, void *stream)
 {
-  pulse_field_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, step, out_user);
+  pulse_field_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, step, out_user);
 }
 
 __global__ void set_int_kernel(int *p, int v) { *p = v; }
@@ -470,7 +450,7 @@ void launch_init_state(const StepArgs &a, void *stream)
 __global__ void ring_write_kernel(StepArgs a, int t, const double2 *rho01_user)
 {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if(idx >= a.n) return;
+  if(idx >= a.n_pad || a.user[idx] < 0) return;
   const int slot = ((t % a.W) + a.W) % a.W;
   const double2 v = rho01_user[a.user[idx]];
   double2 *ring = a.ring + (long long)idx * a.stride;
@@ -480,20 +460,20 @@ __global__ void ring_write_kernel(StepArgs a, int t, const double2 *rho01_user)
 
 void launch_ring_write(const StepArgs &a, int t, const double2 *rho01_user, void *stream)
 {
-  ring_write_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
+  ring_write_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
 }
 
 __global__ void ring_read_kernel(StepArgs a, int t, double2 *rho01_user)
 {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if(idx >= a.n) return;
+  if(idx >= a.n_pad || a.user[idx] < 0) return;
   const int slot = ((t % a.W) + a.W) % a.W;
   rho01_user[a.user[idx]] = a.ring[(long long)idx * a.stride + slot];
 }
 
 void launch_ring_read(const StepArgs &a, int t, double2 *rho01_user, void *stream)
 {
-  ring_read_kernel<<<(a.n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
+  ring_read_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
 }
 
 }  // namespace qg

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   int *d1 = a.delay + T1 * kTilePairs + e1, *d2 = a.delay + T2 * kTilePairs + e2;
   double2 *c1 = a.coef + T1 * (Q + 1) * kTilePairs + e1;
   double2 *c2 = a.coef + T2 * (Q + 1) * kTilePairs + e2;
-  const bool valid = ia < a.n && ib < a.n && ia != ib;
+  const bool valid = ia != ib && a.user[ia] >= 0 && a.user[ib] >= 0;
   if(!valid) {
     *d1 = -1;
     *d2 = -1;
@@ -134,6 +134,50 @@ void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q, in
   const unsigned blocks = (unsigned)((total + threads - 1) / threads);
   mid_extract_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(delay, coef, nT, q, out_pairs,
                                                                    out_coef, counter, cap);
+}
+
+// Pairs at floor delay 0, found before the table exists so the dot order can
+// put every group coupled at delay 0 inside one 32-dot step block.  The delay
+// is computed with exactly the operations of pair_coef_ref (reference
+// orientation, norm, division, modf), so it agrees with the table.
+__global__ void near_find_kernel(const double *pos, const int *user, int n_pad, double c0dt,
+                                 int *out_pairs, unsigned long long *counter, unsigned long long cap)
+{
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nt = (n_pad + kTile - 1) / kTile;
+  const long long nblk = nt * (nt + 1) / 2;
+  if(gid >= nblk * kTilePairs) return;
+  int I, J;
+  decode_block(gid / kTilePairs, I, J);
+  const int e = (int)(gid % kTilePairs);
+  const int la = e / kTile, lb = e % kTile;
+  if(I == J && la <= lb) return;
+  const int ia = I * kTile + la, ib = J * kTile + lb;
+  if(ia >= n_pad || ib >= n_pad) return;
+  const int ua = user[ia], ub = user[ib];
+  if(ua < 0 || ub < 0) return;
+  const int is = ua > ub ? ia : ib, io = ua > ub ? ib : ia;
+  double dr[3];
+#pragma unroll
+  for(int k = 0; k < 3; ++k) dr[k] = pos[3 * io + k] - pos[3 * is + k];
+  const double nrm = sqrt((dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2]);
+  double idelay;
+  modf(nrm / c0dt, &idelay);
+  if((int)idelay != 0) return;
+  const unsigned long long slot = atomicAdd(counter, 1ULL);
+  if(slot >= cap) return;
+  out_pairs[2 * slot] = ia;
+  out_pairs[2 * slot + 1] = ib;
+}
+
+void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int *out_pairs,
+                      unsigned long long *counter, unsigned long long cap, void *stream)
+{
+  const long long nt = (n_pad + kTile - 1) / kTile;
+  const long long total = nt * (nt + 1) / 2 * kTilePairs;
+  const int threads = 256;
+  near_find_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(
+      pos, user, n_pad, c0dt, out_pairs, counter, cap);
 }
 
 }  // namespace qg
