@@ -188,7 +188,9 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
                          double *step_ms, int *step_launches);
 
 /* Options: "graph" (1 = replay each K-step block as a CUDA graph, default),
- * "profile" (1 = launch directly with CUDA events around every kernel),
+ * "profile" (1 = CUDA events around the far-pair kernel and the step
+ * kernels: event nodes inside the block graphs, or around each launch when
+ * "graph" is 0),
  * "far_variant" (0..2: resource shape of the far-pair kernel, same results),
  * "reset" (restart the history at step 0, main.cpp:30-36). */
 qg_status qg_set_option(qg_handle *h, const char *key, int value);

@@ -93,6 +93,14 @@ struct qg_handle_s {
   int eval_cached = -0x7fffffff;
 
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // K-step block: [traj off, traj on]
+  // profiling in graph mode: kProfRing instances of the block graph, each
+  // with its own events around the far kernel and around the K step kernels;
+  // an instance's times are collected when it is reused, so the stream stays full
+  static constexpr int kProfRing = 8;
+  cudaGraphExec_t gprof[2][kProfRing] = {};
+  cudaEvent_t pev[kProfRing][3];
+  bool pev_ready = false, pending[kProfRing] = {};
+  int prof_next = 0;
   bool use_graph = true;
   int far_variant = 0;
   bool profile = false;
@@ -202,6 +210,12 @@ static void destroy_handle(qg_handle *h)
   if(h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   for(auto &g : h->graph)
     if(g) cudaGraphExecDestroy(g);
+  for(auto &row : h->gprof)
+    for(auto &g : row)
+      if(g) cudaGraphExecDestroy(g);
+  if(h->pev_ready)
+    for(auto &row : h->pev)
+      for(auto &e : row) cudaEventDestroy(e);
   if(h->events_ready) {
     for(int i = 0; i < 256; ++i) {
       cudaEventDestroy(h->ev_a[i]);
@@ -762,17 +776,55 @@ static void enqueue_dot_step(qg_handle *h, int k, bool traj)
   }
 }
 
-// One K-step block starting on a boundary: far kernel + K dot steps.
+// One K-step block starting on a boundary: far kernel + K dot steps
+// (prof >= 0: instance `prof` of the profiling ring, with event nodes).
+static qg_status capture_block(qg_handle *h, int traj, int prof, cudaGraphExec_t *out)
+{
+  cudaGraph_t g;
+  QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_far(h, 0, true, prof >= 0 ? h->pev[prof][0] : nullptr, prof >= 0 ? h->pev[prof][1] : nullptr);
+  for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
+  if(prof >= 0) cudaEventRecord(h->pev[prof][2], h->stream);
+  QG_CUDA(cudaStreamEndCapture(h->stream, &g));
+  QG_CUDA(cudaGraphInstantiate(out, g, 0));
+  cudaGraphDestroy(g);
+  return QG_OK;
+}
+
 static qg_status ensure_graph(qg_handle *h, int traj)
 {
   if(h->graph[traj]) return QG_OK;
-  cudaGraph_t g;
-  QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_far(h, 0, true, nullptr, nullptr);
-  for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
-  QG_CUDA(cudaStreamEndCapture(h->stream, &g));
-  QG_CUDA(cudaGraphInstantiate(&h->graph[traj], g, 0));
-  cudaGraphDestroy(g);
+  return capture_block(h, traj, -1, &h->graph[traj]);
+}
+
+static qg_status collect_prof(qg_handle *h, int i)
+{
+  if(!h->pending[i]) return QG_OK;
+  QG_CUDA(cudaEventSynchronize(h->pev[i][2]));
+  float far = 0, steps = 0;
+  cudaEventElapsedTime(&far, h->pev[i][0], h->pev[i][1]);
+  cudaEventElapsedTime(&steps, h->pev[i][1], h->pev[i][2]);
+  h->pair_ms += far;
+  h->pair_launches += 1;
+  h->step_ms += steps;
+  h->step_launches += kTimeBlock;
+  h->pending[i] = false;
+  return QG_OK;
+}
+
+static qg_status launch_prof_block(qg_handle *h, int traj)
+{
+  if(!h->pev_ready) {
+    for(auto &row : h->pev)
+      for(auto &e : row) QG_CUDA(cudaEventCreate(&e));
+    h->pev_ready = true;
+  }
+  const int i = h->prof_next;
+  h->prof_next = (h->prof_next + 1) % qg_handle_s::kProfRing;
+  QG_TRY(collect_prof(h, i));
+  if(!h->gprof[traj][i]) QG_TRY(capture_block(h, traj, i, &h->gprof[traj][i]));
+  QG_CUDA(cudaGraphLaunch(h->gprof[traj][i], h->stream));
+  h->pending[i] = true;
   return QG_OK;
 }
 
@@ -806,9 +858,13 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
   if(count > 0 && t % kTimeBlock == 0) launch_set_int(h->d_ints + 0, t, h->stream);
   while(count > 0) {
     const int t0 = t - t % kTimeBlock;
-    if(t == t0 && count >= kTimeBlock && h->use_graph && !h->profile) {
-      QG_TRY(ensure_graph(h, traj ? 1 : 0));
-      QG_CUDA(cudaGraphLaunch(h->graph[traj ? 1 : 0], h->stream));
+    if(t == t0 && count >= kTimeBlock && h->use_graph) {
+      if(h->profile) {
+        QG_TRY(launch_prof_block(h, traj ? 1 : 0));
+      } else {
+        QG_TRY(ensure_graph(h, traj ? 1 : 0));
+        QG_CUDA(cudaGraphLaunch(h->graph[traj ? 1 : 0], h->stream));
+      }
       h->far_block = t0;
       t += kTimeBlock;
       count -= kTimeBlock;
@@ -831,7 +887,10 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
     --count;
   }
   QG_CUDA(cudaGetLastError());
-  if(h->profile) QG_TRY(collect_events(h, nev, nstep));
+  if(h->profile) {
+    QG_TRY(collect_events(h, nev, nstep));
+    for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
+  }
   return QG_OK;
 }
 
@@ -1050,6 +1109,13 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
         cudaGraphExecDestroy(g);
         g = nullptr;
       }
+    for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
+    for(auto &row : h->gprof)
+      for(auto &g : row)
+        if(g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
   } else if(!std::strcmp(key, "reset")) {
     return reset_state(h);
   } else {

@@ -180,17 +180,20 @@ __device__ __forceinline__ void publish_next_block(const StepArgs &a, int k, int
   if(k == kTimeBlock - 1 && blockIdx.x == 0 && threadIdx.x == 0) *a.d_next = t + 1;
 }
 
-// The gathers of one step for one dot, split over kParts threads: part p
-// takes predictor/corrector window slots h = p, p + kParts, ... and mid-list
-// entries p, p + kParts, ...; results are combined in part order, so the
-// sums are deterministic.
+// The gathers of one step, split over the 4 warps of a block (32 dots):
+// warp p takes predictor/corrector window slots h = p, p + 4, ... of its
+// lane's dot; the block's mid-list entries (delay < K pairs of all 32 dots)
+// are spread evenly over all 128 threads, each entry's contribution is
+// staged in shared memory and warp 0 adds a dot's entries in list order, so
+// a dot with many close partners does not hold up the block and the sums
+// are deterministic.
 constexpr int kParts = 4;
+constexpr int kMidChunk = 512;  // mid-list entries staged per pass
 
 template <int NT>
-__device__ __forceinline__ void prep_part(const StepArgs &a, int idx, int t, int part,
-                                          double2 (&out)[5])
+__device__ __forceinline__ void pc_part(const StepArgs &a, int idx, int t, int part, double2 (&out)[4])
 {
-  double2 P0 = make_double2(0.0, 0.0), P1 = P0, H0 = P0, H1 = P0, M = P0;
+  double2 P0 = make_double2(0.0, 0.0), P1 = P0, H0 = P0, H1 = P0;
   const int nt = NT > 0 ? NT : a.w.n_time;
   const double dt = a.dt;
 #pragma unroll
@@ -212,64 +215,93 @@ __device__ __forceinline__ void prep_part(const StepArgs &a, int idx, int t, int
       H1.y += x1.y * c0 + (y1.y * c1) * dt;
     }
   }
-  // mid-list pairs (delay < K): taps before step -22 skipped, the
-  // (delay 0, tap 0) term left to the near list
-  const int q = a.q;
-  for(int e = a.mid_ptr[idx] + part; e < a.mid_ptr[idx + 1]; e += kParts) {
-    const int b = a.mid_idx[e];
-    const int d = a.mid_delay[e];
-    const double2 *c = a.mid_coef + (long long)e * (q + 1);
-    const double2 *ring = a.ring + (long long)b * a.stride;
-    const int s = t - d;
-    const int base = ring_slot(s - q, a.W);  // tap i at base + q - i (mirrored)
-#pragma unroll
-    for(int i = 0; i <= kMaxOrder; ++i) {
-      if(i <= q && s - i >= -kWindow && !(d == 0 && i == 0)) {
-        const double2 v = cmul(prefactor(ring[base + q - i], a.frame), c[i]);
-        M.x += v.x;
-        M.y += v.y;
-      }
-    }
-  }
   out[0] = P0;
   out[1] = P1;
   out[2] = H0;
   out[3] = H1;
-  out[4] = M;
 }
 
-// Fused step for 32 dots per block and kParts threads per dot: the gathers
-// in parallel, then warp 0 runs predictor, 11 evaluations and 10
-// corrections; dots coupled at delay 0 share the block and exchange their
-// iterates through shared memory after each correction.
+// One mid-list entry at step t: taps before step -22 skipped, the
+// (delay 0, tap 0) term left to the near list.
+__device__ __forceinline__ double2 mid_entry(const StepArgs &a, int e, int t)
+{
+  const int q = a.q;
+  const int b = a.mid_idx[e];
+  const int d = a.mid_delay[e];
+  const double2 *c = a.mid_coef + (long long)e * (q + 1);
+  const double2 *ring = a.ring + (long long)b * a.stride;
+  const int s = t - d;
+  const int base = ring_slot(s - q, a.W);  // tap i at base + q - i (mirrored)
+  double2 M = make_double2(0.0, 0.0);
+#pragma unroll
+  for(int i = 0; i <= kMaxOrder; ++i) {
+    if(i <= q && s - i >= -kWindow && !(d == 0 && i == 0)) {
+      const double2 v = cmul(prefactor(ring[base + q - i], a.frame), c[i]);
+      M.x += v.x;
+      M.y += v.y;
+    }
+  }
+  return M;
+}
+
+// Fused step for 32 dots per block, 128 threads: the gathers in parallel,
+// then warp 0 runs predictor, 11 evaluations and 10 corrections; dots
+// coupled at delay 0 share the block and exchange their iterates through
+// shared memory after each correction.
 template <int NT>
 __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int k)
 {
   constexpr int BS = 32;
-  __shared__ double2 red[kParts][5][BS];
+  __shared__ double2 red[kParts][4][BS];
+  __shared__ double2 midv[kMidChunk];
   __shared__ double2 cur[BS];
   const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
   const int idx = blockIdx.x * BS + lane;
   const int t = *a.far_t0 + k;
   const bool live = a.user[idx] >= 0;
 
-  if(live) {
-    double2 out[5];
-    prep_part<NT>(a, idx, t, part, out);
-#pragma unroll
-    for(int v = 0; v < 5; ++v) red[part][v][lane] = out[v];
+  // warp 0's per-dot inputs, requested before the gathers complete
+  double2 past = make_double2(0.0, 0.0);
+  double det = 0, t1 = 1, t2 = 1, pul = 0;
+  if(part == 0 && live) {
+    past = a.far_field[(long long)k * a.n_pad + idx];
+    pul = pulse_rabi(a, idx, t);
+    det = a.laser_freq - a.freq[idx];
+    t1 = a.t1[idx];
+    t2 = a.t2[idx];
   }
-  __syncthreads();
+  if(live) {
+    double2 out[4];
+    pc_part<NT>(a, idx, t, part, out);
+#pragma unroll
+    for(int v = 0; v < 4; ++v) red[part][v][lane] = out[v];
+  }
+
+  // mid list of the block's 32 dots: CSR range [E0, E1)
+  const int E0 = a.mid_ptr[blockIdx.x * BS], E1 = a.mid_ptr[blockIdx.x * BS + BS];
+  const int my0 = a.mid_ptr[idx], my1 = a.mid_ptr[idx + 1];
+  double2 M = make_double2(0.0, 0.0);
+  for(int c0 = E0; c0 < E1; c0 += kMidChunk) {
+    const int c1 = min(E1, c0 + kMidChunk);
+    for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_entry(a, e, t);
+    __syncthreads();
+    if(part == 0)
+      for(int e = max(my0, c0); e < min(my1, c1); ++e) {
+        M.x += midv[e - c0].x;
+        M.y += midv[e - c0].y;
+      }
+    __syncthreads();
+  }
+  if(E0 == E1) __syncthreads();  // the window partials are complete
+
   if(part == 0) {
     const int nb0 = a.near_ptr[blockIdx.x * BS];
     const bool block_near = a.near_ptr[(blockIdx.x + 1) * BS] > nb0;
-    const int slot = idx;
-    double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
-    double det = 0, t1 = 1, t2 = 1, pul = 0;
+    double2 P[2], H[2], r[2], dr[2];
     if(live) {
-      double2 sum[5];
+      double2 sum[4];
 #pragma unroll
-      for(int v = 0; v < 5; ++v) {
+      for(int v = 0; v < 4; ++v) {
         sum[v] = red[0][v][lane];
 #pragma unroll
         for(int p = 1; p < kParts; ++p) {
@@ -281,17 +313,12 @@ __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int
       P[1] = sum[1];
       H[0] = sum[2];
       H[1] = sum[3];
-      past = a.far_field[(long long)k * a.n_pad + idx];
-      past.x += sum[4].x;
-      past.y += sum[4].y;
-      pul = pulse_rabi(a, idx, t);
-      det = a.laser_freq - a.freq[idx];
-      t1 = a.t1[idx];
-      t2 = a.t2[idx];
+      past.x += M.x;
+      past.y += M.y;
       r[0] = P[0];
       r[1] = P[1];
     }
-    const int e0 = a.near_ptr[slot], e1 = a.near_ptr[slot + 1];
+    const int e0 = a.near_ptr[idx], e1 = a.near_ptr[idx + 1];
     for(int it = 0; it <= kCorrectorSteps; ++it) {
       if(it > 0 && live) corrector(a, dr, H, r);
       double2 nf = make_double2(0.0, 0.0);

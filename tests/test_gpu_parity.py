@@ -250,10 +250,22 @@ def test_graph_and_direct_launches_agree(golden_weights):
     assert launches >= 6 and ms > 0  # one far-kernel launch per 16-step block
 
 
+def test_profiling_in_graph_mode_changes_nothing(golden_weights):
+    wl = stable_small(200, 200, 0.1)
+    a, _ = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        sim.set_option("profile", 1)
+        b = sim.run(200)
+        far_ms, far_n, step_ms, step_n = sim.kernel_times()
+    np.testing.assert_array_equal(a, b)
+    assert far_n == 200 // 16 and step_n == far_n * 16
+    assert far_ms > 0 and step_ms > 0
+
+
 def test_far_kernel_variants_agree_bitwise(golden_weights):
     """The far-kernel variants differ only in register budget and load
     width; their arithmetic, and so their results, are identical."""
-    wl = I.plain_small(n=300, steps=160, pulse_delay=0.06)
+    wl = stable_small(300, 160, 0.06)
     outs = []
     for v in (0, 1, 2):
         with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
