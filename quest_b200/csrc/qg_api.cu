@@ -760,9 +760,10 @@ static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, 
     launch_set_int(h->d_ints + 7, t0, h->stream);
     src = h->d_ints + 7;
   }
-  if(ea) cudaEventRecord(ea, h->stream);
+  // External: inside a stream capture this becomes an event-record node
+  if(ea) cudaEventRecordWithFlags(ea, h->stream, cudaEventRecordExternal);
   launch_far(h->far_args(src, h->d_ints + 6), h->stream);
-  if(eb) cudaEventRecord(eb, h->stream);
+  if(eb) cudaEventRecordWithFlags(eb, h->stream, cudaEventRecordExternal);
 }
 
 static void enqueue_dot_step(qg_handle *h, int k, bool traj)
@@ -784,7 +785,7 @@ static qg_status capture_block(qg_handle *h, int traj, int prof, cudaGraphExec_t
   QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   enqueue_far(h, 0, true, prof >= 0 ? h->pev[prof][0] : nullptr, prof >= 0 ? h->pev[prof][1] : nullptr);
   for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
-  if(prof >= 0) cudaEventRecord(h->pev[prof][2], h->stream);
+  if(prof >= 0) cudaEventRecordWithFlags(h->pev[prof][2], h->stream, cudaEventRecordExternal);
   QG_CUDA(cudaStreamEndCapture(h->stream, &g));
   QG_CUDA(cudaGraphInstantiate(out, g, 0));
   cudaGraphDestroy(g);
