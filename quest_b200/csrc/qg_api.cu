@@ -751,6 +751,18 @@ extern "C" qg_status qg_destroy(qg_handle *h)
 // boundary it reads t0 from the device step counter (so it can live in a
 // CUDA graph); a block resumed part-way (after qg_history_evaluate reused the
 // partial buffer, or when a run starts off a boundary) gets t0 explicitly.
+// Inside a stream capture an event must be recorded as an external node to
+// be readable after the graph runs; outside a capture that flag is invalid.
+static void record_event(qg_handle *h, cudaEvent_t e)
+{
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(h->stream, &st);
+  if(st == cudaStreamCaptureStatusActive)
+    cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal);
+  else
+    cudaEventRecord(e, h->stream);
+}
+
 static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, cudaEvent_t eb)
 {
   // at a boundary the previous block's last step kernel (or launch_steps)
@@ -760,10 +772,9 @@ static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, 
     launch_set_int(h->d_ints + 7, t0, h->stream);
     src = h->d_ints + 7;
   }
-  // External: inside a stream capture this becomes an event-record node
-  if(ea) cudaEventRecordWithFlags(ea, h->stream, cudaEventRecordExternal);
+  if(ea) record_event(h, ea);
   launch_far(h->far_args(src, h->d_ints + 6), h->stream);
-  if(eb) cudaEventRecordWithFlags(eb, h->stream, cudaEventRecordExternal);
+  if(eb) record_event(h, eb);
 }
 
 static void enqueue_dot_step(qg_handle *h, int k, bool traj)
@@ -785,7 +796,7 @@ static qg_status capture_block(qg_handle *h, int traj, int prof, cudaGraphExec_t
   QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   enqueue_far(h, 0, true, prof >= 0 ? h->pev[prof][0] : nullptr, prof >= 0 ? h->pev[prof][1] : nullptr);
   for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
-  if(prof >= 0) cudaEventRecordWithFlags(h->pev[prof][2], h->stream, cudaEventRecordExternal);
+  if(prof >= 0) record_event(h, h->pev[prof][2]);
   QG_CUDA(cudaStreamEndCapture(h->stream, &g));
   QG_CUDA(cudaGraphInstantiate(out, g, 0));
   cudaGraphDestroy(g);
