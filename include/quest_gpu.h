@@ -143,6 +143,31 @@ qg_status qg_next_step(const qg_handle *h, int *step);
 qg_status qg_history_evaluate(qg_handle *h, int step, const double *rho01_step,
                               double *field_out);
 
+/* HistoryInteraction::evaluate(step) as qg_history_evaluate computes it, for
+ * callers that cannot allocate device memory at the point of the call: code
+ * running inside a global-mode CUDA stream capture (where cudaMalloc is
+ * prohibited), or hosts whose memory pool owns all device memory and must not
+ * see allocations from a library.  It has no counterpart in the reference.
+ *
+ * Inputs and output are device pointers the caller owns: d_rho01_step
+ * (nullable, N complex, user order) first overwrites the history's rho01 at
+ * `step` (the handle's device history, like qg_history_evaluate);
+ * d_field_out receives N complex, user order.  Work is enqueued on `stream`
+ * (a cudaStream_t; NULL = the handle's stream) and the call returns without
+ * waiting; the result is ready when that stream reaches this point.
+ *
+ * The call allocates nothing and copies nothing to or from the host: its
+ * scratch is a fixed 2.2 MB array in the library's device memory, held on
+ * every device that loads the library until the process exits.  It holds at
+ * most 4096 dots (after padding to multiples of 32); larger handles get
+ * QG_ERR_INVALID_ARG.  All calls share that array, so calls whose work
+ * overlaps on the GPU (other streams, other handles on the same device) race
+ * and must be ordered by the caller.  The first call on each device looks
+ * up the array's device address; make that first call before any stream
+ * capture begins. */
+qg_status qg_history_evaluate_noalloc(qg_handle *h, int step, const double *d_rho01_step,
+                                      double *d_field_out, void *stream);
+
 /* PulseInteraction::evaluate(step) (pulse_interaction.cpp:9-20): N complex. */
 qg_status qg_pulse_evaluate(qg_handle *h, int step, double *field_out);
 

@@ -72,7 +72,7 @@ class QgInfo(ctypes.Structure):
 EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_destroy", "qg_run",
            "qg_next_step", "qg_history_evaluate", "qg_pulse_evaluate", "qg_set_history",
            "qg_get_history", "qg_get_info", "qg_footprint", "qg_stream", "qg_kernel_time",
-           "qg_set_option"]
+           "qg_set_option", "qg_history_evaluate_noalloc"]
 
 _lib = None
 
@@ -106,6 +106,7 @@ def lib():
         L.qg_stream.restype = vp
         L.qg_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip, dp, ip]
         L.qg_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.qg_history_evaluate_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp]
         _lib = L
     return _lib
 

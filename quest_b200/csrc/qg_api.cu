@@ -1009,6 +1009,43 @@ extern "C" qg_status qg_history_evaluate(qg_handle *h, int step, const double *r
   return download_io(h, field_out);
 }
 
+extern "C" qg_status qg_history_evaluate_noalloc(qg_handle *h, int step, const double *d_rho01_step,
+                                                 double *d_field_out, void *stream)
+{
+  if(!h || !d_field_out)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_history_evaluate_noalloc: NULL handle or output");
+  if(step < 0 || step >= std::max(h->T, 1))
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_history_evaluate_noalloc: step %d outside [0, %d)", step, h->T);
+  if(h->n_pad > kNoAllocMaxDots)
+    return qg_fail(QG_ERR_INVALID_ARG,
+                   "qg_history_evaluate_noalloc: %d dots (%d padded) exceed the fixed scratch, "
+                   "which holds at most %d padded dots; use qg_history_evaluate",
+                   h->n, h->n_pad, kNoAllocMaxDots);
+  QG_CUDA(cudaSetDevice(h->device));
+  NoAllocScratch sc;
+  QG_TRY(noalloc_scratch(&sc));
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  StepArgs a = h->step_args(true);
+  if(d_rho01_step) {
+    launch_ring_write(a, step, (const double2 *)d_rho01_step, s);
+    h->eval_cached = -0x7fffffff;
+    h->far_block = -0x7fffffff;
+  }
+  // the completion counters must start at zero; the rest is overwritten
+  QG_CUDA(cudaMemsetAsync(sc.tile_done, 0, sc.tile_bytes, s));
+  launch_set_int(sc.ints + 0, step, s);
+  FarArgs fa = h->far_args(sc.ints + 0, sc.ints + 1);
+  fa.partial = sc.partial;
+  fa.field = sc.field;
+  fa.tile_done = sc.tile_done;
+  launch_far_step1(fa, s);
+  a.far_field = sc.field;
+  a.far_t0 = sc.ints + 0;
+  launch_eval_field(a, sc.ints + 0, (double2 *)d_field_out, s);
+  QG_CUDA(cudaGetLastError());
+  return QG_OK;
+}
+
 extern "C" qg_status qg_pulse_evaluate(qg_handle *h, int step, double *field_out)
 {
   if(!h || !field_out) return qg_fail(QG_ERR_INVALID_ARG, "qg_pulse_evaluate: NULL argument");

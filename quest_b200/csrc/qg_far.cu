@@ -35,6 +35,8 @@
 // (green_function.h:23-27).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "qg_internal.h"
 
 namespace qg {
@@ -57,11 +59,10 @@ __device__ __forceinline__ double2 ring_pref(const double2 *p)
 // acc[k] += sum_i c[i] * w[k + Q - i] over the window w[m] = ring[slot0 + m],
 // m = 0 .. K+Q-1, whose first sample is step tau0.  Samples before step -22
 // are skipped (their taps are skipped by the reference).
-template <int Q, bool LAB>
+template <int Q, bool LAB, int K>
 __device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int tau0,
-                                            const double2 (&c)[Q + 1], double2 (&acc)[kTimeBlock])
+                                            const double2 (&c)[Q + 1], double2 (&acc)[K])
 {
-  constexpr int K = kTimeBlock;
   if(tau0 >= -kWindow) {
 #pragma unroll
     for(int m = 0; m < K + Q; ++m) {
@@ -92,11 +93,10 @@ __device__ __forceinline__ void ld2(const double2 *p, double2 &x, double2 &y)
   y = LAB ? make_double2(2 * a2, 0.0) : make_double2(a2, a3);
 }
 
-template <int Q, bool LAB, int PAR>
+template <int Q, bool LAB, int PAR, int K>
 __device__ __forceinline__ void window_conv2(const double2 *ring, int slot_even, int tau0,
-                                             const double2 (&c)[Q + 1], double2 (&acc)[kTimeBlock])
+                                             const double2 (&c)[Q + 1], double2 (&acc)[K])
 {
-  constexpr int K = kTimeBlock;
   constexpr int NV = (K + Q + PAR + 1) / 2;
   const bool full = tau0 >= -kWindow;
 #pragma unroll
@@ -114,10 +114,12 @@ __device__ __forceinline__ void window_conv2(const double2 *ring, int slot_even,
   }
 }
 
-template <int Q, bool LAB, int VEC>
+// K outputs: the first K steps of the block (K = kTimeBlock in the run; 1 for
+// a single-step evaluation).  Pairs with delay < kTimeBlock are left to the
+// mid list in either case.
+template <int Q, bool LAB, int VEC, int K = kTimeBlock>
 __device__ __forceinline__ void far_body(const FarArgs &a)
 {
-  constexpr int K = kTimeBlock;
   const int lane = threadIdx.x & 31;
   const int task = blockIdx.x * 4 + (threadIdx.x >> 5);
   static_assert(VEC == 0 || VEC == 1, "VEC");
@@ -155,7 +157,7 @@ __device__ __forceinline__ void far_body(const FarArgs &a)
 #pragma unroll
       for(int i = 0; i <= Q; ++i) cn[i] = __ldcs(a.coef + (tile * (Q + 1) + i) * kTilePairs + e);
     }
-    if(d >= K) {
+    if(d >= kTimeBlock) {
       const int ib = (J0 + it / kTile) * kTile + (it % kTile);
       const int tau0 = t0 - d - Q;
       int slot0 = tau0 % W;
@@ -163,11 +165,11 @@ __device__ __forceinline__ void far_body(const FarArgs &a)
       const double2 *row = a.ring + (long long)ib * a.stride;
       if(VEC) {
         if(slot0 & 1)
-          window_conv2<Q, LAB, 1>(row, slot0 - 1, tau0, c, acc);
+          window_conv2<Q, LAB, 1, K>(row, slot0 - 1, tau0, c, acc);
         else
-          window_conv2<Q, LAB, 0>(row, slot0, tau0, c, acc);
+          window_conv2<Q, LAB, 0, K>(row, slot0, tau0, c, acc);
       } else {
-        window_conv<Q, LAB>(row, slot0, tau0, c, acc);
+        window_conv<Q, LAB, K>(row, slot0, tau0, c, acc);
       }
     }
   }
@@ -243,6 +245,81 @@ void launch_far(const FarArgs &a, void *stream)
     launch_far_frame<false>(a, (cudaStream_t)stream);
   else
     launch_far_frame<true>(a, (cudaStream_t)stream);
+}
+
+// ---- single-step evaluation without device allocation ----------------------
+// Scratch of qg_history_evaluate_noalloc: one file-scope array, carved into
+// the group partials, the reduced far field, the tile completion counters and
+// two step indices.  Sized for at most kNoAllocMaxDots (padded) dots.
+constexpr size_t kNoAllocPartialBytes = sizeof(double2) * kNoAllocMaxGroups * kNoAllocMaxDots;
+constexpr size_t kNoAllocFieldBytes = sizeof(double2) * kNoAllocMaxDots;
+constexpr size_t kNoAllocTileBytes = 256 * ((sizeof(unsigned) * kNoAllocMaxTiles + 255) / 256);
+constexpr size_t kNoAllocScratchBytes = kNoAllocPartialBytes + kNoAllocFieldBytes + kNoAllocTileBytes + 256;
+static_assert(kNoAllocScratchBytes == kNoAllocScratchTotal, "scratch size");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// symbol is only a stand-in; the address comes from cudaGetSymbolAddress,
+// looked up once per device (the first call on a device does it, so that
+// call must precede any stream capture).
+qg_status noalloc_scratch(NoAllocScratch *out)
+{
+  static std::mutex mu;
+  static void *addr[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) return qg_fail(QG_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  if(dev < 0 || dev >= 64) return qg_fail(QG_ERR_UNSUPPORTED, "device index %d beyond 63", dev);
+  void *p = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if(!addr[dev]) {
+      e = cudaGetSymbolAddress(&addr[dev], g_noalloc_scratch);
+      if(e != cudaSuccess) {
+        addr[dev] = nullptr;
+        return qg_fail(QG_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s",
+                       cudaGetErrorString(e));
+      }
+    }
+    p = addr[dev];
+  }
+  unsigned char *b = (unsigned char *)p;
+  out->partial = (double2 *)b;
+  out->field = (double2 *)(b + kNoAllocPartialBytes);
+  out->tile_done = (unsigned *)(b + kNoAllocPartialBytes + kNoAllocFieldBytes);
+  out->ints = (int *)(b + kNoAllocPartialBytes + kNoAllocFieldBytes + kNoAllocTileBytes);
+  out->tile_bytes = kNoAllocTileBytes;
+  return QG_OK;
+}
+
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128) far_kernel_step1(FarArgs a) { far_body<Q, LAB, 0, 1>(a); }
+
+template <bool LAB>
+static void launch_far1_frame(const FarArgs &a, cudaStream_t s)
+{
+  const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
+  switch(a.q) {
+    case 1: far_kernel_step1<1, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 2: far_kernel_step1<2, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 3: far_kernel_step1<3, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 4: far_kernel_step1<4, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 5: far_kernel_step1<5, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 6: far_kernel_step1<6, LAB><<<blocks, 128, 0, s>>>(a); break;
+    case 7: far_kernel_step1<7, LAB><<<blocks, 128, 0, s>>>(a); break;
+    default: break;
+  }
+}
+
+// The far-pair field of one step (slice 0) into the scratch's field.
+void launch_far_step1(const FarArgs &a, void *stream)
+{
+  if(a.nT <= 0) return;
+  if(a.frame == 0)
+    launch_far1_frame<false>(a, (cudaStream_t)stream);
+  else
+    launch_far1_frame<true>(a, (cudaStream_t)stream);
 }
 
 }  // namespace qg

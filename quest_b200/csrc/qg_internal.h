@@ -110,6 +110,23 @@ struct StepArgs {
   PCW w;
 };
 
+// Scratch of the allocation-free evaluation (qg_history_evaluate_noalloc):
+// a static device array in qg_far.cu, at most kNoAllocMaxDots padded dots.
+constexpr int kNoAllocMaxDots = 4096;
+constexpr int kNoAllocMaxTiles = kNoAllocMaxDots / kTile;
+constexpr int kNoAllocMaxGroups = (kNoAllocMaxTiles + kTileGroup - 1) / kTileGroup;
+constexpr size_t kNoAllocScratchTotal = 16ull * kNoAllocMaxGroups * kNoAllocMaxDots + 16ull * kNoAllocMaxDots +
+                                        256 * ((4ull * kNoAllocMaxTiles + 255) / 256) + 256;
+struct NoAllocScratch {
+  double2 *partial;    // [kNoAllocMaxGroups][n_pad]
+  double2 *field;      // [n_pad]
+  unsigned *tile_done; // [nT]
+  int *ints;           // [0] step, [1] far_t0 written by the kernel
+  size_t tile_bytes;
+};
+qg_status noalloc_scratch(NoAllocScratch *out);
+void launch_far_step1(const FarArgs &a, void *stream);
+
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);
 void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q,
