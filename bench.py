@@ -294,7 +294,7 @@ def run_ours(args, world, rank, local):
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     fp64_tf = flops / (avg_ms / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops()
-    traffic = profile_traffic("far_kernel_fp64_N4096")
+    traffic = profile_traffic("far_kernel_fp64_N4096")  # ncu dram read+write per launch
     line = {
         "metric": "pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
