@@ -327,6 +327,79 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_batched(args, world, rank, local):
+    """The batched workload: independent ensembles, N log-uniform in
+    [64, 4096], side U[0.05, 0.3], E_0 U[1, 30], steps U[2000, 20000],
+    all in one batch (one persistent far-pair launch + 16 step launches per
+    16-step block, replayed as a CUDA graph); finished ensembles are retired
+    as they finish."""
+    import torch
+
+    from quest_b200 import capi, serving
+    torch.cuda.set_device(local)
+    reqs = serving.batched_ensembles(args.ensembles, seed=40 + rank)
+    weights = capi.pc_weights()
+    sims = [capi.Simulation(r.dots, r.pulse, r.constants, weights=weights) for r in reqs]
+    batch = capi.Batch(len(sims))
+    for s in sims:
+        batch.add(s)
+    total = sum(r.pair_updates for r in reqs)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    live = list(zip(reqs, sims))
+    blocks = 0
+    while live:
+        batch.run(args.blocks_per_round)
+        blocks += args.blocks_per_round
+        done = [(r, s) for r, s in live if s.next_step >= r.constants.num_timesteps]
+        for r, s in done:
+            batch.remove(s)
+        live = [(r, s) for r, s in live if s.next_step < r.constants.num_timesteps]
+    torch.cuda.synchronize()
+    wall = max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+    ns = np.array([r.n for r in reqs])
+    line = {"metric": "pair-updates/s", "value": world * total / wall, "unit": "pair-updates/s",
+            "n_gpus": world, "steps": int(blocks * 16), "warmup": 0, "ms_per_step": wall * 1e3 / (blocks * 16),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded ensembles)",
+            "config": {"workload": f"batched_{args.ensembles}_ensembles", "ensembles": args.ensembles,
+                       "N_min": int(ns.min()), "N_max": int(ns.max()), "sum_N2T": total,
+                       "precision": "fp64", "coef_mode": "table"},
+            "wall_s": wall}
+    for s in sims:
+        s.close()
+    batch.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_serving(args, world, rank, local):
+    """The serving workload: Poisson arrivals at --rate requests/s, N
+    log-uniform in [32, --serve-nmax], side U[0.05, 0.5], steps U[1000,
+    20000], admitted under a --budget-gb memory budget; p50/p99
+    time-to-completion and aggregate pair-updates/s."""
+    import torch
+
+    from quest_b200 import capi, serving
+    torch.cuda.set_device(local)
+    reqs = serving.serving_requests(args.requests, args.rate, seed=70 + rank, n_range=(32, args.serve_nmax))
+    srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=capi.pc_weights())
+    barrier(world)
+    stats = srv.serve(reqs)
+    srv.close()
+    stats["pair_updates_per_s"] = max_over_ranks(stats["pair_updates_per_s"], world)
+    line = {"metric": "pair-updates/s", "value": world * stats["pair_updates_per_s"], "unit": "pair-updates/s",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Poisson request stream)",
+            "config": {"workload": "serving", "requests": args.requests, "rate_per_s": args.rate,
+                       "N_max": args.serve_nmax, "budget_gb": args.budget_gb, "precision": "fp64"},
+            "serving": stats}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -340,6 +413,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dipole-scale", type=float, default=1.0)
     ap.add_argument("--far-variant", type=int, default=0)
+    ap.add_argument("--workload", choices=["table", "batched", "serving"], default="table")
+    ap.add_argument("--ensembles", type=int, default=256)
+    ap.add_argument("--blocks-per-round", type=int, default=8)
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--serve-nmax", type=int, default=16384)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -347,6 +427,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "batched":
+            run_batched(args, world, rank, local)
+        elif args.workload == "serving":
+            run_serving(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

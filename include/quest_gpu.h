@@ -183,6 +183,33 @@ qg_status qg_set_history(qg_handle *h, int t0, int n, const double *rho01);
  * complex per step. */
 qg_status qg_get_history(qg_handle *h, int t0, int n, double *rho01_out);
 
+/* Current state: rho (rho00, rho01) of every dot after the last computed
+ * step (main.cpp:34's initial value before any step), 2 complex per dot,
+ * user order. */
+qg_status qg_get_state(qg_handle *h, double *rho_out);
+
+/* First step at which a non-finite value appeared, or -1. */
+qg_status qg_bad_step(qg_handle *h, int *bad_step);
+
+/* Batches: many independent ensembles (handles) advanced together, one
+ * persistent far-pair launch and one step launch per step for all of them,
+ * driven by an (ensemble, target tile, source-tile group) work list, the
+ * 16-step block replayed as one CUDA graph.  No reference counterpart: the
+ * reference runs one ensemble per process.  Members keep their own device
+ * state and are advanced exactly as qg_run would advance them (bitwise the
+ * same results); they must share interpolation order, frame and history
+ * width, must join at a step that is a multiple of 16, and must not be run on
+ * their own while in a batch.  A member that reaches num_timesteps stops
+ * there while the others go on. */
+typedef struct qg_batch_s qg_batch;
+qg_status qg_batch_create(int capacity, qg_batch **out);
+qg_status qg_batch_destroy(qg_batch *b);
+qg_status qg_batch_add(qg_batch *b, qg_handle *h);
+qg_status qg_batch_remove(qg_batch *b, qg_handle *h);
+/* Advances every member by n_blocks x 16 steps (capped at its num_timesteps). */
+qg_status qg_batch_run(qg_batch *b, int n_blocks);
+qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks);
+
 /* Diagnostics of the built state. */
 typedef struct {
   int n;                 /* dots */

@@ -72,7 +72,9 @@ class QgInfo(ctypes.Structure):
 EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_destroy", "qg_run",
            "qg_next_step", "qg_history_evaluate", "qg_pulse_evaluate", "qg_set_history",
            "qg_get_history", "qg_get_info", "qg_footprint", "qg_stream", "qg_kernel_time",
-           "qg_set_option", "qg_history_evaluate_noalloc"]
+           "qg_set_option", "qg_history_evaluate_noalloc", "qg_get_state", "qg_bad_step",
+           "qg_batch_create", "qg_batch_destroy", "qg_batch_add", "qg_batch_remove", "qg_batch_run",
+           "qg_batch_size"]
 
 _lib = None
 
@@ -107,6 +109,14 @@ def lib():
         L.qg_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip, dp, ip]
         L.qg_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.qg_history_evaluate_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+        L.qg_get_state.argtypes = [vp, dp]
+        L.qg_bad_step.argtypes = [vp, ip]
+        L.qg_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.qg_batch_destroy.argtypes = [vp]
+        L.qg_batch_add.argtypes = [vp, vp]
+        L.qg_batch_remove.argtypes = [vp, vp]
+        L.qg_batch_run.argtypes = [vp, ctypes.c_int]
+        L.qg_batch_size.argtypes = [vp, ip, ip, ip]
         _lib = L
     return _lib
 
@@ -246,6 +256,17 @@ class Simulation:
         _check(lib().qg_get_history(self.h, t0, n, _dp(out.view(np.float64))))
         return out
 
+    def state(self) -> np.ndarray:
+        """rho (N, 2) complex after the last computed step."""
+        out = np.empty((self.n, 2), dtype=np.complex128)
+        _check(lib().qg_get_state(self.h, _dp(out.view(np.float64))))
+        return out
+
+    def bad_step(self) -> int:
+        b = ctypes.c_int()
+        _check(lib().qg_bad_step(self.h, ctypes.byref(b)))
+        return b.value
+
     def info(self) -> dict:
         i = QgInfo()
         _check(lib().qg_get_info(self.h, ctypes.byref(i)))
@@ -264,6 +285,43 @@ class Simulation:
         _check(lib().qg_kernel_time(self.h, int(reset), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(sms),
                                     ctypes.byref(sn)))
         return ms.value, n.value, sms.value, sn.value
+
+
+class Batch:
+    """Many ensembles advanced together (qg_batch_*)."""
+
+    def __init__(self, capacity: int):
+        b = ctypes.c_void_p()
+        _check(lib().qg_batch_create(capacity, ctypes.byref(b)))
+        self.b = b
+        self.members: list[Simulation] = []
+
+    def add(self, sim: Simulation) -> None:
+        _check(lib().qg_batch_add(self.b, sim.h))
+        self.members.append(sim)
+
+    def remove(self, sim: Simulation) -> None:
+        _check(lib().qg_batch_remove(self.b, sim.h))
+        self.members.remove(sim)
+
+    def run(self, n_blocks: int) -> None:
+        _check(lib().qg_batch_run(self.b, n_blocks))
+
+    def size(self) -> tuple[int, int, int]:
+        m, t, bl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().qg_batch_size(self.b, ctypes.byref(m), ctypes.byref(t), ctypes.byref(bl)))
+        return m.value, t.value, bl.value
+
+    def close(self) -> None:
+        if getattr(self, "b", None) is not None and self.b.value:
+            lib().qg_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def footprint(n: int, constants, side: float, precision=PREC_FP64, coef_mode=COEF_AUTO) -> int:

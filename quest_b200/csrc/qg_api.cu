@@ -108,7 +108,7 @@ struct qg_handle_s {
   bool events_ready = false;
   double pair_ms = 0, step_ms = 0;
   int pair_launches = 0, step_launches = 0;
-  cudaEvent_t ev_chunk[2], ev_copy[2];
+  cudaEvent_t ev_chunk[2] = {nullptr, nullptr}, ev_copy[2] = {nullptr, nullptr};
 
   FarArgs far_args(const int *d_t0, int *far_t0_out) const
   {
@@ -138,6 +138,7 @@ struct qg_handle_s {
     a.n = n;
     a.n_pad = n_pad;
     a.nT = nT;
+    a.T = T;
     a.W = W;
     a.stride = stride;
     a.q = q;
@@ -223,10 +224,10 @@ static void destroy_handle(qg_handle *h)
       cudaEventDestroy(h->ev_c[i]);
       cudaEventDestroy(h->ev_d[i]);
     }
-    for(int i = 0; i < 2; ++i) {
-      cudaEventDestroy(h->ev_chunk[i]);
-      cudaEventDestroy(h->ev_copy[i]);
-    }
+  }
+  for(int i = 0; i < 2; ++i) {
+    if(h->ev_chunk[i]) cudaEventDestroy(h->ev_chunk[i]);
+    if(h->ev_copy[i]) cudaEventDestroy(h->ev_copy[i]);
   }
   for(void *p : h->allocs) cudaFree(p);
   if(h->h_traj) cudaFreeHost(h->h_traj);
@@ -705,20 +706,12 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_TRY(dalloc(h, &h->d_scratch, (size_t)h->n_pad * 8));
   h->traj_k = traj_steps(n);
   QG_TRY(dalloc(h, &h->d_traj, (size_t)2 * h->traj_k * n * 2));
-  QG_CUDA(cudaMallocHost((void **)&h->h_traj, sizeof(double2) * (size_t)2 * h->traj_k * n * 2));
   QG_TRY(dalloc(h, &h->d_io, (size_t)n));
   QG_CUDA(cudaMallocHost((void **)&h->h_io, sizeof(double2) * (size_t)n));
-  for(int i = 0; i < 256; ++i) {
-    QG_CUDA(cudaEventCreate(&h->ev_a[i]));
-    QG_CUDA(cudaEventCreate(&h->ev_b[i]));
-    QG_CUDA(cudaEventCreate(&h->ev_c[i]));
-    QG_CUDA(cudaEventCreate(&h->ev_d[i]));
-  }
   for(int i = 0; i < 2; ++i) {
     QG_CUDA(cudaEventCreateWithFlags(&h->ev_chunk[i], cudaEventDisableTiming));
     QG_CUDA(cudaEventCreateWithFlags(&h->ev_copy[i], cudaEventDisableTiming));
   }
-  h->events_ready = true;
 
   QG_TRY(build_lists(h));
   QG_TRY(reset_state(h));
@@ -840,6 +833,28 @@ static qg_status launch_prof_block(qg_handle *h, int traj)
   return QG_OK;
 }
 
+// Host-side resources made on first use: pinned trajectory staging (a
+// recorded qg_run or qg_get_state) and the profiling events.
+static qg_status ensure_host_staging(qg_handle *h)
+{
+  if(h->h_traj) return QG_OK;
+  QG_CUDA(cudaMallocHost((void **)&h->h_traj, sizeof(double2) * (size_t)2 * h->traj_k * h->n * 2));
+  return QG_OK;
+}
+
+static qg_status ensure_events(qg_handle *h)
+{
+  if(h->events_ready) return QG_OK;
+  for(int i = 0; i < 256; ++i) {
+    QG_CUDA(cudaEventCreate(&h->ev_a[i]));
+    QG_CUDA(cudaEventCreate(&h->ev_b[i]));
+    QG_CUDA(cudaEventCreate(&h->ev_c[i]));
+    QG_CUDA(cudaEventCreate(&h->ev_d[i]));
+  }
+  h->events_ready = true;
+  return QG_OK;
+}
+
 static qg_status collect_events(qg_handle *h, int nev, int nstep)
 {
   if(nev > 0) {
@@ -921,6 +936,7 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   if(!rho_out) {
     QG_TRY(launch_steps(h, t_start, n_steps, false));
   } else {
+    QG_TRY(ensure_host_staging(h));
     const int K = h->traj_k;
     const int nchunks = (n_steps + K - 1) / K;
     auto drain = [&](int c) -> qg_status {
@@ -959,6 +975,199 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
     if(bad_step) *bad_step = bad;
     return qg_fail(QG_ERR_NONFINITE, "unbounded history values at or before step %d", bad);
   }
+  return QG_OK;
+}
+
+// ---- batches: many ensembles advanced together -----------------------------
+struct qg_batch_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int capacity = 0;
+  std::vector<qg_handle *> members;
+  FarArgs *d_far = nullptr;
+  StepArgs *d_step = nullptr;
+  int *d_task_off = nullptr, *d_block_off = nullptr;
+  int q = -1, frame = -1, n_time = -1;
+  int total_tasks = 0, total_blocks = 0;
+  int far_grid = 0;
+  bool dirty = true;
+  cudaGraphExec_t graph = nullptr;
+};
+
+extern "C" qg_status qg_batch_create(int capacity, qg_batch **out)
+{
+  if(!out || capacity < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_create: bad argument");
+  *out = nullptr;
+  qg_batch *b = new qg_batch();
+  b->capacity = capacity;
+  auto fail = [&](qg_status st) {
+    if(b->d_far) cudaFree(b->d_far);
+    if(b->d_step) cudaFree(b->d_step);
+    if(b->d_task_off) cudaFree(b->d_task_off);
+    if(b->d_block_off) cudaFree(b->d_block_off);
+    if(b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return st;
+  };
+  cudaError_t e;
+  if((e = cudaGetDevice(&b->device)) != cudaSuccess ||
+     (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+     (e = cudaMalloc(&b->d_far, sizeof(FarArgs) * capacity)) != cudaSuccess ||
+     (e = cudaMalloc(&b->d_step, sizeof(StepArgs) * capacity)) != cudaSuccess ||
+     (e = cudaMalloc(&b->d_task_off, sizeof(int) * (capacity + 1))) != cudaSuccess ||
+     (e = cudaMalloc(&b->d_block_off, sizeof(int) * (capacity + 1))) != cudaSuccess)
+    return fail(qg_fail(e == cudaErrorMemoryAllocation ? QG_ERR_OOM : QG_ERR_CUDA, "qg_batch_create: %s",
+                        cudaGetErrorString(e)));
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  per_sm = 3;  // far kernel: 168 registers x 128 threads -> 3 blocks per SM
+  b->far_grid = std::max(1, sms * per_sm);
+  *out = b;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_batch_destroy(qg_batch *b)
+{
+  if(!b) return QG_OK;
+  cudaStreamSynchronize(b->stream);
+  if(b->graph) cudaGraphExecDestroy(b->graph);
+  cudaFree(b->d_far);
+  cudaFree(b->d_step);
+  cudaFree(b->d_task_off);
+  cudaFree(b->d_block_off);
+  cudaStreamDestroy(b->stream);
+  delete b;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_batch_add(qg_batch *b, qg_handle *h)
+{
+  if(!b || !h) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: NULL argument");
+  if((int)b->members.size() >= b->capacity)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: batch is full (%d members)", b->capacity);
+  if(std::find(b->members.begin(), b->members.end(), h) != b->members.end())
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: handle already in the batch");
+  if(h->device != b->device) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: handle on another device");
+  if(!h->fused)
+    return qg_fail(QG_ERR_UNSUPPORTED,
+                   "qg_batch_add: a group of dots coupled at delay 0 exceeds 32; run this handle alone");
+  if(h->next_step % kTimeBlock != 0)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: next step %d is not a multiple of %d", h->next_step,
+                   kTimeBlock);
+  if(!b->members.empty() && (h->q != b->q || h->params.frame != b->frame || h->w.n_time != b->n_time))
+    return qg_fail(QG_ERR_INVALID_ARG,
+                   "qg_batch_add: members must share interpolation order, frame and history width");
+  b->q = h->q;
+  b->frame = h->params.frame;
+  b->n_time = h->w.n_time;
+  // the member's device state must name the next block's first step
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  launch_set_int(h->d_ints + 0, h->next_step, b->stream);
+  b->members.push_back(h);
+  b->dirty = true;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_batch_remove(qg_batch *b, qg_handle *h)
+{
+  if(!b || !h) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_remove: NULL argument");
+  auto it = std::find(b->members.begin(), b->members.end(), h);
+  if(it == b->members.end()) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_remove: handle not in the batch");
+  QG_CUDA(cudaStreamSynchronize(b->stream));
+  b->members.erase(it);
+  b->dirty = true;
+  return QG_OK;
+}
+
+static qg_status batch_rebuild(qg_batch *b)
+{
+  const int n = (int)b->members.size();
+  std::vector<FarArgs> fa(n);
+  std::vector<StepArgs> sa(n);
+  std::vector<int> toff(n + 1, 0), boff(n + 1, 0);
+  for(int e = 0; e < n; ++e) {
+    qg_handle *h = b->members[e];
+    fa[e] = h->far_args(h->d_ints + 0, h->d_ints + 6);
+    sa[e] = h->step_args(false);
+    toff[e + 1] = toff[e] + h->nT * h->nG;
+    boff[e + 1] = boff[e] + h->step_blocks;
+  }
+  b->total_tasks = toff[n];
+  b->total_blocks = boff[n];
+  if(n > 0) {
+    QG_CUDA(cudaMemcpyAsync(b->d_far, fa.data(), sizeof(FarArgs) * n, cudaMemcpyHostToDevice, b->stream));
+    QG_CUDA(cudaMemcpyAsync(b->d_step, sa.data(), sizeof(StepArgs) * n, cudaMemcpyHostToDevice, b->stream));
+  }
+  QG_CUDA(cudaMemcpyAsync(b->d_task_off, toff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, b->stream));
+  QG_CUDA(cudaMemcpyAsync(b->d_block_off, boff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, b->stream));
+  QG_CUDA(cudaStreamSynchronize(b->stream));
+  if(b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if(n > 0) {
+    cudaGraph_t g;
+    QG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->far_grid, b->stream);
+    for(int k = 0; k < kTimeBlock; ++k)
+      launch_step_batch(b->d_step, b->d_block_off, n, b->total_blocks, b->n_time, k, b->stream);
+    QG_CUDA(cudaStreamEndCapture(b->stream, &g));
+    QG_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
+    cudaGraphDestroy(g);
+  }
+  b->dirty = false;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_batch_run(qg_batch *b, int n_blocks)
+{
+  if(!b || n_blocks < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_run: bad argument");
+  QG_CUDA(cudaSetDevice(b->device));
+  if(b->dirty) QG_TRY(batch_rebuild(b));
+  if(b->members.empty()) return QG_OK;
+  for(int i = 0; i < n_blocks; ++i) QG_CUDA(cudaGraphLaunch(b->graph, b->stream));
+  QG_CUDA(cudaStreamSynchronize(b->stream));
+  QG_CUDA(cudaGetLastError());
+  for(qg_handle *h : b->members) {
+    const int start = h->next_step;
+    h->next_step = std::min(h->T, start + n_blocks * kTimeBlock);
+    h->far_block = start + (n_blocks - 1) * kTimeBlock;
+    h->eval_cached = -0x7fffffff;
+  }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks)
+{
+  if(!b) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_size: NULL batch");
+  if(members) *members = (int)b->members.size();
+  if(tasks) *tasks = b->total_tasks;
+  if(blocks) *blocks = b->total_blocks;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_bad_step(qg_handle *h, int *bad_step)
+{
+  if(!h || !bad_step) return qg_fail(QG_ERR_INVALID_ARG, "qg_bad_step: NULL argument");
+  QG_CUDA(cudaSetDevice(h->device));
+  int bad = kBadNone;
+  QG_CUDA(cudaMemcpy(&bad, h->d_ints + 2, sizeof(int), cudaMemcpyDeviceToHost));
+  *bad_step = bad == kBadNone ? -1 : bad;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_get_state(qg_handle *h, double *rho_out)
+{
+  if(!h || !rho_out) return qg_fail(QG_ERR_INVALID_ARG, "qg_get_state: NULL argument");
+  QG_CUDA(cudaSetDevice(h->device));
+  QG_TRY(ensure_host_staging(h));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  launch_state_read(h->step_args(true), h->next_step - 1, h->d_traj, h->stream);
+  QG_CUDA(cudaGetLastError());
+  QG_CUDA(cudaMemcpyAsync(h->h_traj, h->d_traj, sizeof(double2) * 2 * (size_t)h->n, cudaMemcpyDeviceToHost,
+                          h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  std::memcpy(rho_out, h->h_traj, sizeof(double2) * 2 * (size_t)h->n);
   return QG_OK;
 }
 
@@ -1149,6 +1358,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
   if(!std::strcmp(key, "graph")) {
     h->use_graph = value != 0;
   } else if(!std::strcmp(key, "profile")) {
+    if(value) QG_TRY(ensure_events(h));
     h->profile = value != 0;
   } else if(!std::strcmp(key, "far_variant")) {
     if(value < 0 || value > 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..2");

@@ -118,10 +118,9 @@ __device__ __forceinline__ void window_conv2(const double2 *ring, int slot_even,
 // a single-step evaluation).  Pairs with delay < kTimeBlock are left to the
 // mid list in either case.
 template <int Q, bool LAB, int VEC, int K = kTimeBlock>
-__device__ __forceinline__ void far_body(const FarArgs &a)
+__device__ __forceinline__ void far_body(const FarArgs &a, int task)
 {
   const int lane = threadIdx.x & 31;
-  const int task = blockIdx.x * 4 + (threadIdx.x >> 5);
   static_assert(VEC == 0 || VEC == 1, "VEC");
   if(task >= a.nT * a.nG) return;  // uniform per warp
   const int I = task / a.nG, g = task % a.nG;
@@ -204,12 +203,64 @@ __device__ __forceinline__ void far_body(const FarArgs &a)
 //   far_kernel      3 blocks of 4 warps per SM, one sample per load
 //   far_kernel_r4   registers capped for 4 blocks per SM
 //   far_kernel_v2   capped, two samples per 32-byte load
+__device__ __forceinline__ int warp_task() { return blockIdx.x * 4 + (threadIdx.x >> 5); }
+
 template <int Q, bool LAB>
-__global__ void __launch_bounds__(128) far_kernel(FarArgs a) { far_body<Q, LAB, 0>(a); }
+__global__ void __launch_bounds__(128) far_kernel(FarArgs a) { far_body<Q, LAB, 0>(a, warp_task()); }
 template <int Q, bool LAB>
-__global__ void __launch_bounds__(128, 4) far_kernel_r4(FarArgs a) { far_body<Q, LAB, 0>(a); }
+__global__ void __launch_bounds__(128, 4) far_kernel_r4(FarArgs a) { far_body<Q, LAB, 0>(a, warp_task()); }
 template <int Q, bool LAB>
-__global__ void __launch_bounds__(128, 4) far_kernel_v2(FarArgs a) { far_body<Q, LAB, 1>(a); }
+__global__ void __launch_bounds__(128, 4) far_kernel_v2(FarArgs a) { far_body<Q, LAB, 1>(a, warp_task()); }
+
+// Many ensembles in one persistent launch: a work list of (ensemble,
+// target tile, source-tile group) tasks, task_off[e] = first task of
+// ensemble e (prefix sums, task_off[n_ens] = total).  Warps stride over the
+// list; every task writes its own partial slot, so the assignment of tasks to
+// warps does not change any result.
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restrict__ args,
+                                                        const int *__restrict__ task_off, int n_ens)
+{
+  const int total = task_off[n_ens];
+  for(int task = warp_task(); task < total; task += gridDim.x * 4) {
+    int lo = 0, hi = n_ens - 1;
+    while(lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if(task_off[mid] <= task)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const FarArgs a = args[lo];
+    far_body<Q, LAB, 0>(a, task - task_off[lo]);
+  }
+}
+
+template <bool LAB>
+static void launch_far_batch_frame(const FarArgs *args, const int *task_off, int n_ens, int q, int grid,
+                                   cudaStream_t s)
+{
+  switch(q) {
+    case 1: far_batch_kernel<1, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 2: far_batch_kernel<2, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 3: far_batch_kernel<3, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 4: far_batch_kernel<4, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 5: far_batch_kernel<5, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 6: far_batch_kernel<6, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 7: far_batch_kernel<7, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    default: break;
+  }
+}
+
+void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int grid,
+                      void *stream)
+{
+  if(n_ens <= 0) return;
+  if(frame == 0)
+    launch_far_batch_frame<false>(args, task_off, n_ens, q, grid, (cudaStream_t)stream);
+  else
+    launch_far_batch_frame<true>(args, task_off, n_ens, q, grid, (cudaStream_t)stream);
+}
 
 template <int Q, bool LAB>
 static void launch_far_q(const FarArgs &a, cudaStream_t s)
@@ -294,7 +345,7 @@ qg_status noalloc_scratch(NoAllocScratch *out)
 }
 
 template <int Q, bool LAB>
-__global__ void __launch_bounds__(128) far_kernel_step1(FarArgs a) { far_body<Q, LAB, 0, 1>(a); }
+__global__ void __launch_bounds__(128) far_kernel_step1(FarArgs a) { far_body<Q, LAB, 0, 1>(a, warp_task()); }
 
 template <bool LAB>
 static void launch_far1_frame(const FarArgs &a, cudaStream_t s)

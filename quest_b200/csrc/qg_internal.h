@@ -78,6 +78,7 @@ struct FarArgs {
 // Arguments of the per-dot step kernels.
 struct StepArgs {
   int n, n_pad, nT, W, stride, q, frame;
+  int T;                 // num_timesteps: steps at or past T are not computed
   double dt, laser_freq, hbar;
   PulseParams pulse;
   const double *pos;     // [n_pad][3] internal order
@@ -126,6 +127,10 @@ struct NoAllocScratch {
 };
 qg_status noalloc_scratch(NoAllocScratch *out);
 void launch_far_step1(const FarArgs &a, void *stream);
+void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int grid,
+                      void *stream);
+void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
+                       int k, void *stream);
 
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);
@@ -143,5 +148,6 @@ void launch_set_int(int *p, int v, void *stream);
 void launch_init_state(const StepArgs &a, void *stream);
 void launch_ring_write(const StepArgs &a, int t, const double2 *rho01_user, void *stream);
 void launch_ring_read(const StepArgs &a, int t, double2 *rho01_user, void *stream);
+void launch_state_read(const StepArgs &a, int t, double2 *rho_user, void *stream);
 
 }  // namespace qg

@@ -175,9 +175,9 @@ __device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, co
 
 // The step index is the far block's first step plus the launch's offset k;
 // the last step of a block tells the next far-kernel launch where it starts.
-__device__ __forceinline__ void publish_next_block(const StepArgs &a, int k, int t)
+__device__ __forceinline__ void publish_next_block(const StepArgs &a, int blk, int k, int t)
 {
-  if(k == kTimeBlock - 1 && blockIdx.x == 0 && threadIdx.x == 0) *a.d_next = t + 1;
+  if(k == kTimeBlock - 1 && blk == 0 && threadIdx.x == 0) *a.d_next = t + 1;
 }
 
 // The gathers of one step, split over the 4 warps of a block (32 dots):
@@ -249,15 +249,16 @@ __device__ __forceinline__ double2 mid_entry(const StepArgs &a, int e, int t)
 // coupled at delay 0 share the block and exchange their iterates through
 // shared memory after each correction.
 template <int NT>
-__global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int k)
+__device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int k)
 {
   constexpr int BS = 32;
   __shared__ double2 red[kParts][4][BS];
   __shared__ double2 midv[kMidChunk];
   __shared__ double2 cur[BS];
   const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
-  const int idx = blockIdx.x * BS + lane;
+  const int idx = blk * BS + lane;
   const int t = *a.far_t0 + k;
+  if(t >= a.T) return;  // past this ensemble's last step (uniform per block)
   const bool live = a.user[idx] >= 0;
 
   // warp 0's per-dot inputs, requested before the gathers complete
@@ -278,7 +279,7 @@ __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int
   }
 
   // mid list of the block's 32 dots: CSR range [E0, E1)
-  const int E0 = a.mid_ptr[blockIdx.x * BS], E1 = a.mid_ptr[blockIdx.x * BS + BS];
+  const int E0 = a.mid_ptr[blk * BS], E1 = a.mid_ptr[blk * BS + BS];
   const int my0 = a.mid_ptr[idx], my1 = a.mid_ptr[idx + 1];
   double2 M = make_double2(0.0, 0.0);
   for(int c0 = E0; c0 < E1; c0 += kMidChunk) {
@@ -295,8 +296,8 @@ __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int
   if(E0 == E1) __syncthreads();  // the window partials are complete
 
   if(part == 0) {
-    const int nb0 = a.near_ptr[blockIdx.x * BS];
-    const bool block_near = a.near_ptr[(blockIdx.x + 1) * BS] > nb0;
+    const int nb0 = a.near_ptr[blk * BS];
+    const bool block_near = a.near_ptr[(blk + 1) * BS] > nb0;
     double2 P[2], H[2], r[2], dr[2];
     if(live) {
       double2 sum[4];
@@ -339,7 +340,42 @@ __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int
     }
     if(live) finish_dot(a, idx, t, r, dr);
   }
-  publish_next_block(a, k, t);
+  publish_next_block(a, blk, k, t);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int k)
+{
+  step_fused_body<NT>(a, blockIdx.x, k);
+}
+
+// Many ensembles, one launch: block_off[e] = first 32-dot block of ensemble e.
+template <int NT>
+__global__ void __launch_bounds__(32 * kParts) step_batch_kernel(const StepArgs *__restrict__ args,
+                                                                 const int *__restrict__ block_off,
+                                                                 int n_ens, int k)
+{
+  const int b = blockIdx.x;
+  int lo = 0, hi = n_ens - 1;
+  while(lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if(block_off[mid] <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  step_fused_body<NT>(args[lo], b - block_off[lo], k);
+}
+
+void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
+                       int k, void *stream)
+{
+  if(n_ens <= 0 || total_blocks <= 0) return;
+  cudaStream_t s = (cudaStream_t)stream;
+  if(n_time == 22)
+    step_batch_kernel<22><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
+  else
+    step_batch_kernel<0><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
 }
 
 // General form, one launch per phase: phase 0 predicts, phases 1..11 are the
@@ -393,7 +429,7 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
       finish_dot(a, idx, t, r, dr);
     }
   }
-  if(it == kCorrectorSteps) publish_next_block(a, k, t);
+  if(it == kCorrectorSteps) publish_next_block(a, blockIdx.x, k, t);
 }
 
 void launch_step_fused(const StepArgs &a, int k, int nblocks, void *stream)
@@ -501,6 +537,21 @@ __global__ void ring_read_kernel(StepArgs a, int t, double2 *rho01_user)
 void launch_ring_read(const StepArgs &a, int t, double2 *rho01_user, void *stream)
 {
   ring_read_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho01_user);
+}
+
+// rho (rho00, rho01) of every dot at step t (t >= -22), user order.
+__global__ void state_read_kernel(StepArgs a, int t, double2 *rho_user)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= a.n_pad || a.user[idx] < 0) return;
+  const double2 *base = a.pcr + (long long)pc_slot(t) * 4 * a.n_pad + idx;
+  rho_user[2 * a.user[idx]] = base[0];
+  rho_user[2 * a.user[idx] + 1] = base[a.n_pad];
+}
+
+void launch_state_read(const StepArgs &a, int t, double2 *rho_user, void *stream)
+{
+  state_read_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho_user);
 }
 
 }  // namespace qg

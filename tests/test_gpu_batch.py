@@ -1,0 +1,75 @@
+"""Batches: many ensembles in one persistent launch per step must give each
+ensemble exactly the result it gets alone (same kernels, same summation
+order), whatever else is in the batch and whenever it joined."""
+import numpy as np
+import pytest
+
+from quest_b200 import capi, inputs as I
+
+pytestmark = pytest.mark.gpu
+
+
+def ensemble(seed, n, side, steps, amp):
+    dots = I.make_dots(n, side, seed, omega_sigma=0.5, dipole=None, dipole_magnitude=2e-4)
+    pulse = I.make_pulse(amplitude=amp, delay=0.05)
+    return dots, pulse, I.Constants(num_timesteps=steps)
+
+
+def solo(d, p, c, weights, steps):
+    with capi.Simulation(d, p, c, weights=weights) as sim:
+        sim.run(steps, record=False)
+        return sim.state(), sim.bad_step()
+
+
+def test_batch_equals_solo_runs(golden_weights):
+    specs = [(11, 64, 0.05, 160, 5.0), (12, 200, 0.1, 96, 20.0), (13, 1000, 0.2, 160, 15.0)]
+    ens = [ensemble(*s) for s in specs]
+    batch = capi.Batch(8)
+    sims = [capi.Simulation(d, p, c, weights=golden_weights) for d, p, c in ens]
+    for s in sims:
+        batch.add(s)
+    assert batch.size()[0] == 3
+    batch.run(10)  # 160 steps; the second member stops at its 96
+    for (d, p, c), sim, spec in zip(ens, sims, specs):
+        assert sim.next_step == spec[3]
+        ref, bad = solo(d, p, c, golden_weights, spec[3])
+        np.testing.assert_array_equal(sim.state(), ref)
+        assert sim.bad_step() == bad == -1
+    for s in sims:
+        batch.remove(s)
+        s.close()
+    batch.close()
+
+
+def test_member_joining_later_is_unaffected(golden_weights):
+    a = ensemble(21, 300, 0.1, 128, 10.0)
+    b = ensemble(22, 500, 0.15, 64, 25.0)
+    batch = capi.Batch(4)
+    sa = capi.Simulation(*a, weights=golden_weights)
+    sb = capi.Simulation(*b, weights=golden_weights)
+    batch.add(sa)
+    batch.run(4)            # a alone: steps 0..63
+    batch.add(sb)
+    batch.run(4)            # a: 64..127, b: 0..63 together
+    np.testing.assert_array_equal(sa.state(), solo(*a, golden_weights, 128)[0])
+    np.testing.assert_array_equal(sb.state(), solo(*b, golden_weights, 64)[0])
+    batch.close()
+    sa.close()
+    sb.close()
+
+
+def test_batch_rejects_mismatched_members(golden_weights):
+    a = ensemble(31, 100, 0.1, 64, 10.0)
+    b = ensemble(32, 100, 0.1, 64, 10.0)
+    b[2].interpolation_order = 3
+    batch = capi.Batch(2)
+    sa = capi.Simulation(*a, weights=golden_weights)
+    sb = capi.Simulation(*b, weights=golden_weights)
+    batch.add(sa)
+    with pytest.raises(capi.QuestError):
+        batch.add(sb)
+    sc = capi.Simulation(*ensemble(33, 100, 0.1, 64, 10.0), weights=golden_weights)
+    sc.run(5, record=False)
+    with pytest.raises(capi.QuestError):
+        batch.add(sc)  # not on a 16-step boundary
+    batch.close()
