@@ -118,13 +118,16 @@ def workload(args, rank: int) -> I.Workload:
     return wl
 
 
-def fp64_peak_tflops() -> float:
-    """Dense FP64 throughput of this GPU, measured as the best of 5 cuBLAS
-    DGEMMs of 8192^3 (2 n^3 flops each), CUDA events."""
+def fp64_peak_tflops(dtype="float64") -> float:
+    """Dense throughput of this GPU in the given type, measured as the best
+    of 5 cuBLAS GEMMs of 8192^3 (2 n^3 flops each), CUDA events; FP32 with
+    TF32 disabled (CUDA-core FMA)."""
     import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    dt = torch.float64 if dtype == "float64" else torch.float32
+    a = torch.randn(n, n, dtype=dt, device="cuda")
+    b = torch.randn(n, n, dtype=dt, device="cuda")
     c = a @ b
     best = 1e30
     for _ in range(5):
@@ -215,7 +218,7 @@ def run_reference(args, world, rank):
 
 
 def config_dict(args):
-    return {"workload": f"fp64_table_N{args.n}_T{args.warmup + args.steps}", "N": args.n,
+    return {"workload": f"{args.precision}_table_N{args.n}_T{args.warmup + args.steps}", "N": args.n,
             "steps_total": args.warmup + args.steps, "interpolation_order": 5, "side": 0.2,
             "dt": 1e-3, "c0": 1.0, "hbar": 1.0, "mu0": 1.0, "laser_frequency": 200.0,
             "pulse_delay": args.pulse_delay, "precision": "fp64", "coef_mode": "table",
@@ -237,7 +240,8 @@ def run_ours(args, world, rank, local):
 
     # ---- device-resident throughput (value) and the sweep kernel's roofline
     nonfinite = None
-    sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights)
+    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec)
     info = sim.info()
     try:
         sim.run(args.warmup, record=False)
@@ -272,7 +276,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights) as sim2:
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec) as sim2:
         try:
             sim2.run(total, out=rho_host)
         except capi.NonFiniteError:
@@ -285,20 +289,23 @@ def run_ours(args, world, rank, local):
     hbm, src = peaks()
     q = 5
     K = info["time_block"]
+    mixed = args.precision == "mixed"
     # the table holds every ordered pair (each unordered pair twice) and one
-    # launch streams it once for K steps
-    alg_bytes = 2 * info["num_pairs"] * TABLE_BYTES_PER_PAIR(q)
+    # launch streams it once for K steps; mixed: q+1 complex64 taps + their sum
+    per_pair = (4 + 8 * (q + 2)) if mixed else TABLE_BYTES_PER_PAIR(q)
+    alg_bytes = 2 * info["num_pairs"] * per_pair
     far_ordered = 2 * (info["num_pairs"] - info["mid_pairs"])
     flops = far_ordered * K * (q + 1) * 8  # complex multiply-add = 4 FMA = 8 flops
     avg_ms = pair_ms / max(launches, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     fp64_tf = flops / (avg_ms / 1e3) / 1e12
-    fp64_peak = fp64_peak_tflops()
+    fp64_peak = fp64_peak_tflops("float32" if mixed else "float64")
     traffic = profile_traffic("far_kernel_fp64_N4096")  # ncu dram read+write per launch
     line = {
         "metric": "pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair sum + f64 state (mixed)" if mixed else "f64",
         "data": "synthetic (seeded dots and pulse of the stated distributions)",
         "config": config_dict(args),
         "roofline": {"bound": "hbm", "kernel": "far_kernel<5,false>", "achieved": achieved, "peak": hbm,
@@ -307,9 +314,11 @@ def run_ours(args, world, rank, local):
                      "avg_launch_ms": avg_ms, "share_of_timed_region": pair_ms / ms if ms > 0 else None,
                      "step_kernels_ms_per_step": step_ms / max(step_launches, 1),
                      "far_variant": args.far_variant,
-                     "fp64": {"achieved": fp64_tf, "peak": fp64_peak, "unit": "TFLOP/s",
-                              "frac": fp64_tf / fp64_peak, "flops_per_launch": flops,
-                              "peak_source": "measured here: best cuBLAS DGEMM 8192^3"}},
+                     ("fp32" if mixed else "fp64"): {
+                         "achieved": fp64_tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": fp64_tf / fp64_peak,
+                         "flops_per_launch": flops,
+                         "peak_source": "measured here: best cuBLAS %s 8192^3" % ("SGEMM (no TF32)" if mixed
+                                                                                   else "DGEMM")}},
         "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s,
                 "h2d_bytes_per_step": (n * 72 + 80) / total, "d2h_bytes_per_step": n * 32,
                 "includes": "qg_create (dots upload + table build) + qg_run with every step's rho read back"},
@@ -339,7 +348,8 @@ def run_batched(args, world, rank, local):
     torch.cuda.set_device(local)
     reqs = serving.batched_ensembles(args.ensembles, seed=40 + rank)
     weights = capi.pc_weights()
-    sims = [capi.Simulation(r.dots, r.pulse, r.constants, weights=weights) for r in reqs]
+    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    sims = [capi.Simulation(r.dots, r.pulse, r.constants, weights=weights, precision=prec) for r in reqs]
     batch = capi.Batch(len(sims))
     for s in sims:
         batch.add(s)
@@ -366,7 +376,7 @@ def run_batched(args, world, rank, local):
             "data": "synthetic (seeded ensembles)",
             "config": {"workload": f"batched_{args.ensembles}_ensembles", "ensembles": args.ensembles,
                        "N_min": int(ns.min()), "N_max": int(ns.max()), "sum_N2T": total,
-                       "precision": "fp64", "coef_mode": "table"},
+                       "precision": args.precision, "coef_mode": "table"},
             "wall_s": wall}
     for s in sims:
         s.close()
@@ -385,7 +395,8 @@ def run_serving(args, world, rank, local):
     from quest_b200 import capi, serving
     torch.cuda.set_device(local)
     reqs = serving.serving_requests(args.requests, args.rate, seed=70 + rank, n_range=(32, args.serve_nmax))
-    srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=capi.pc_weights())
+    srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=capi.pc_weights(),
+                         precision=capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64)
     barrier(world)
     stats = srv.serve(reqs)
     srv.close()
@@ -394,7 +405,7 @@ def run_serving(args, world, rank, local):
             "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Poisson request stream)",
             "config": {"workload": "serving", "requests": args.requests, "rate_per_s": args.rate,
-                       "N_max": args.serve_nmax, "budget_gb": args.budget_gb, "precision": "fp64"},
+                       "N_max": args.serve_nmax, "budget_gb": args.budget_gb, "precision": args.precision},
             "serving": stats}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -414,6 +425,7 @@ def main():
     ap.add_argument("--dipole-scale", type=float, default=1.0)
     ap.add_argument("--far-variant", type=int, default=0)
     ap.add_argument("--workload", choices=["table", "batched", "serving"], default="table")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--ensembles", type=int, default=256)
     ap.add_argument("--blocks-per-round", type=int, default=8)
     ap.add_argument("--requests", type=int, default=64)

@@ -62,6 +62,9 @@ struct qg_handle_s {
   int *d_user = nullptr;
   int *d_delay = nullptr;
   double2 *d_coef = nullptr;
+  float2 *d_coef32 = nullptr;              // mixed precision table
+  float2 *d_ring32w = nullptr, *d_ring32d = nullptr;
+  bool mixed = false;
   double2 *d_ring = nullptr;
   int W = 0, stride = 0;
   double2 *d_pcr = nullptr, *d_partial = nullptr, *d_field = nullptr, *d_scratch = nullptr;
@@ -115,6 +118,10 @@ struct qg_handle_s {
     FarArgs s{};
     s.delay = d_delay;
     s.coef = d_coef;
+    s.coef32 = d_coef32;
+    s.ring32w = d_ring32w;
+    s.ring32d = d_ring32d;
+    s.mixed = mixed ? 1 : 0;
     s.ring = d_ring;
     s.partial = d_partial;
     s.field = d_field;
@@ -167,6 +174,8 @@ struct qg_handle_s {
     a.mid_coef = d_mid_coef;
     a.pcr = d_pcr;
     a.ring = d_ring;
+    a.ring32w = d_ring32w;
+    a.ring32d = d_ring32d;
     a.near_ptr = general ? d_gnear_ptr : d_fnear_ptr;
     a.near_idx = general ? d_gnear_idx : d_fnear_idx;
     a.near_coef = general ? d_gnear_coef : d_fnear_coef;
@@ -305,8 +314,8 @@ static qg_status validate(const qg_dot *dots, int n, const qg_pulse *pulse, cons
   if(p->num_timesteps < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_create: num_timesteps < 0");
   if(p->frame != QG_FRAME_ROTATING && p->frame != QG_FRAME_LAB)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown frame %d", p->frame);
-  if(p->precision != QG_PREC_FP64)
-    return qg_fail(QG_ERR_UNSUPPORTED, "qg_create: only QG_PREC_FP64 is built in this handle type");
+  if(p->precision != QG_PREC_FP64 && p->precision != QG_PREC_MIXED)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown precision %d", p->precision);
   if(p->coef_mode == QG_COEF_ON_THE_FLY)
     return qg_fail(QG_ERR_UNSUPPORTED, "qg_create: on-the-fly coefficients use qg_otf_* handles");
   if(p->coef_mode != QG_COEF_AUTO && p->coef_mode != QG_COEF_TABLE)
@@ -314,10 +323,12 @@ static qg_status validate(const qg_dot *dots, int n, const qg_pulse *pulse, cons
   return QG_OK;
 }
 
-// Ordered tile pairs: every unordered pair is stored twice.
-static size_t table_bytes(int nT, int q)
+// Ordered tile pairs: every unordered pair is stored twice.  FP64: q+1
+// complex128 taps; mixed: q+1 complex64 taps and their sum.
+static size_t table_bytes(int nT, int q, bool mixed)
 {
-  return (size_t)nT * nT * kTilePairs * (sizeof(int) + sizeof(double2) * (q + 1));
+  const size_t per = mixed ? sizeof(int) + sizeof(float2) * (q + 2) : sizeof(int) + sizeof(double2) * (q + 1);
+  return (size_t)nT * nT * kTilePairs * per;
 }
 
 // Even, so every ring row starts 32-byte aligned for paired-sample loads.
@@ -339,23 +350,35 @@ static int traj_steps(int n)
 // list (all their taps, read by the dot-step kernels every step) and the near
 // list (tap 0 of the delay-0 pairs, re-read in every corrector iteration),
 // and packs the groups of dots coupled at delay 0 into step blocks.
-static qg_status build_lists(qg_handle *h)
+static qg_status build_lists(qg_handle *h, const TableArgs &ta)
 {
   const int q1 = h->q + 1;
-  const unsigned long long cap = (unsigned long long)std::max<long long>(h->mid_pairs, 1);
+  // pairs with floor delay < K (same delay arithmetic as the table), then
+  // their FP64 coefficients: the mid list is FP64 in both precisions
   int *d_pairs = nullptr;
   double2 *d_mc = nullptr;
-  QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
-  QG_CUDA(cudaMalloc(&d_mc, sizeof(double2) * q1 * cap));
-  QG_CUDA(cudaMemsetAsync(h->d_u64 + 2, 0, sizeof(unsigned long long), h->stream));
-  if(h->mid_pairs > 0)
-    launch_mid_extract(h->d_delay, h->d_coef, h->nT, h->q, d_pairs, d_mc, h->d_u64 + 2, cap, h->stream);
+  unsigned long long cnt = 0;
+  const double c0dt = h->params.c0 * h->params.dt;
+  for(int pass = 0; pass < 2; ++pass) {
+    const unsigned long long cap = pass == 0 ? 0 : std::max<unsigned long long>(cnt, 1);
+    if(pass == 1) {
+      QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
+      QG_CUDA(cudaMalloc(&d_mc, sizeof(double2) * q1 * cap));
+    }
+    QG_CUDA(cudaMemsetAsync(h->d_u64 + 2, 0, sizeof(unsigned long long), h->stream));
+    launch_near_find(h->d_pos, h->d_user, h->n_pad, c0dt, kTimeBlock, d_pairs, h->d_u64 + 2, cap, h->stream);
+    QG_CUDA(cudaGetLastError());
+    QG_CUDA(cudaMemcpyAsync(&cnt, h->d_u64 + 2, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
+    QG_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  h->mid_pairs = (long long)cnt;
+  launch_pair_list_coef(ta, h->q, d_pairs, (long long)cnt, d_mc, h->stream);
+  QG_CUDA(cudaGetLastError());
+  const unsigned long long cap = std::max<unsigned long long>(cnt, 1);
   std::vector<int> pairs(3 * cap);
   std::vector<double2> mc(q1 * cap);
-  QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 3 * cap, cudaMemcpyDeviceToHost,
-                          h->stream));
-  QG_CUDA(cudaMemcpyAsync(mc.data(), d_mc, sizeof(double2) * q1 * cap, cudaMemcpyDeviceToHost,
-                          h->stream));
+  QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 3 * cap, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaMemcpyAsync(mc.data(), d_mc, sizeof(double2) * q1 * cap, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   cudaFree(d_pairs);
   cudaFree(d_mc);
@@ -463,6 +486,10 @@ static qg_status build_lists(qg_handle *h)
 static qg_status reset_state(qg_handle *h)
 {
   QG_CUDA(cudaMemsetAsync(h->d_ring, 0, sizeof(double2) * (size_t)h->n_pad * h->stride, h->stream));
+  if(h->mixed) {
+    QG_CUDA(cudaMemsetAsync(h->d_ring32w, 0, sizeof(float2) * (size_t)h->n_pad * h->stride, h->stream));
+    QG_CUDA(cudaMemsetAsync(h->d_ring32d, 0, sizeof(float2) * (size_t)h->n_pad * h->stride, h->stream));
+  }
   QG_CUDA(cudaMemsetAsync(h->d_partial, 0,
                           sizeof(double2) * (size_t)kTimeBlock * h->nG * h->n_pad, h->stream));
   QG_CUDA(cudaMemsetAsync(h->d_field, 0, sizeof(double2) * (size_t)kTimeBlock * h->n_pad, h->stream));
@@ -505,15 +532,15 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
   unsigned long long cnt = 0;
   for(int pass = 0; pass < 2; ++pass) {
     const unsigned long long cap = pass == 0 ? 0 : std::max<unsigned long long>(cnt, 1);
-    if(pass == 1) QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 2 * cap));
+    if(pass == 1) QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
     QG_CUDA(cudaMemset(d_cnt, 0, sizeof(unsigned long long)));
-    launch_near_find(d_pos, d_user, np0, c0dt, d_pairs, d_cnt, cap, h->stream);
+    launch_near_find(d_pos, d_user, np0, c0dt, 1, d_pairs, d_cnt, cap, h->stream);
     QG_CUDA(cudaGetLastError());
     QG_CUDA(cudaMemcpyAsync(&cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
     QG_CUDA(cudaStreamSynchronize(h->stream));
   }
-  std::vector<int> pairs(2 * std::max<unsigned long long>(cnt, 1));
-  if(cnt) QG_CUDA(cudaMemcpy(pairs.data(), d_pairs, sizeof(int) * 2 * cnt, cudaMemcpyDeviceToHost));
+  std::vector<int> pairs(3 * std::max<unsigned long long>(cnt, 1));
+  if(cnt) QG_CUDA(cudaMemcpy(pairs.data(), d_pairs, sizeof(int) * 3 * cnt, cudaMemcpyDeviceToHost));
   cudaFree(d_pos);
   cudaFree(d_user);
   cudaFree(d_cnt);
@@ -523,8 +550,8 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
   DSU dsu(n);
   std::vector<char> coupled(n, 0);
   for(unsigned long long k = 0; k < cnt; ++k) {
-    dsu.unite(pairs[2 * k], pairs[2 * k + 1]);
-    coupled[pairs[2 * k]] = coupled[pairs[2 * k + 1]] = 1;
+    dsu.unite(pairs[3 * k], pairs[3 * k + 1]);
+    coupled[pairs[3 * k]] = coupled[pairs[3 * k + 1]] = 1;
   }
   std::vector<std::vector<int>> comps;
   {
@@ -643,13 +670,17 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaMemset(h->d_u64, 0, sizeof(unsigned long long) * 4));
 
   // coefficient table
-  const size_t tb = table_bytes(h->nT, h->q);
+  h->mixed = p->precision == QG_PREC_MIXED;
+  const size_t tb = table_bytes(h->nT, h->q, h->mixed);
   size_t free_b = 0, total_b = 0;
   QG_CUDA(cudaMemGetInfo(&free_b, &total_b));
   if(tb > free_b * 0.9)
     return qg_fail(QG_ERR_OOM, "qg_create: coefficient table needs %zu bytes, %zu free", tb, free_b);
   QG_TRY(dalloc(h, &h->d_delay, (size_t)h->nT * h->nT * kTilePairs));
-  QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nT * h->nT * kTilePairs * (h->q + 1)));
+  if(h->mixed)
+    QG_TRY(dalloc(h, &h->d_coef32, (size_t)h->nT * h->nT * kTilePairs * (h->q + 2)));
+  else
+    QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nT * h->nT * kTilePairs * (h->q + 1)));
   TableArgs ta{};
   ta.pos = h->d_pos;
   ta.dip = h->d_dip;
@@ -660,6 +691,8 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   ta.nblk = h->nblk;
   ta.delay = h->d_delay;
   ta.coef = h->d_coef;
+  ta.coef32 = h->d_coef32;
+  ta.mixed = h->mixed ? 1 : 0;
   ta.max_delay = h->d_ints + 5;
   ta.near_count = h->d_u64;
   ta.cp.c0 = p->c0;
@@ -699,6 +732,10 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   h->W = ring_depth(md, h->q);
   h->stride = h->W + kRingMirror;
   QG_TRY(dalloc(h, &h->d_ring, (size_t)h->n_pad * h->stride));
+  if(h->mixed) {
+    QG_TRY(dalloc(h, &h->d_ring32w, (size_t)h->n_pad * h->stride));
+    QG_TRY(dalloc(h, &h->d_ring32d, (size_t)h->n_pad * h->stride));
+  }
   QG_TRY(dalloc(h, &h->d_pcr, (size_t)kPcDepth * 4 * h->n_pad));
   QG_TRY(dalloc(h, &h->d_partial, (size_t)kTimeBlock * h->nG * h->n_pad));
   QG_TRY(dalloc(h, &h->d_field, (size_t)kTimeBlock * h->n_pad));
@@ -713,7 +750,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
     QG_CUDA(cudaEventCreateWithFlags(&h->ev_copy[i], cudaEventDisableTiming));
   }
 
-  QG_TRY(build_lists(h));
+  QG_TRY(build_lists(h, ta));
   QG_TRY(reset_state(h));
   return QG_OK;
 }
@@ -987,7 +1024,7 @@ struct qg_batch_s {
   FarArgs *d_far = nullptr;
   StepArgs *d_step = nullptr;
   int *d_task_off = nullptr, *d_block_off = nullptr;
-  int q = -1, frame = -1, n_time = -1;
+  int q = -1, frame = -1, n_time = -1, mixed = 0;
   int total_tasks = 0, total_blocks = 0;
   int far_grid = 0;
   bool dirty = true;
@@ -1054,10 +1091,12 @@ extern "C" qg_status qg_batch_add(qg_batch *b, qg_handle *h)
   if(h->next_step % kTimeBlock != 0)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: next step %d is not a multiple of %d", h->next_step,
                    kTimeBlock);
-  if(!b->members.empty() && (h->q != b->q || h->params.frame != b->frame || h->w.n_time != b->n_time))
+  if(!b->members.empty() && (h->q != b->q || h->params.frame != b->frame || h->w.n_time != b->n_time ||
+                             (int)h->mixed != b->mixed))
     return qg_fail(QG_ERR_INVALID_ARG,
-                   "qg_batch_add: members must share interpolation order, frame and history width");
+                   "qg_batch_add: members must share interpolation order, frame, history width and precision");
   b->q = h->q;
+  b->mixed = (int)h->mixed;
   b->frame = h->params.frame;
   b->n_time = h->w.n_time;
   // the member's device state must name the next block's first step
@@ -1108,7 +1147,7 @@ static qg_status batch_rebuild(qg_batch *b)
   if(n > 0) {
     cudaGraph_t g;
     QG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->far_grid, b->stream);
+    launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->mixed, b->far_grid, b->stream);
     for(int k = 0; k < kTimeBlock; ++k)
       launch_step_batch(b->d_step, b->d_block_off, n, b->total_blocks, b->n_time, k, b->stream);
     QG_CUDA(cudaStreamEndCapture(b->stream, &g));
@@ -1204,6 +1243,7 @@ extern "C" qg_status qg_history_evaluate(qg_handle *h, int step, const double *r
   if(rho01_step) {
     QG_TRY(upload_io(h, rho01_step));
     launch_ring_write(a, step, h->d_io, h->stream);
+    launch_ring32_rebuild(a, h->stream);
   }
   if(h->eval_cached != step) {
     // the far partials of [step, step + K) in the run's buffer
@@ -1237,6 +1277,7 @@ extern "C" qg_status qg_history_evaluate_noalloc(qg_handle *h, int step, const d
   StepArgs a = h->step_args(true);
   if(d_rho01_step) {
     launch_ring_write(a, step, (const double2 *)d_rho01_step, s);
+    launch_ring32_rebuild(a, s);
     h->eval_cached = -0x7fffffff;
     h->far_block = -0x7fffffff;
   }
@@ -1276,6 +1317,7 @@ extern "C" qg_status qg_set_history(qg_handle *h, int t0, int n, const double *r
     launch_ring_write(a, t0 + k, h->d_io, h->stream);
     QG_CUDA(cudaStreamSynchronize(h->stream));
   }
+  launch_ring32_rebuild(a, h->stream);
   QG_CUDA(cudaGetLastError());
   h->eval_cached = -0x7fffffff;
   h->far_block = -0x7fffffff;
@@ -1308,7 +1350,7 @@ extern "C" qg_status qg_get_info(const qg_handle *h, qg_info *info)
   info->mid_pairs = h->mid_pairs;
   info->time_block = kTimeBlock;
   info->coef_mode = QG_COEF_TABLE;
-  info->precision = QG_PREC_FP64;
+  info->precision = h->mixed ? QG_PREC_MIXED : QG_PREC_FP64;
   info->fused_step = h->fused ? 1 : 0;
   info->device_bytes = h->bytes;
   info->table_build_ms = h->table_ms;
@@ -1323,8 +1365,9 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
   const int q = p->interpolation_order;
   const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
   const int W = ring_depth(md, q);
-  size_t b = table_bytes(nT, q);
-  b += sizeof(double2) * (size_t)n_pad * (W + kRingMirror);
+  const bool mixed = p->precision == QG_PREC_MIXED;
+  size_t b = table_bytes(nT, q, mixed);
+  b += sizeof(double2) * (size_t)n_pad * (W + kRingMirror) * (mixed ? 2 : 1);
   b += sizeof(double2) * (size_t)kPcDepth * 4 * n_pad;
   b += sizeof(double2) * (size_t)kTimeBlock * (nG + 1) * n_pad + sizeof(unsigned) * nT;
   b += sizeof(double2) * (size_t)n_pad * 8;

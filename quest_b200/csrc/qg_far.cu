@@ -203,6 +203,133 @@ __device__ __forceinline__ void far_body(const FarArgs &a, int task)
 //   far_kernel      3 blocks of 4 warps per SM, one sample per load
 //   far_kernel_r4   registers capped for 4 blocks per SM
 //   far_kernel_v2   capped, two samples per 32-byte load
+// ---- mixed precision ---------------------------------------------------------
+// The tap sum of one pair, sum_i c_i w_i, is formed as
+//     (sum_i c_i) w_0 + sum_i c_i (w_i - w_0),
+// w_0 the window's first sample and w_i - w_0 the running sum of the FP32
+// step-to-step differences (themselves computed in FP64).  The large
+// interpolation weights (w1 ~ 1/dt, w2 ~ 1/dt^2) multiply only differences,
+// and sum_i c_i carries no such factor, so FP32 storage loses no more than a
+// few units in the last place of the pair's contribution.
+__device__ __forceinline__ void cfmaf(float2 &acc, float2 c, float2 r)
+{
+  acc.x = fmaf(c.x, r.x, acc.x);
+  acc.x = fmaf(-c.y, r.y, acc.x);
+  acc.y = fmaf(c.x, r.y, acc.y);
+  acc.y = fmaf(c.y, r.x, acc.y);
+}
+
+template <bool LAB>
+__device__ __forceinline__ float2 pref32(float2 r)
+{
+  return LAB ? make_float2(2.f * r.x, 0.f) : r;
+}
+
+template <int Q, bool LAB, int K>
+__device__ __forceinline__ void window_conv_mixed(const float2 *rw, const float2 *rd, int slot0, int tau0,
+                                                  const float2 (&c)[Q + 2], float2 (&acc)[K])
+{
+  const float2 w0 = pref32<LAB>(__ldg(rw + slot0));
+  float2 u = make_float2(0.f, 0.f);
+  if(tau0 >= -kWindow) {
+#pragma unroll
+    for(int k = 0; k < K; ++k) cfmaf(acc[k], c[Q + 1], w0);
+#pragma unroll
+    for(int m = 1; m < K + Q; ++m) {
+      const float2 d = pref32<LAB>(__ldg(rd + slot0 + m));
+      u.x += d.x;
+      u.y += d.y;
+#pragma unroll
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfmaf(acc[k], c[k + Q - m], u);
+    }
+  } else {
+    // early steps: absolute samples, taps before step -22 skipped
+#pragma unroll
+    for(int m = 0; m < K + Q; ++m) {
+      if(m > 0) {
+        const float2 d = pref32<LAB>(__ldg(rd + slot0 + m));
+        u.x += d.x;
+        u.y += d.y;
+      }
+      if(tau0 + m < -kWindow) continue;
+      const float2 w = make_float2(w0.x + u.x, w0.y + u.y);
+#pragma unroll
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfmaf(acc[k], c[k + Q - m], w);
+    }
+  }
+}
+
+template <int Q, bool LAB, int K = kTimeBlock>
+__device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
+{
+  const int lane = threadIdx.x & 31;
+  if(task >= a.nT * a.nG) return;  // uniform per warp
+  const int I = task / a.nG, g = task % a.nG;
+  const int J0 = g * kTileGroup;
+  const int nJ = min(kTileGroup, a.nT - J0);
+  const int t0 = *a.d_t0;
+  if(task == 0 && lane == 0) *a.far_t0_out = t0;
+  const int W = a.W;
+  const int ia = I * kTile + lane;
+
+  float2 acc[K];
+#pragma unroll
+  for(int k = 0; k < K; ++k) acc[k] = make_float2(0.f, 0.f);
+
+  const long long tile0 = (long long)I * a.nT + J0;
+  const int iters = nJ * kTile;
+  int dn = __ldcs(a.delay + tile0 * kTilePairs + lane);
+  float2 cn[Q + 2];
+#pragma unroll
+  for(int i = 0; i <= Q + 1; ++i) cn[i] = __ldcs(a.coef32 + (tile0 * (Q + 2) + i) * kTilePairs + lane);
+  for(int it = 0; it < iters; ++it) {
+    const int d = dn;
+    float2 c[Q + 2];
+#pragma unroll
+    for(int i = 0; i <= Q + 1; ++i) c[i] = cn[i];
+    if(it + 1 < iters) {
+      const long long tile = tile0 + (it + 1) / kTile;
+      const int e = ((it + 1) % kTile) * kTile + lane;
+      dn = __ldcs(a.delay + tile * kTilePairs + e);
+#pragma unroll
+      for(int i = 0; i <= Q + 1; ++i) cn[i] = __ldcs(a.coef32 + (tile * (Q + 2) + i) * kTilePairs + e);
+    }
+    if(d >= kTimeBlock) {
+      const int ib = (J0 + it / kTile) * kTile + (it % kTile);
+      const int tau0 = t0 - d - Q;
+      int slot0 = tau0 % W;
+      if(slot0 < 0) slot0 += W;
+      window_conv_mixed<Q, LAB, K>(a.ring32w + (long long)ib * a.stride, a.ring32d + (long long)ib * a.stride,
+                                   slot0, tau0, c, acc);
+    }
+  }
+
+  // the per-dot sums across groups are carried in FP64
+  const long long gslice = (long long)a.nG * a.n_pad;
+#pragma unroll
+  for(int k = 0; k < K; ++k)
+    a.partial[k * gslice + (long long)g * a.n_pad + ia] = make_double2((double)acc[k].x, (double)acc[k].y);
+  __threadfence();
+  unsigned prev = 0;
+  if(lane == 0) prev = atomicAdd(a.tile_done + I, 1u);
+  prev = __shfl_sync(0xffffffffu, prev, 0);
+  if(prev == (unsigned)(a.nG - 1)) {
+    __threadfence();
+#pragma unroll 1
+    for(int k = 0; k < K; ++k) {
+      double2 f = make_double2(0.0, 0.0);
+      const double2 *P = a.partial + k * gslice + ia;
+      for(int gg = 0; gg < a.nG; ++gg) {
+        const double2 v = __ldcg(P + (long long)gg * a.n_pad);
+        f.x += v.x;
+        f.y += v.y;
+      }
+      a.field[(long long)k * a.n_pad + ia] = f;
+    }
+    if(lane == 0) a.tile_done[I] = 0;
+  }
+}
+
 __device__ __forceinline__ int warp_task() { return blockIdx.x * 4 + (threadIdx.x >> 5); }
 
 template <int Q, bool LAB>
@@ -217,7 +344,7 @@ __global__ void __launch_bounds__(128, 4) far_kernel_v2(FarArgs a) { far_body<Q,
 // ensemble e (prefix sums, task_off[n_ens] = total).  Warps stride over the
 // list; every task writes its own partial slot, so the assignment of tasks to
 // warps does not change any result.
-template <int Q, bool LAB>
+template <int Q, bool LAB, bool MIXED>
 __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restrict__ args,
                                                         const int *__restrict__ task_off, int n_ens)
 {
@@ -232,41 +359,52 @@ __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restric
         hi = mid - 1;
     }
     const FarArgs a = args[lo];
-    far_body<Q, LAB, 0>(a, task - task_off[lo]);
+    if(MIXED)
+      far_body_mixed<Q, LAB>(a, task - task_off[lo]);
+    else
+      far_body<Q, LAB, 0>(a, task - task_off[lo]);
   }
 }
 
-template <bool LAB>
+template <bool LAB, bool MIXED>
 static void launch_far_batch_frame(const FarArgs *args, const int *task_off, int n_ens, int q, int grid,
                                    cudaStream_t s)
 {
   switch(q) {
-    case 1: far_batch_kernel<1, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 2: far_batch_kernel<2, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 3: far_batch_kernel<3, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 4: far_batch_kernel<4, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 5: far_batch_kernel<5, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 6: far_batch_kernel<6, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 7: far_batch_kernel<7, LAB><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 1: far_batch_kernel<1, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 2: far_batch_kernel<2, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 3: far_batch_kernel<3, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 4: far_batch_kernel<4, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 5: far_batch_kernel<5, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 6: far_batch_kernel<6, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 7: far_batch_kernel<7, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
     default: break;
   }
 }
 
-void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int grid,
-                      void *stream)
+void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
+                      int grid, void *stream)
 {
   if(n_ens <= 0) return;
+  cudaStream_t s = (cudaStream_t)stream;
   if(frame == 0)
-    launch_far_batch_frame<false>(args, task_off, n_ens, q, grid, (cudaStream_t)stream);
+    mixed ? launch_far_batch_frame<false, true>(args, task_off, n_ens, q, grid, s)
+          : launch_far_batch_frame<false, false>(args, task_off, n_ens, q, grid, s);
   else
-    launch_far_batch_frame<true>(args, task_off, n_ens, q, grid, (cudaStream_t)stream);
+    mixed ? launch_far_batch_frame<true, true>(args, task_off, n_ens, q, grid, s)
+          : launch_far_batch_frame<true, false>(args, task_off, n_ens, q, grid, s);
 }
+
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128) far_kernel_mixed(FarArgs a) { far_body_mixed<Q, LAB>(a, warp_task()); }
 
 template <int Q, bool LAB>
 static void launch_far_q(const FarArgs &a, cudaStream_t s)
 {
   const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
-  if(a.variant == 1)
+  if(a.mixed)
+    far_kernel_mixed<Q, LAB><<<blocks, 128, 0, s>>>(a);
+  else if(a.variant == 1)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
@@ -345,7 +483,13 @@ qg_status noalloc_scratch(NoAllocScratch *out)
 }
 
 template <int Q, bool LAB>
-__global__ void __launch_bounds__(128) far_kernel_step1(FarArgs a) { far_body<Q, LAB, 0, 1>(a, warp_task()); }
+__global__ void __launch_bounds__(128) far_kernel_step1(FarArgs a)
+{
+  if(a.mixed)
+    far_body_mixed<Q, LAB, 1>(a, warp_task());
+  else
+    far_body<Q, LAB, 0, 1>(a, warp_task());
+}
 
 template <bool LAB>
 static void launch_far1_frame(const FarArgs &a, cudaStream_t s)

@@ -54,7 +54,9 @@ struct TableArgs {
   int n, n_pad, nT;
   long long nblk;
   int *delay;          // [nT][nT][kTilePairs]
-  double2 *coef;       // [nT][nT][q+1][kTilePairs]
+  double2 *coef;       // FP64: [nT][nT][q+1][kTilePairs]
+  float2 *coef32;      // mixed: [nT][nT][q+2][kTilePairs] (taps, then their sum)
+  int mixed;
   int *max_delay;      // atomicMax
   unsigned long long *near_count;  // [0] pairs with delay 0, [1] pairs with delay < K
   CoefParams cp;
@@ -66,6 +68,12 @@ struct FarArgs {
   const int *delay;     // [nT][nT][kTilePairs] ordered tile pairs
   const double2 *coef;  // [nT][nT][q+1][kTilePairs]
   const double2 *ring;  // [n_pad][stride]: rho01 by time slot
+  // mixed precision: FP32 table with the tap sum after the taps, and FP32
+  // rings of rho01 and of its step-to-step differences (computed in FP64)
+  const float2 *coef32;
+  const float2 *ring32w;
+  const float2 *ring32d;
+  int mixed;
   double2 *partial;     // [K][nG][n_pad] per source-tile group
   double2 *field;       // [K][n_pad] far-pair field
   unsigned *tile_done;  // [nT] completion counters (zero between launches)
@@ -95,6 +103,8 @@ struct StepArgs {
   const double2 *mid_coef;  // [entry][q+1]
   double2 *pcr;          // [kPcDepth][4][n_pad]
   double2 *ring;         // [n_pad][stride] rho01 by step slot
+  float2 *ring32w;       // mixed: FP32 rho01 by slot (null in FP64)
+  float2 *ring32d;       // mixed: FP32 rho01(t) - rho01(t-1), differences in FP64
   // current-step coupling: CSR by slot (fused: partner = local slot in the
   // block; general: partner = internal index)
   const int *near_ptr;
@@ -127,19 +137,18 @@ struct NoAllocScratch {
 };
 qg_status noalloc_scratch(NoAllocScratch *out);
 void launch_far_step1(const FarArgs &a, void *stream);
-void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int grid,
-                      void *stream);
+void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
+                      int grid, void *stream);
+void launch_ring32_rebuild(const StepArgs &a, void *stream);
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
                        int k, void *stream);
 
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);
-void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q,
-                        int *out_pairs /*[cap][3] internal a, b, delay*/, double2 *out_coef,
-                        unsigned long long *counter, unsigned long long cap, void *stream);
 void launch_far(const FarArgs &a, void *stream);
-void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int *out_pairs,
+void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int below, int *out_pairs,
                       unsigned long long *counter, unsigned long long cap, void *stream);
+void launch_pair_list_coef(const TableArgs &a, int q, const int *pairs, long long m, double2 *out, void *stream);
 void launch_step_fused(const StepArgs &a, int k, int nblocks, void *stream);
 void launch_step_general(const StepArgs &a, int k, int phase, void *stream);
 void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream);

@@ -158,6 +158,20 @@ __device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, co
   base[3 * a.n_pad] = dr[1];
   const int slot = t % a.W;
   double2 *ring = a.ring + (long long)idx * a.stride;
+  if(a.ring32w) {
+    // mixed precision: FP32 value and FP32 step-to-step difference, the
+    // difference formed in FP64 from the previous step's rho01
+    const double2 prev = ring[ring_slot(t - 1, a.W)];
+    const float2 w = make_float2((float)r[1].x, (float)r[1].y);
+    const float2 d = make_float2((float)(r[1].x - prev.x), (float)(r[1].y - prev.y));
+    float2 *rw = a.ring32w + (long long)idx * a.stride, *rd = a.ring32d + (long long)idx * a.stride;
+    rw[slot] = w;
+    rd[slot] = d;
+    if(slot < kRingMirror) {
+      rw[a.W + slot] = w;
+      rd[a.W + slot] = d;
+    }
+  }
   ring[slot] = r[1];
   if(slot < kRingMirror) ring[a.W + slot] = r[1];
   if(a.traj) {
@@ -552,6 +566,33 @@ __global__ void state_read_kernel(StepArgs a, int t, double2 *rho_user)
 void launch_state_read(const StepArgs &a, int t, double2 *rho_user, void *stream)
 {
   state_read_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, rho_user);
+}
+
+// Mixed precision: the FP32 rings rebuilt from the FP64 ring (after the
+// caller wrote history with qg_set_history).
+__global__ void ring32_rebuild_kernel(StepArgs a)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= (long long)a.n_pad * a.W) return;
+  const int idx = (int)(i / a.W), slot = (int)(i % a.W);
+  const double2 *ring = a.ring + (long long)idx * a.stride;
+  const double2 v = ring[slot], prev = ring[slot == 0 ? a.W - 1 : slot - 1];
+  const float2 w = make_float2((float)v.x, (float)v.y);
+  const float2 d = make_float2((float)(v.x - prev.x), (float)(v.y - prev.y));
+  float2 *rw = a.ring32w + (long long)idx * a.stride, *rd = a.ring32d + (long long)idx * a.stride;
+  rw[slot] = w;
+  rd[slot] = d;
+  if(slot < kRingMirror) {
+    rw[a.W + slot] = w;
+    rd[a.W + slot] = d;
+  }
+}
+
+void launch_ring32_rebuild(const StepArgs &a, void *stream)
+{
+  if(!a.ring32w) return;
+  const long long total = (long long)a.n_pad * a.W;
+  ring32_rebuild_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
 }
 
 }  // namespace qg

@@ -31,7 +31,7 @@ __device__ __forceinline__ void decode_block(long long blk, int &I, int &J)
   J = (int)(blk - r * (r + 1) / 2);
 }
 
-template <int Q>
+template <int Q, bool MIXED>
 __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
 {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -48,14 +48,22 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   const int e1 = lb * kTile + la;  // in (I, J): target a, source b
   const int e2 = la * kTile + lb;  // in (J, I): target b, source a
   int *d1 = a.delay + T1 * kTilePairs + e1, *d2 = a.delay + T2 * kTilePairs + e2;
+  // FP64: q+1 taps; mixed: q+1 taps and their sum, in FP32
   double2 *c1 = a.coef + T1 * (Q + 1) * kTilePairs + e1;
   double2 *c2 = a.coef + T2 * (Q + 1) * kTilePairs + e2;
+  float2 *f1 = a.coef32 + T1 * (Q + 2) * kTilePairs + e1;
+  float2 *f2 = a.coef32 + T2 * (Q + 2) * kTilePairs + e2;
   const bool valid = ia != ib && a.user[ia] >= 0 && a.user[ib] >= 0;
   if(!valid) {
     *d1 = -1;
     *d2 = -1;
+    if(MIXED) {
 #pragma unroll
-    for(int i = 0; i <= Q; ++i) c1[(long long)i * kTilePairs] = c2[(long long)i * kTilePairs] = make_double2(0.0, 0.0);
+      for(int i = 0; i <= Q + 1; ++i) f1[(long long)i * kTilePairs] = f2[(long long)i * kTilePairs] = make_float2(0.f, 0.f);
+    } else {
+#pragma unroll
+      for(int i = 0; i <= Q; ++i) c1[(long long)i * kTilePairs] = c2[(long long)i * kTilePairs] = make_double2(0.0, 0.0);
+    }
     return;
   }
   // reference orientation: src = row = larger user index, obs = col
@@ -74,73 +82,57 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   const int fd = pair_coef_ref<Q>(ps, po, ds, dob, a.cp, coef);
   *d1 = fd;
   *d2 = fd;
+  if(MIXED) {
+    double2 sum = make_double2(0.0, 0.0);
 #pragma unroll
-  for(int i = 0; i <= Q; ++i) c1[(long long)i * kTilePairs] = c2[(long long)i * kTilePairs] = coef[i];
+    for(int i = 0; i <= Q; ++i) {
+      const float2 v = make_float2((float)coef[i].x, (float)coef[i].y);
+      f1[(long long)i * kTilePairs] = f2[(long long)i * kTilePairs] = v;
+      sum.x += coef[i].x;
+      sum.y += coef[i].y;
+    }
+    f1[(long long)(Q + 1) * kTilePairs] = f2[(long long)(Q + 1) * kTilePairs] = make_float2((float)sum.x, (float)sum.y);
+  } else {
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) c1[(long long)i * kTilePairs] = c2[(long long)i * kTilePairs] = coef[i];
+  }
   atomicMax(a.max_delay, fd);
   if(fd == 0) atomicAdd(a.near_count, 1ULL);
   if(fd < kTimeBlock) atomicAdd(a.near_count + 1, 1ULL);
 }
 
-void launch_table_build(const TableArgs &a, int q, void *stream)
+template <bool MIXED>
+static void launch_table_build_p(const TableArgs &a, int q, cudaStream_t s)
 {
   const long long total = a.nblk * kTilePairs;
   const int threads = 128;
   const unsigned blocks = (unsigned)((total + threads - 1) / threads);
-  cudaStream_t s = (cudaStream_t)stream;
   switch(q) {
-    case 1: table_build_kernel<1><<<blocks, threads, 0, s>>>(a); break;
-    case 2: table_build_kernel<2><<<blocks, threads, 0, s>>>(a); break;
-    case 3: table_build_kernel<3><<<blocks, threads, 0, s>>>(a); break;
-    case 4: table_build_kernel<4><<<blocks, threads, 0, s>>>(a); break;
-    case 5: table_build_kernel<5><<<blocks, threads, 0, s>>>(a); break;
-    case 6: table_build_kernel<6><<<blocks, threads, 0, s>>>(a); break;
-    case 7: table_build_kernel<7><<<blocks, threads, 0, s>>>(a); break;
+    case 1: table_build_kernel<1, MIXED><<<blocks, threads, 0, s>>>(a); break;
+    case 2: table_build_kernel<2, MIXED><<<blocks, threads, 0, s>>>(a); break;
+    case 3: table_build_kernel<3, MIXED><<<blocks, threads, 0, s>>>(a); break;
+    case 4: table_build_kernel<4, MIXED><<<blocks, threads, 0, s>>>(a); break;
+    case 5: table_build_kernel<5, MIXED><<<blocks, threads, 0, s>>>(a); break;
+    case 6: table_build_kernel<6, MIXED><<<blocks, threads, 0, s>>>(a); break;
+    case 7: table_build_kernel<7, MIXED><<<blocks, threads, 0, s>>>(a); break;
     default: break;
   }
 }
 
-// Compacts the pairs with floor delay < K (the ones the far-pair kernel
-// leaves to the per-step kernels) into (a, b, delay) + q+1 coefficients, each
-// unordered pair once (tiles I >= J, and a > b inside a diagonal tile); the
-// host sorts them.
-__global__ void mid_extract_kernel(const int *delay, const double2 *coef, int nT, int q,
-                                   int *out_pairs, double2 *out_coef, unsigned long long *counter,
-                                   unsigned long long cap)
+void launch_table_build(const TableArgs &a, int q, void *stream)
 {
-  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if(gid >= (long long)nT * nT * kTilePairs) return;
-  const long long tile = gid / kTilePairs;
-  const int I = (int)(tile / nT), J = (int)(tile % nT);
-  const int e = (int)(gid % kTilePairs);
-  const int l = e % kTile, j = e / kTile;  // target lane, source index
-  if(I < J || (I == J && l <= j)) return;
-  const int d = delay[gid];
-  if(d < 0 || d >= kTimeBlock) return;
-  const unsigned long long slot = atomicAdd(counter, 1ULL);
-  if(slot >= cap) return;
-  out_pairs[3 * slot] = I * kTile + l;
-  out_pairs[3 * slot + 1] = J * kTile + j;
-  out_pairs[3 * slot + 2] = d;
-  for(int i = 0; i <= q; ++i)
-    out_coef[slot * (q + 1) + i] = coef[(tile * (q + 1) + i) * kTilePairs + e];
+  if(a.mixed)
+    launch_table_build_p<true>(a, q, (cudaStream_t)stream);
+  else
+    launch_table_build_p<false>(a, q, (cudaStream_t)stream);
 }
 
-void launch_mid_extract(const int *delay, const double2 *coef, int nT, int q, int *out_pairs,
-                        double2 *out_coef, unsigned long long *counter, unsigned long long cap,
-                        void *stream)
-{
-  const long long total = (long long)nT * nT * kTilePairs;
-  const int threads = 256;
-  const unsigned blocks = (unsigned)((total + threads - 1) / threads);
-  mid_extract_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(delay, coef, nT, q, out_pairs,
-                                                                   out_coef, counter, cap);
-}
-
-// Pairs at floor delay 0, found before the table exists so the dot order can
-// put every group coupled at delay 0 inside one 32-dot step block.  The delay
-// is computed with exactly the operations of pair_coef_ref (reference
+// Pairs with floor delay below `below`: 1 finds the delay-0 pairs before
+// the table exists, so the dot order can put every group coupled at delay 0
+// inside one 32-dot step block; kTimeBlock finds the mid-list pairs.  The
+// delay is computed with exactly the operations of pair_coef_ref (reference
 // orientation, norm, division, modf), so it agrees with the table.
-__global__ void near_find_kernel(const double *pos, const int *user, int n_pad, double c0dt,
+__global__ void near_find_kernel(const double *pos, const int *user, int n_pad, double c0dt, int below,
                                  int *out_pairs, unsigned long long *counter, unsigned long long cap)
 {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -163,21 +155,63 @@ __global__ void near_find_kernel(const double *pos, const int *user, int n_pad, 
   const double nrm = sqrt((dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2]);
   double idelay;
   modf(nrm / c0dt, &idelay);
-  if((int)idelay != 0) return;
+  if((int)idelay >= below) return;
   const unsigned long long slot = atomicAdd(counter, 1ULL);
   if(slot >= cap) return;
-  out_pairs[2 * slot] = ia;
-  out_pairs[2 * slot + 1] = ib;
+  out_pairs[3 * slot] = ia;
+  out_pairs[3 * slot + 1] = ib;
+  out_pairs[3 * slot + 2] = (int)idelay;
 }
 
-void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int *out_pairs,
+// FP64 coefficients of listed pairs (the per-step mid list), computed as the
+// table build computes them.
+template <int Q>
+__global__ void pair_list_coef_kernel(TableArgs a, const int *pairs, long long m, double2 *out)
+{
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= m) return;
+  const int ia = pairs[3 * k], ib = pairs[3 * k + 1];
+  const int ua = a.user[ia], ub = a.user[ib];
+  const int is = ua > ub ? ia : ib, io = ua > ub ? ib : ia;
+  double ps[3], po[3], ds[3], dob[3];
+#pragma unroll
+  for(int c = 0; c < 3; ++c) {
+    ps[c] = a.pos[3 * is + c];
+    po[c] = a.pos[3 * io + c];
+    ds[c] = a.dip[3 * is + c];
+    dob[c] = a.dip[3 * io + c];
+  }
+  double2 coef[Q + 1];
+  pair_coef_ref<Q>(ps, po, ds, dob, a.cp, coef);
+#pragma unroll
+  for(int i = 0; i <= Q; ++i) out[k * (Q + 1) + i] = coef[i];
+}
+
+void launch_pair_list_coef(const TableArgs &a, int q, const int *pairs, long long m, double2 *out, void *stream)
+{
+  if(m <= 0) return;
+  const unsigned blocks = (unsigned)((m + 127) / 128);
+  cudaStream_t s = (cudaStream_t)stream;
+  switch(q) {
+    case 1: pair_list_coef_kernel<1><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    case 2: pair_list_coef_kernel<2><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    case 3: pair_list_coef_kernel<3><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    case 4: pair_list_coef_kernel<4><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    case 5: pair_list_coef_kernel<5><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    case 6: pair_list_coef_kernel<6><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    case 7: pair_list_coef_kernel<7><<<blocks, 128, 0, s>>>(a, pairs, m, out); break;
+    default: break;
+  }
+}
+
+void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int below, int *out_pairs,
                       unsigned long long *counter, unsigned long long cap, void *stream)
 {
   const long long nt = (n_pad + kTile - 1) / kTile;
   const long long total = nt * (nt + 1) / 2 * kTilePairs;
   const int threads = 256;
   near_find_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(
-      pos, user, n_pad, c0dt, out_pairs, counter, cap);
+      pos, user, n_pad, c0dt, below, out_pairs, counter, cap);
 }
 
 }  // namespace qg

@@ -67,7 +67,8 @@ class Result:
 
 class Server:
     def __init__(self, budget_bytes: float = 150e9, capacity: int = 1024, weights=None,
-                 blocks_per_round: int = 1):
+                 blocks_per_round: int = 1, precision: int = capi.PREC_FP64):
+        self.precision = precision
         self.budget = float(budget_bytes)
         self.capacity = capacity
         self.weights = weights if weights is not None else capi.pc_weights()
@@ -79,11 +80,11 @@ class Server:
         self.pair_updates_done = 0.0
 
     def footprint(self, req: Request) -> int:
-        return capi.footprint(req.n, req.constants, req.side())
+        return capi.footprint(req.n, req.constants, req.side(), precision=self.precision)
 
     def _admit(self, req: Request, now: float) -> None:
         fp = self.footprint(req)
-        sim = capi.Simulation(req.dots, req.pulse, req.constants, weights=self.weights)
+        sim = capi.Simulation(req.dots, req.pulse, req.constants, weights=self.weights, precision=self.precision)
         self.batch.add(sim)
         self.running[req.rid] = (req, sim, now, fp)
         self.used += fp

@@ -1,0 +1,90 @@
+"""Mixed precision (FP32 coefficient table, FP32 history values and
+differences, FP64 state, predictor-corrector and per-dot sums) against the
+FP64 path, which matches the oracle to 1e-10.
+
+Tolerance: max |rho_mixed - rho_fp64| / max |rho_fp64| <= 1e-6 for rho00
+and rho01, on workloads where the reference's scheme is stable (dipoles
+2e-4); with dipoles 2e-3 the scheme amplifies any perturbation
+exponentially after excitation (see test_gpu_parity.py), FP32 rounding
+included."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from quest_b200 import capi, inputs as I
+from tests.conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+TOL_MIXED = 1e-6
+
+
+def run(wl, weights, precision, steps):
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=precision) as sim:
+        rho = sim.run(steps)
+        info = sim.info()
+    return rho, info
+
+
+@pytest.mark.parametrize("n,steps", [(300, 400), (1000, 600)])
+def test_mixed_matches_fp64(golden_weights, n, steps):
+    wl = I.plain_small(n=n, steps=steps, pulse_delay=0.15)
+    wl.dots[:, 8] = 2e-4
+    ref, _ = run(wl, golden_weights, capi.PREC_FP64, steps)
+    got, info = run(wl, golden_weights, capi.PREC_MIXED, steps)
+    assert info["precision"] == capi.PREC_MIXED
+    e00 = rel_err(ref[..., 0], got[..., 0])
+    e01 = rel_err(ref[..., 1], got[..., 1])
+    print(f"mixed N={n}: rel err rho00 {e00:.2e} rho01 {e01:.2e}")
+    assert e00 <= TOL_MIXED and e01 <= TOL_MIXED
+
+
+@pytest.mark.slow
+def test_mixed_n4096_against_oracle(golden_weights, oracle_weights):
+    wl = I.plain_table(n=4096, steps=700, pulse_delay=0.3)
+    wl.dots[:, 6:9] *= 0.1
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 700)
+    assert bad is None
+    ref = O.rho_trajectory(hist)
+    got, _ = run(wl, golden_weights, capi.PREC_MIXED, 700)
+    e00 = rel_err(ref[..., 0], got[..., 0])
+    e01 = rel_err(ref[..., 1], got[..., 1])
+    print(f"mixed N=4096 vs oracle: rel err rho00 {e00:.2e} rho01 {e01:.2e}")
+    assert e00 <= TOL_MIXED and e01 <= TOL_MIXED
+
+
+def test_mixed_history_evaluate(golden_weights):
+    wl = I.plain_small(n=150, steps=400)
+    c = wl.constants
+    n = wl.n
+    rng = np.random.default_rng(5)
+    hist = np.zeros((n, 400 + O.WINDOW, 2, 2), dtype=np.complex128)
+    hist[:, :, 0, 1] = rng.normal(size=(n, 400 + O.WINDOW)) + 1j * rng.normal(size=(n, 400 + O.WINDOW))
+    delays, coefs = O.build_table(wl.dots, c)
+    with capi.Simulation(wl.dots, wl.pulse, c, weights=golden_weights, precision=capi.PREC_MIXED) as sim:
+        W = sim.info()["ring_depth"]
+        step = 300
+        lo = step - W + 1
+        sim.set_history(lo, np.ascontiguousarray(hist[:, lo + O.WINDOW: step + O.WINDOW, 0, 1].T))
+        got = sim.history_evaluate(step, hist[:, step + O.WINDOW, 0, 1])
+        ref = O.history_evaluate(wl.dots, c, delays, coefs, hist, step)
+        assert rel_err(ref, got) < 1e-5
+
+
+def test_mixed_batch_equals_solo(golden_weights):
+    specs = [(41, 100, 0.08, 96), (42, 400, 0.15, 160)]
+    ens = []
+    for seed, n, side, steps in specs:
+        d = I.make_dots(n, side, seed, omega_sigma=0.5, dipole=None, dipole_magnitude=2e-4)
+        ens.append((d, I.make_pulse(amplitude=10.0, delay=0.05), I.Constants(num_timesteps=steps)))
+    sims = [capi.Simulation(d, p, c, weights=golden_weights, precision=capi.PREC_MIXED) for d, p, c in ens]
+    batch = capi.Batch(4)
+    for s in sims:
+        batch.add(s)
+    batch.run(10)
+    for (d, p, c), s, spec in zip(ens, sims, specs):
+        with capi.Simulation(d, p, c, weights=golden_weights, precision=capi.PREC_MIXED) as solo:
+            solo.run(spec[3], record=False)
+            np.testing.assert_array_equal(s.state(), solo.state())
+    batch.close()
+    for s in sims:
+        s.close()
