@@ -221,7 +221,7 @@ def config_dict(args):
     return {"workload": f"{args.precision}_table_N{args.n}_T{args.warmup + args.steps}", "N": args.n,
             "steps_total": args.warmup + args.steps, "interpolation_order": 5, "side": 0.2,
             "dt": 1e-3, "c0": 1.0, "hbar": 1.0, "mu0": 1.0, "laser_frequency": 200.0,
-            "pulse_delay": args.pulse_delay, "precision": "fp64", "coef_mode": "table",
+            "pulse_delay": args.pulse_delay, "precision": args.precision, "coef_mode": "table",
             "l2": "inputs larger than L2 (coefficient table %.0f MB > 126 MB)" %
                   (args.n * (args.n - 1) / 2 * TABLE_BYTES_PER_PAIR(5) / 1e6),
             "parallelism": "independent ensemble per GPU" if int(os.environ.get("WORLD_SIZE", "1")) > 1
@@ -312,7 +312,9 @@ def run_ours(args, world, rank, local):
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "steps_per_launch": K,
                      "avg_launch_ms": avg_ms, "share_of_timed_region": pair_ms / ms if ms > 0 else None,
-                     "step_kernels_ms_per_step": step_ms / max(step_launches, 1),
+                     "step_kernels_ms_per_step": step_ms / max(launches * K, 1),
+                     "step_form": {0: "general (12 launches per step)", 1: "fused (1 launch per step)",
+                                   2: "block (1 cooperative launch per 16 steps)"}[info["fused_step"]],
                      "far_variant": args.far_variant,
                      ("fp32" if mixed else "fp64"): {
                          "achieved": fp64_tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": fp64_tf / fp64_peak,
@@ -322,7 +324,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s,
                 "h2d_bytes_per_step": (n * 72 + 80) / total, "d2h_bytes_per_step": n * 32,
                 "includes": "qg_create (dots upload + table build) + qg_run with every step's rho read back"},
-        "gpu_launches": launches + args.steps * (1 if info["fused_step"] else 12),
+        "gpu_launches": launches + step_launches,
         "near_pairs": info["near_pairs"], "mid_pairs": info["mid_pairs"], "max_delay": info["max_delay"],
         "nonfinite_from_step": nonfinite,
         "table_build_ms": info["table_build_ms"],

@@ -221,7 +221,9 @@ typedef struct {
   int time_block;        /* K: steps per pass of the far-pair kernel */
   int coef_mode;         /* resolved qg_coef_mode */
   int precision;         /* qg_precision */
-  int fused_step;        /* 1 when all current-step coupling fits one block */
+  int fused_step;        /* 1 when all current-step coupling fits one block;
+                            2 when, in addition, a whole K-step block runs as
+                            one cooperative launch (all 32-dot blocks resident) */
   size_t device_bytes;   /* device memory held by the handle */
   double table_build_ms; /* time of the coefficient-table kernel */
 } qg_info;
@@ -244,6 +246,9 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * kernels: event nodes inside the block graphs, or around each launch when
  * "graph" is 0),
  * "far_variant" (0..2: resource shape of the far-pair kernel, same results),
+ * "block_step" (1 = the K steps of a block in one cooperative launch, the
+ *   default where every 32-dot block fits on the device at once; 0 = one
+ *   launch per step; same results),
  * "reset" (restart the history at step 0, main.cpp:30-36). */
 qg_status qg_set_option(qg_handle *h, const char *key, int value);
 

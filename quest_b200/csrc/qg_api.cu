@@ -77,7 +77,8 @@ struct qg_handle_s {
   int *d_mid_ptr = nullptr, *d_mid_idx = nullptr, *d_mid_delay = nullptr;  // delay < K pairs
   double2 *d_mid_coef = nullptr;
   // d_ints: 0 step, 1 done, 2 bad, 3 traj_t0, 4 eval_step, 5 max_delay,
-  //         6 far_t0 (run), 7 far block start request, 8 far_t0 (evaluate)
+  //         6 far_t0 (run), 7 far block start request, 8 far_t0 (evaluate),
+  //         12 grid-barrier counter of the step-block kernel
   int *d_ints = nullptr;
   unsigned long long *d_u64 = nullptr;
   double2 *d_traj = nullptr;  // 2 * traj_k steps x N x 2
@@ -88,6 +89,9 @@ struct qg_handle_s {
 
   bool fused = true;
   int step_blocks = 0;
+  // all 16 steps of a block in one cooperative launch (fused form, every
+  // 32-dot block resident at once); otherwise one launch per step
+  bool block_step = false, block_step_ok = false;
   int max_delay = 0;
   long long near_pairs = 0, mid_pairs = 0;
   int far_block = -0x7fffffff;  // first step of the far block the partials hold
@@ -458,6 +462,8 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
     fptr.assign(np + 1, 0);
   }
   h->step_blocks = np / 32;
+  h->block_step_ok = h->fused && h->step_blocks <= step_block_max_blocks();
+  h->block_step = h->block_step_ok;
 
   auto upload_i = [&](int **dst, const std::vector<int> &v) -> qg_status {
     QG_TRY(dalloc(h, dst, v.size()));
@@ -807,6 +813,14 @@ static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, 
   if(eb) record_event(h, eb);
 }
 
+// Steps k0 .. k1-1 of the current block in one cooperative launch.
+static void enqueue_step_block(qg_handle *h, int k0, int k1, bool traj)
+{
+  StepArgs a = h->step_args(false);
+  if(traj) a.traj = h->d_traj;
+  launch_step_block(a, k0, k1, h->step_blocks, reinterpret_cast<unsigned *>(h->d_ints + 12), h->stream);
+}
+
 static void enqueue_dot_step(qg_handle *h, int k, bool traj)
 {
   StepArgs a = h->step_args(!h->fused);
@@ -825,7 +839,10 @@ static qg_status capture_block(qg_handle *h, int traj, int prof, cudaGraphExec_t
   cudaGraph_t g;
   QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   enqueue_far(h, 0, true, prof >= 0 ? h->pev[prof][0] : nullptr, prof >= 0 ? h->pev[prof][1] : nullptr);
-  for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
+  if(h->block_step)
+    enqueue_step_block(h, 0, kTimeBlock, traj != 0);
+  else
+    for(int k = 0; k < kTimeBlock; ++k) enqueue_dot_step(h, k, traj != 0);
   if(prof >= 0) record_event(h, h->pev[prof][2]);
   QG_CUDA(cudaStreamEndCapture(h->stream, &g));
   QG_CUDA(cudaGraphInstantiate(out, g, 0));
@@ -849,7 +866,7 @@ static qg_status collect_prof(qg_handle *h, int i)
   h->pair_ms += far;
   h->pair_launches += 1;
   h->step_ms += steps;
-  h->step_launches += kTimeBlock;
+  h->step_launches += h->block_step ? 1 : kTimeBlock * (h->fused ? 1 : kCorrectorSteps + 2);
   h->pending[i] = false;
   return QG_OK;
 }
@@ -910,7 +927,7 @@ static qg_status collect_events(qg_handle *h, int nev, int nstep)
       cudaEventElapsedTime(&ms, h->ev_c[j], h->ev_d[j]);
       h->step_ms += ms;
     }
-    h->step_launches += nstep;
+    h->step_launches += h->fused ? nstep : nstep * (kCorrectorSteps + 2);
   }
   return QG_OK;
 }
@@ -940,15 +957,20 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
       if(h->profile) ++nev;
       h->far_block = t0;
     }
+    // the rest of this block (or of the run) in one launch when allowed
+    const int span = h->block_step ? std::min(count, t0 + kTimeBlock - t) : 1;
     if(h->profile) cudaEventRecord(h->ev_c[nstep], h->stream);
-    enqueue_dot_step(h, t - t0, traj);
+    if(span > 1)
+      enqueue_step_block(h, t - t0, t - t0 + span, traj);
+    else
+      enqueue_dot_step(h, t - t0, traj);
     if(h->profile) cudaEventRecord(h->ev_d[nstep++], h->stream);
     if(h->profile && (nev == 256 || nstep == 256)) {
       QG_TRY(collect_events(h, nev, nstep));
       nev = nstep = 0;
     }
-    ++t;
-    --count;
+    t += span;
+    count -= span;
   }
   QG_CUDA(cudaGetLastError());
   if(h->profile) {
@@ -1006,6 +1028,8 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   QG_CUDA(cudaStreamSynchronize(h->stream));
   QG_CUDA(cudaGetLastError());
   h->next_step = t_start + n_steps;
+  if(bad == -2)
+    return qg_fail(QG_ERR_CUDA, "qg_run: the step-block kernel's grid barrier timed out");
   if(bad < 0)
     return qg_fail(QG_ERR_CUDA, "qg_run: internal scheduling error (far block or trajectory row)");
   if(bad != kBadNone) {
@@ -1351,7 +1375,7 @@ extern "C" qg_status qg_get_info(const qg_handle *h, qg_info *info)
   info->time_block = kTimeBlock;
   info->coef_mode = QG_COEF_TABLE;
   info->precision = h->mixed ? QG_PREC_MIXED : QG_PREC_FP64;
-  info->fused_step = h->fused ? 1 : 0;
+  info->fused_step = h->fused ? (h->block_step ? 2 : 1) : 0;
   info->device_bytes = h->bytes;
   info->table_build_ms = h->table_ms;
   return QG_OK;
@@ -1403,9 +1427,16 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
   } else if(!std::strcmp(key, "profile")) {
     if(value) QG_TRY(ensure_events(h));
     h->profile = value != 0;
-  } else if(!std::strcmp(key, "far_variant")) {
-    if(value < 0 || value > 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..2");
-    h->far_variant = value;
+  } else if(!std::strcmp(key, "far_variant") || !std::strcmp(key, "block_step")) {
+    if(!std::strcmp(key, "far_variant")) {
+      if(value < 0 || value > 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..2");
+      h->far_variant = value;
+    } else {
+      if(value && !h->block_step_ok)
+        return qg_fail(QG_ERR_UNSUPPORTED, "qg_set_option: block_step needs the fused form with all %d "
+                       "blocks resident", h->step_blocks);
+      h->block_step = value != 0;
+    }
     for(auto &g : h->graph)
       if(g) {
         cudaGraphExecDestroy(g);

@@ -140,6 +140,8 @@ void launch_far_step1(const FarArgs &a, void *stream);
 void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
                       int grid, void *stream);
 void launch_ring32_rebuild(const StepArgs &a, void *stream);
+void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *bar, void *stream);
+int step_block_max_blocks();
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
                        int k, void *stream);
 

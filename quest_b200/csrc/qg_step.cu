@@ -392,6 +392,240 @@ void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, in
     step_batch_kernel<0><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
 }
 
+// ---- one launch for a whole 16-step block ------------------------------------
+// The same step as step_fused_body, repeated for k = k0 .. k1-1 inside one
+// cooperative launch (all blocks resident).  Each block keeps its 32 dots'
+// predictor-corrector window (23 steps of rho and rho-dot) in shared memory,
+// so a step reads only its mid-list partners' history (written by other
+// blocks in the previous step, read through L2).  Steps are separated by a
+// grid barrier: an arrival counter and a bounded wait; a wait that runs out
+// sets *a.d_bad to -2 and the block returns.
+constexpr int kBarrierSpins = 1 << 24;  // x ~64 ns: about a second
+
+__device__ __forceinline__ bool grid_barrier(unsigned *ctr, unsigned target)
+{
+  __syncthreads();
+  int ok = 1;
+  if(threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1u);
+    int spins = 0;
+    while(*(volatile unsigned *)ctr < target) {
+      if(++spins > kBarrierSpins) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  return __syncthreads_and(threadIdx.x == 0 ? ok : 1) != 0;
+}
+
+// mid_entry for the block kernel: partners' history read through L2, since
+// other blocks of the same launch wrote it after this SM may have cached it.
+__device__ __forceinline__ double2 mid_entry_cg(const StepArgs &a, int e, int t)
+{
+  const int q = a.q;
+  const int b = a.mid_idx[e];
+  const int d = a.mid_delay[e];
+  const double2 *c = a.mid_coef + (long long)e * (q + 1);
+  const double2 *ring = a.ring + (long long)b * a.stride;
+  const int s = t - d;
+  const int base = ring_slot(s - q, a.W);
+  double2 M = make_double2(0.0, 0.0);
+#pragma unroll
+  for(int i = 0; i <= kMaxOrder; ++i) {
+    if(i <= q && s - i >= -kWindow && !(d == 0 && i == 0)) {
+      const double2 v = cmul(prefactor(__ldcg(ring + base + q - i), a.frame), c[i]);
+      M.x += v.x;
+      M.y += v.y;
+    }
+  }
+  return M;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(32 * kParts) step_block_kernel(StepArgs a, int k0, int k1, unsigned *bar)
+{
+  constexpr int BS = 32;
+  // 62.5 KB of dynamic shared memory (above the 48 KB static limit)
+  extern __shared__ double2 smem_block[];
+  auto win = reinterpret_cast<double2(*)[4][BS]>(smem_block);  // rho00, rho01, drho00, drho01 by step slot
+  auto red = reinterpret_cast<double2(*)[4][BS]>(smem_block + kPcDepth * 4 * BS);
+  double2 *midv = smem_block + (kPcDepth + kParts) * 4 * BS;
+  double2 *cur = midv + kMidChunk;
+  const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
+  const int blk = blockIdx.x;
+  const int idx = blk * BS + lane;
+  const int t0 = *a.far_t0;
+  const bool live = a.user[idx] >= 0;
+  const int nt = NT > 0 ? NT : a.w.n_time;
+
+  // the integrator's window: all 23 slots of the predictor-corrector ring
+  for(int sl = part; sl < kPcDepth; sl += kParts)
+    for(int c = 0; c < 4; ++c) win[sl][c][lane] = a.pcr[((long long)sl * 4 + c) * a.n_pad + idx];
+  double det = 0, t1 = 1, t2 = 1;
+  if(live) {
+    det = a.laser_freq - a.freq[idx];
+    t1 = a.t1[idx];
+    t2 = a.t2[idx];
+  }
+  const int E0 = a.mid_ptr[blk * BS], E1 = a.mid_ptr[blk * BS + BS];
+  const int my0 = a.mid_ptr[idx], my1 = a.mid_ptr[idx + 1];
+  const int nb0 = a.near_ptr[blk * BS];
+  const bool block_near = a.near_ptr[(blk + 1) * BS] > nb0;
+  const int ne0 = a.near_ptr[idx], ne1 = a.near_ptr[idx + 1];
+  __syncthreads();
+
+  for(int k = k0; k < k1; ++k) {
+    const int t = t0 + k;
+    if(t >= a.T) break;  // uniform: every block stops at the same k
+    if(live) {
+      double2 P0 = make_double2(0.0, 0.0), P1 = P0, H0 = P0, H1 = P0;
+      const double dt = a.dt;
+#pragma unroll
+      for(int h0 = 0; h0 < (NT > 0 ? NT : 32); h0 += kParts) {
+        const int h = h0 + part;
+        if(h < nt) {
+          const int sl = pc_slot(t - nt + h);
+          const double2 x0 = win[sl][0][lane], x1 = win[sl][1][lane], y0 = win[sl][2][lane], y1 = win[sl][3][lane];
+          const double p0 = a.w.ps[h], p1 = a.w.ps[nt + h];
+          const double c0 = a.w.cs[h], c1 = a.w.cs[nt + h];
+          P0.x += x0.x * p0 + (y0.x * p1) * dt;
+          P0.y += x0.y * p0 + (y0.y * p1) * dt;
+          P1.x += x1.x * p0 + (y1.x * p1) * dt;
+          P1.y += x1.y * p0 + (y1.y * p1) * dt;
+          H0.x += x0.x * c0 + (y0.x * c1) * dt;
+          H0.y += x0.y * c0 + (y0.y * c1) * dt;
+          H1.x += x1.x * c0 + (y1.x * c1) * dt;
+          H1.y += x1.y * c0 + (y1.y * c1) * dt;
+        }
+      }
+      red[part][0][lane] = P0;
+      red[part][1][lane] = P1;
+      red[part][2][lane] = H0;
+      red[part][3][lane] = H1;
+    }
+    double2 M = make_double2(0.0, 0.0);
+    for(int c0 = E0; c0 < E1; c0 += kMidChunk) {
+      const int c1 = min(E1, c0 + kMidChunk);
+      for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_entry_cg(a, e, t);
+      __syncthreads();
+      if(part == 0)
+        for(int e = max(my0, c0); e < min(my1, c1); ++e) {
+          M.x += midv[e - c0].x;
+          M.y += midv[e - c0].y;
+        }
+      __syncthreads();
+    }
+    if(E0 == E1) __syncthreads();
+
+    if(part == 0) {
+      double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
+      double pul = 0;
+      if(live) {
+        double2 sum[4];
+#pragma unroll
+        for(int v = 0; v < 4; ++v) {
+          sum[v] = red[0][v][lane];
+#pragma unroll
+          for(int p = 1; p < kParts; ++p) {
+            sum[v].x += red[p][v][lane].x;
+            sum[v].y += red[p][v][lane].y;
+          }
+        }
+        P[0] = sum[0];
+        P[1] = sum[1];
+        H[0] = sum[2];
+        H[1] = sum[3];
+        past = a.far_field[(long long)k * a.n_pad + idx];
+        past.x += M.x;
+        past.y += M.y;
+        pul = pulse_rabi(a, idx, t);
+        r[0] = P[0];
+        r[1] = P[1];
+      }
+      for(int it = 0; it <= kCorrectorSteps; ++it) {
+        if(it > 0 && live) corrector(a, dr, H, r);
+        double2 nf = make_double2(0.0, 0.0);
+        if(block_near) {
+          __syncwarp();
+          cur[lane] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
+          __syncwarp();
+          for(int e = ne0; e < ne1; ++e) {
+            const double2 v = cmul(cur[a.near_idx[e]], a.near_coef[e]);
+            nf.x += v.x;
+            nf.y += v.y;
+          }
+        }
+        if(live) {
+          const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
+          liouville(r[0], r[1], om, t1, t2, det, dr[0], dr[1]);
+        }
+      }
+      if(live) {
+        finish_dot(a, idx, t, r, dr);
+        const int sl = pc_slot(t);
+        win[sl][0][lane] = r[0];
+        win[sl][1][lane] = r[1];
+        win[sl][2][lane] = dr[0];
+        win[sl][3][lane] = dr[1];
+      }
+    }
+    if(k == kTimeBlock - 1 && blk == 0 && threadIdx.x == 0) *a.d_next = t + 1;
+    if(k + 1 < k1 && !grid_barrier(bar, (unsigned)(k - k0 + 1) * gridDim.x)) {
+      if(threadIdx.x == 0) atomicMin(a.d_bad, -2);
+      return;
+    }
+  }
+}
+
+constexpr size_t kStepBlockSmem = sizeof(double2) * ((kPcDepth + kParts) * 4 * 32 + kMidChunk + 32);
+
+static void step_block_attrs()
+{
+  static int dev_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if(dev < 64 && !dev_done[dev]) {
+    cudaFuncSetAttribute(step_block_kernel<22>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStepBlockSmem);
+    cudaFuncSetAttribute(step_block_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStepBlockSmem);
+    dev_done[dev] = 1;
+  }
+}
+
+void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *bar, void *stream)
+{
+  cudaStream_t s = (cudaStream_t)stream;
+  step_block_attrs();
+  cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nblocks);
+  cfg.blockDim = dim3(32 * kParts);
+  cfg.dynamicSmemBytes = kStepBlockSmem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeCooperative;
+  attr.val.cooperative = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  if(a.w.n_time == 22)
+    cudaLaunchKernelEx(&cfg, step_block_kernel<22>, a, k0, k1, bar);
+  else
+    cudaLaunchKernelEx(&cfg, step_block_kernel<0>, a, k0, k1, bar);
+}
+
+int step_block_max_blocks()
+{
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  step_block_attrs();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_block_kernel<22>, 32 * kParts, kStepBlockSmem);
+  return sms * per;
+}
+
 // General form, one launch per phase: phase 0 predicts, phases 1..11 are the
 // 11 evaluations (each followed by a correction except the last).
 // scratch[idx*8 + k]: 0 past field, 1 pulse, 2-3 H, 4-5 rho (even

@@ -60,7 +60,7 @@ def test_small_against_faithful_oracle(golden_weights, oracle_weights):
     hist, bad = O.run_faithful(wl.dots, wl.pulse, wl.constants, oracle_weights, 350)
     assert bad is None
     rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
-    assert info["fused_step"] == 1
+    assert info["fused_step"] == 2
     assert_parity(hist, rho)
     assert np.abs(rho[..., 1]).max() > 1e-6
 
@@ -106,7 +106,7 @@ def test_reference_example_two_dots(golden_weights, oracle_weights):
     hist, bad = O.run_faithful(dots, pulse, c, oracle_weights, c.num_timesteps)
     assert bad is None
     rho, info = gpu_run(dots, pulse, c, golden_weights)
-    assert info["near_pairs"] == 1 and info["fused_step"] == 1
+    assert info["near_pairs"] == 1 and info["fused_step"] == 2
     assert_parity(hist, rho)
 
 
@@ -144,7 +144,7 @@ def test_small_near_groups_fused(golden_weights, oracle_weights):
     hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 400)
     assert bad is None
     rho, info = gpu_run(wl.dots, wl.pulse, wl.constants, golden_weights)
-    assert info["near_pairs"] >= 14 and info["fused_step"] == 1
+    assert info["near_pairs"] >= 14 and info["fused_step"] == 2
     assert_parity(hist, rho)
 
 
@@ -257,9 +257,28 @@ def test_profiling_in_graph_mode_changes_nothing(golden_weights):
         sim.set_option("profile", 1)
         b = sim.run(200)
         far_ms, far_n, step_ms, step_n = sim.kernel_times()
+        block = sim.info()["fused_step"] == 2
     np.testing.assert_array_equal(a, b)
-    assert far_n == 13 and step_n == 200  # 12 graphed 16-step blocks + 8 direct steps
+    # 12 graphed 16-step blocks + 8 direct steps; the block form runs each
+    # block's steps (and the last 8) as one launch
+    assert far_n == 13 and step_n == (13 if block else 200)
     assert far_ms > 0 and step_ms > 0
+
+
+@pytest.mark.parametrize("graph", [1, 0])
+def test_block_step_matches_per_step_launches(golden_weights, graph):
+    """One cooperative launch per 16-step block against one launch per step:
+    same kernels' arithmetic, so bitwise-equal trajectories, including runs
+    that start and stop off a block boundary."""
+    wl = stable_small(300, 200, 0.1)
+    outs = []
+    for block in (0, 1):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+            assert sim.info()["fused_step"] == 2
+            sim.set_option("block_step", block)
+            sim.set_option("graph", graph)
+            outs.append(np.concatenate([sim.run(37), sim.run(100), sim.run(63)]))
+    np.testing.assert_array_equal(outs[0], outs[1])
 
 
 def test_far_kernel_variants_agree_bitwise(golden_weights):
