@@ -76,6 +76,9 @@ struct qg_handle_s {
   double2 *d_gnear_coef = nullptr;
   int *d_mid_ptr = nullptr, *d_mid_idx = nullptr, *d_mid_delay = nullptr;  // delay < K pairs
   double2 *d_mid_coef = nullptr;
+  int *d_new_ptr = nullptr, *d_new_idx = nullptr;  // taps reading step t-1
+  double2 *d_new_coef = nullptr;
+  bool lag = false;  // every delay-0/1 partner shares the dot's 32-dot block
   // d_ints: 0 step, 1 done, 2 bad, 3 traj_t0, 4 eval_step, 5 max_delay,
   //         6 far_t0 (run), 7 far block start request, 8 far_t0 (evaluate),
   //         12 grid-barrier counter of the step-block kernel
@@ -92,6 +95,7 @@ struct qg_handle_s {
   // all 16 steps of a block in one cooperative launch (fused form, every
   // 32-dot block resident at once); otherwise one launch per step
   bool block_step = false, block_step_ok = false;
+  int mid_cache = 0;  // mid-list entries per block kept in shared memory by that kernel
   int max_delay = 0;
   long long near_pairs = 0, mid_pairs = 0;
   int far_block = -0x7fffffff;  // first step of the far block the partials hold
@@ -176,6 +180,11 @@ struct qg_handle_s {
     a.mid_idx = d_mid_idx;
     a.mid_delay = d_mid_delay;
     a.mid_coef = d_mid_coef;
+    a.new_ptr = d_new_ptr;
+    a.new_idx = d_new_idx;
+    a.new_coef = d_new_coef;
+    a.lag = lag ? 1 : 0;
+    a.mid_cache = mid_cache;
     a.pcr = d_pcr;
     a.ring = d_ring;
     a.ring32w = d_ring32w;
@@ -424,6 +433,19 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   for(auto &v : adj)
     std::sort(v.begin(), v.end(), [](const std::pair<int, double2> &x,
                                      const std::pair<int, double2> &y) { return x.first < y.first; });
+  // taps that read step t-1 (delay 1 tap 0, delay 0 tap 1), by dot in mid-list order
+  std::vector<int> nptr(n + 1, 0), nidx;
+  std::vector<double2> ncoef;
+  bool lag = true;
+  for(int i = 0; i < n; ++i) {
+    for(auto &e : mid[i])
+      if(e.d <= 1) {
+        nidx.push_back(e.b);
+        ncoef.push_back(mc[e.k * q1 + (1 - e.d)]);
+        if(e.b / 32 != i / 32) lag = false;
+      }
+    nptr[i + 1] = (int)nidx.size();
+  }
   std::vector<int> gptr(n + 1, 0), gidx;
   std::vector<double2> gcoef;
   for(int i = 0; i < n; ++i) {
@@ -462,7 +484,20 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
     fptr.assign(np + 1, 0);
   }
   h->step_blocks = np / 32;
-  h->block_step_ok = h->fused && h->step_blocks <= step_block_max_blocks();
+  // the step-block kernel: all blocks resident, each with its part of the
+  // mid list in shared memory when that still fits
+  int max_e = 0;
+  for(int b = 0; b < h->step_blocks; ++b) max_e = std::max(max_e, mptr[32 * (b + 1)] - mptr[32 * b]);
+  h->mid_cache = 0;
+  h->block_step_ok = false;
+  if(h->fused) {
+    if(h->step_blocks <= step_block_max_blocks(h->q, max_e)) {
+      h->mid_cache = max_e;
+      h->block_step_ok = true;
+    } else if(h->step_blocks <= step_block_max_blocks(h->q, 0)) {
+      h->block_step_ok = true;
+    }
+  }
   h->block_step = h->block_step_ok;
 
   auto upload_i = [&](int **dst, const std::vector<int> &v) -> qg_status {
@@ -486,6 +521,10 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   QG_TRY(upload_i(&h->d_fnear_ptr, fptr));
   QG_TRY(upload_i(&h->d_fnear_idx, fidx));
   QG_TRY(upload_c(&h->d_fnear_coef, fcoef));
+  QG_TRY(upload_i(&h->d_new_ptr, nptr));
+  QG_TRY(upload_i(&h->d_new_idx, nidx));
+  QG_TRY(upload_c(&h->d_new_coef, ncoef));
+  h->lag = h->fused && lag;
   return QG_OK;
 }
 
@@ -540,7 +579,7 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
     const unsigned long long cap = pass == 0 ? 0 : std::max<unsigned long long>(cnt, 1);
     if(pass == 1) QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
     QG_CUDA(cudaMemset(d_cnt, 0, sizeof(unsigned long long)));
-    launch_near_find(d_pos, d_user, np0, c0dt, 1, d_pairs, d_cnt, cap, h->stream);
+    launch_near_find(d_pos, d_user, np0, c0dt, 2, d_pairs, d_cnt, cap, h->stream);
     QG_CUDA(cudaGetLastError());
     QG_CUDA(cudaMemcpyAsync(&cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
     QG_CUDA(cudaStreamSynchronize(h->stream));
@@ -552,15 +591,22 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
   cudaFree(d_cnt);
   if(d_pairs) cudaFree(d_pairs);
 
-  // groups over Morton positions
-  DSU dsu(n);
-  std::vector<char> coupled(n, 0);
-  for(unsigned long long k = 0; k < cnt; ++k) {
-    dsu.unite(pairs[3 * k], pairs[3 * k + 1]);
-    coupled[pairs[3 * k]] = coupled[pairs[3 * k + 1]] = 1;
-  }
+  // groups over Morton positions: the connected components of the pairs at
+  // floor delay <= 1 when each fits in a block (then the delay-1 partners
+  // share the block too, and the step-block kernel never waits for a step
+  // just finished in another block), else of the delay-0 pairs alone
+  std::vector<char> coupled;
   std::vector<std::vector<int>> comps;
-  {
+  size_t largest = 0;
+  for(int level = 1; level >= 0; --level) {
+    DSU dsu(n);
+    coupled.assign(n, 0);
+    for(unsigned long long k = 0; k < cnt; ++k) {
+      if(pairs[3 * k + 2] > level) continue;
+      dsu.unite(pairs[3 * k], pairs[3 * k + 1]);
+      coupled[pairs[3 * k]] = coupled[pairs[3 * k + 1]] = 1;
+    }
+    comps.clear();
     std::vector<int> root_to_comp(n, -1);
     for(int i = 0; i < n; ++i) {
       if(!coupled[i]) continue;
@@ -571,9 +617,10 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
       }
       comps[root_to_comp[r]].push_back(i);
     }
+    largest = 0;
+    for(auto &c : comps) largest = std::max(largest, c.size());
+    if(largest <= 32) break;
   }
-  size_t largest = 0;
-  for(auto &c : comps) largest = std::max(largest, c.size());
   h->fused = largest <= 32;
   order.clear();
   if(!h->fused || comps.empty()) {

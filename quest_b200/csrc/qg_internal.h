@@ -101,6 +101,14 @@ struct StepArgs {
   const int *mid_idx;
   const int *mid_delay;
   const double2 *mid_coef;  // [entry][q+1]
+  // the mid-list taps that read step t-1 (delay 1 tap 0, delay 0 tap 1): CSR
+  // by internal index, partner (internal index) and coefficient; lag = 1 when
+  // every such partner is in the dot's own 32-dot block
+  const int *new_ptr;
+  const int *new_idx;
+  const double2 *new_coef;
+  int lag;
+  int mid_cache;  // step-block kernel: mid-list entries a block keeps in shared memory
   double2 *pcr;          // [kPcDepth][4][n_pad]
   double2 *ring;         // [n_pad][stride] rho01 by step slot
   float2 *ring32w;       // mixed: FP32 rho01 by slot (null in FP64)
@@ -141,7 +149,7 @@ void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q
                       int grid, void *stream);
 void launch_ring32_rebuild(const StepArgs &a, void *stream);
 void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *bar, void *stream);
-int step_block_max_blocks();
+int step_block_max_blocks(int q, int mid_cache);
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
                        int k, void *stream);
 

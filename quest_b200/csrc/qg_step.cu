@@ -47,35 +47,79 @@ __device__ __forceinline__ double2 prefactor(double2 r, int frame)
   return frame == 0 ? r : make_double2(2 * r.x, 0.0);
 }
 
-__device__ __forceinline__ void liouville(double2 r0, double2 r1, double2 om, double t1, double t2,
-                                          double det, double2 &m0, double2 &m1)
+// x / t given y = 1/t correctly rounded: q0 = x*y, the remainder x - q0*t
+// exact in one fused multiply-add, then q0 + r*y rounded once.  This is
+// Markstein's correction step (P. W. Markstein, IBM J. Res. Develop. 34(1),
+// 1990): with y within half an ulp of 1/t and q0 within one ulp of x/t it
+// returns the correctly rounded quotient, i.e. exactly x / t, barring
+// underflow and overflow.  r == 0 means q0 is exact (and keeps the sign of a
+// zero quotient).  Four independent divisions per evaluation become twelve
+// independent flops instead of four serial division sequences.
+__device__ __forceinline__ double div_by(double x, double t, double y)
+{
+  const double q0 = x * y;
+  const double r = fma(-q0, t, x);
+  return r == 0.0 ? q0 : fma(r, y, q0);
+}
+
+// Per-dot constants of the right-hand side.
+struct DotConst {
+  double det, t1, t2, inv1, inv2;
+};
+
+__device__ __forceinline__ DotConst dot_const(const StepArgs &a, int idx, bool live)
+{
+  DotConst c{0.0, 1.0, 1.0, 1.0, 1.0};
+  if(live) {
+    c.det = a.laser_freq - a.freq[idx];
+    c.t1 = a.t1[idx];
+    c.t2 = a.t2[idx];
+    c.inv1 = 1.0 / c.t1;
+    c.inv2 = 1.0 / c.t2;
+  }
+  return c;
+}
+
+__device__ __forceinline__ void liouville(double2 r0, double2 r1, double2 om, const DotConst &dc, double2 &m0,
+                                          double2 &m1)
 {
   const double2 r1c = make_double2(r1.x, -r1.y), omc = make_double2(om.x, -om.y);
   const double2 mi = make_double2(-0.0, -1.0);  // -iu
   const double2 u = cmul(om, r1c), v = cmul(omc, r1);
   m0 = cmul(mi, make_double2(u.x - v.x, u.y - v.y));
-  m0.x = m0.x - (r0.x - 1.0) / t1;
-  m0.y = m0.y - r0.y / t1;
+  m0.x = m0.x - div_by(r0.x - 1.0, dc.t1, dc.inv1);
+  m0.y = m0.y - div_by(r0.y, dc.t1, dc.inv1);
   const double2 one_m = make_double2(1.0 - 2.0 * r0.x, -(2.0 * r0.y));
   const double2 aa = cmul(om, one_m);
-  const double2 ab = make_double2(aa.x + r1.x * det, aa.y + r1.y * det);
+  const double2 ab = make_double2(aa.x + r1.x * dc.det, aa.y + r1.y * dc.det);
   m1 = cmul(mi, ab);
-  m1.x = m1.x - r1.x / t2;
-  m1.y = m1.y - r1.y / t2;
+  m1.x = m1.x - div_by(r1.x, dc.t2, dc.inv2);
+  m1.y = m1.y - div_by(r1.y, dc.t2, dc.inv2);
 }
 
-__device__ __forceinline__ double pulse_rabi(const StepArgs &a, int idx, int t)
+// The pulse term from a dot's k.r and dipole (pulse_kr, then pulse_at).
+__device__ __forceinline__ double pulse_kr(const StepArgs &a, int idx)
 {
   const double *p = a.pos + 3 * idx;
   const PulseParams &P = a.pulse;
-  const double kr = (P.k[0] * p[0] + P.k[1] * p[1]) + P.k[2] * p[2];
+  return (P.k[0] * p[0] + P.k[1] * p[1]) + P.k[2] * p[2];
+}
+
+__device__ __forceinline__ double pulse_at(const StepArgs &a, double kr, double d0, double d1, double d2, int t)
+{
+  const PulseParams &P = a.pulse;
   const double time = t * a.dt;
   const double arg = kr - P.freq * (time - P.delay);
   const double x = arg / P.width;
   const double g = exp(-(x * x) / 2);
-  const double *d = a.dip + 3 * idx;
   const double e0 = P.amp_pol[0] * g, e1 = P.amp_pol[1] * g, e2 = P.amp_pol[2] * g;
-  return ((e0 * d[0] + e1 * d[1]) + e2 * d[2]) / a.hbar;
+  return ((e0 * d0 + e1 * d1) + e2 * d2) / a.hbar;
+}
+
+__device__ __forceinline__ double pulse_rabi(const StepArgs &a, int idx, int t)
+{
+  const double *d = a.dip + 3 * idx;
+  return pulse_at(a, pulse_kr(a, idx), d[0], d[1], d[2], t);
 }
 
 // Predictor value P and corrector base H (the history part of the
@@ -194,79 +238,227 @@ __device__ __forceinline__ void publish_next_block(const StepArgs &a, int blk, i
   if(k == kTimeBlock - 1 && blk == 0 && threadIdx.x == 0) *a.d_next = t + 1;
 }
 
-// The gathers of one step, split over the 4 warps of a block (32 dots):
-// warp p takes predictor/corrector window slots h = p, p + 4, ... of its
-// lane's dot; the block's mid-list entries (delay < K pairs of all 32 dots)
-// are spread evenly over all 128 threads, each entry's contribution is
-// staged in shared memory and warp 0 adds a dot's entries in list order, so
-// a dot with many close partners does not hold up the block and the sums
-// are deterministic.
-constexpr int kParts = 4;
-constexpr int kMidChunk = 512;  // mid-list entries staged per pass
+// ---- the fused step --------------------------------------------------------------
+// One step for 32 dots per thread block: predictor, 11 evaluations and 10
+// corrections run in warp 0 (lane = dot); dots coupled at delay 0 share the
+// block and exchange their iterates through shared memory after each
+// correction.  The other warps form the step's sums.
+//
+// Summation order, shared by the per-step kernel and the step-block kernel
+// so that both give the same bits:
+//   window sums  P = S123 + T with S123 = (S1 + S2) + S3: S_p adds the
+//                window terms h = p-1, p+2, ... (h <= nt-2) in increasing h
+//                and T is the newest term (h = nt-1, step t-1); H likewise;
+//   past field   (F + M_old) + M_new: F is the far-pair field; M_old adds,
+//                over the dot's mid-list entries in list order, each entry's
+//                taps that read step t-2 or earlier (in tap order); M_new
+//                adds the taps that read step t-1 (delay 1 tap 0, delay 0
+//                tap 1) in new-list order.
+// S_p, F + M_old and the pulse need nothing from step t-1, so the
+// step-block kernel forms them for step t+1 while step t iterates.
+constexpr int kParts = 4;       // warps per block of the per-step kernel
+constexpr int kMidChunk = 384;  // mid-list entries staged per pass
 
-template <int NT>
-__device__ __forceinline__ void pc_part(const StepArgs &a, int idx, int t, int part, double2 (&out)[4])
+// Window term h (step t - nt + h) of one dot added to acc = {P0, P1, H0, H1};
+// ps, cs: the predictor and corrector weights (kernel parameters or a copy
+// in shared memory).
+__device__ __forceinline__ void pc_term(const StepArgs &a, const double *ps, const double *cs, int nt, int h,
+                                        double2 x0, double2 x1, double2 y0, double2 y1, double2 (&acc)[4])
 {
-  double2 P0 = make_double2(0.0, 0.0), P1 = P0, H0 = P0, H1 = P0;
-  const int nt = NT > 0 ? NT : a.w.n_time;
   const double dt = a.dt;
-#pragma unroll
-  for(int h0 = 0; h0 < (NT > 0 ? NT : 32); h0 += kParts) {
-    const int h = h0 + part;
-    if(h < nt) {
-      const int s = pc_slot(t - nt + h);
-      const double2 *base = a.pcr + (long long)s * 4 * a.n_pad + idx;
-      const double2 x0 = base[0], x1 = base[a.n_pad], y0 = base[2 * a.n_pad], y1 = base[3 * a.n_pad];
-      const double p0 = a.w.ps[h], p1 = a.w.ps[nt + h];
-      const double c0 = a.w.cs[h], c1 = a.w.cs[nt + h];
-      P0.x += x0.x * p0 + (y0.x * p1) * dt;
-      P0.y += x0.y * p0 + (y0.y * p1) * dt;
-      P1.x += x1.x * p0 + (y1.x * p1) * dt;
-      P1.y += x1.y * p0 + (y1.y * p1) * dt;
-      H0.x += x0.x * c0 + (y0.x * c1) * dt;
-      H0.y += x0.y * c0 + (y0.y * c1) * dt;
-      H1.x += x1.x * c0 + (y1.x * c1) * dt;
-      H1.y += x1.y * c0 + (y1.y * c1) * dt;
-    }
-  }
-  out[0] = P0;
-  out[1] = P1;
-  out[2] = H0;
-  out[3] = H1;
+  const double p0 = ps[h], p1 = ps[nt + h];
+  const double c0 = cs[h], c1 = cs[nt + h];
+  acc[0].x += x0.x * p0 + (y0.x * p1) * dt;
+  acc[0].y += x0.y * p0 + (y0.y * p1) * dt;
+  acc[1].x += x1.x * p0 + (y1.x * p1) * dt;
+  acc[1].y += x1.y * p0 + (y1.y * p1) * dt;
+  acc[2].x += x0.x * c0 + (y0.x * c1) * dt;
+  acc[2].y += x0.y * c0 + (y0.y * c1) * dt;
+  acc[3].x += x1.x * c0 + (y1.x * c1) * dt;
+  acc[3].y += x1.y * c0 + (y1.y * c1) * dt;
 }
 
-// One mid-list entry at step t: taps before step -22 skipped, the
-// (delay 0, tap 0) term left to the near list.
-__device__ __forceinline__ double2 mid_entry(const StepArgs &a, int e, int t)
+// Window sources: the predictor-corrector ring in HBM, or a block's copy of
+// it in shared memory ([slot][rho00, rho01, drho00, drho01][lane]).
+struct PcrWindow {
+  const double2 *pcr;
+  int n_pad, idx;
+  __device__ __forceinline__ double2 operator()(int slot, int c) const
+  {
+    return pcr[((long long)slot * 4 + c) * n_pad + idx];
+  }
+};
+struct SmemWindow {
+  const double2 (*win)[4][32];
+  int lane;
+  __device__ __forceinline__ double2 operator()(int slot, int c) const { return win[slot][c][lane]; }
+};
+
+// S_p (p = 1, 2, 3) of the window sums of step t.
+template <int NT, class Win>
+__device__ __forceinline__ void pc_partial(const StepArgs &a, const double *ps, const double *cs, int t, int p,
+                                           const Win &win, double2 (&acc)[4])
+{
+  const int nt = NT > 0 ? NT : a.w.n_time;
+#pragma unroll
+  for(int v = 0; v < 4; ++v) acc[v] = make_double2(0.0, 0.0);
+#pragma unroll
+  for(int h0 = 0; h0 < (NT > 0 ? NT : 32); h0 += 3) {
+    const int h = h0 + p - 1;
+    if(h <= nt - 2) {
+      const int s = pc_slot(t - nt + h);
+      pc_term(a, ps, cs, nt, h, win(s, 0), win(s, 1), win(s, 2), win(s, 3), acc);
+    }
+  }
+}
+
+// T: the newest window term of step t (step t-1).
+template <class Win>
+__device__ __forceinline__ void pc_newest(const StepArgs &a, const double *ps, const double *cs, int t, int nt,
+                                          const Win &win, double2 (&acc)[4])
+{
+#pragma unroll
+  for(int v = 0; v < 4; ++v) acc[v] = make_double2(0.0, 0.0);
+  const int s = pc_slot(t - 1);
+  pc_term(a, ps, cs, nt, nt - 1, win(s, 0), win(s, 1), win(s, 2), win(s, 3), acc);
+}
+
+// The taps of a mid-list entry at step t that read step t-2 or earlier
+// (taps before step -22 skipped): partner b, delay d < W - q, coefficients
+// c[0..q], tslot = ring_slot(t).  All the taps are fetched before any is
+// used, so their loads are in flight together.  CG: loads through L2 only
+// (the data may have been written by another block since this SM last read
+// the line); otherwise ordinary loads, for callers whose acquire of the
+// writers' release already covers them.
+template <bool CG>
+__device__ __forceinline__ void mid_old_fetch(const StepArgs &a, int b, int d, int t, int tslot,
+                                              double2 (&v)[kMaxOrder + 1])
 {
   const int q = a.q;
-  const int b = a.mid_idx[e];
-  const int d = a.mid_delay[e];
-  const double2 *c = a.mid_coef + (long long)e * (q + 1);
   const double2 *ring = a.ring + (long long)b * a.stride;
   const int s = t - d;
-  const int base = ring_slot(s - q, a.W);  // tap i at base + q - i (mirrored)
+  int base = tslot - d - q;  // slot of step s - q; tap i at base + q - i (mirrored)
+  if(base < 0) base += a.W;
+#pragma unroll
+  for(int i = 0; i <= kMaxOrder; ++i) {
+    const bool use = i <= q && s - i >= -kWindow && d + i >= 2;
+    v[i] = make_double2(0.0, 0.0);
+    if(use) v[i] = CG ? __ldcg(ring + base + q - i) : ring[base + q - i];
+  }
+}
+
+__device__ __forceinline__ double2 mid_old_sum(const StepArgs &a, int d, int t, const double2 *c,
+                                               const double2 (&v)[kMaxOrder + 1])
+{
+  const int q = a.q;
+  const int s = t - d;
   double2 M = make_double2(0.0, 0.0);
 #pragma unroll
   for(int i = 0; i <= kMaxOrder; ++i) {
-    if(i <= q && s - i >= -kWindow && !(d == 0 && i == 0)) {
-      const double2 v = cmul(prefactor(ring[base + q - i], a.frame), c[i]);
-      M.x += v.x;
-      M.y += v.y;
+    if(i <= q && s - i >= -kWindow && d + i >= 2) {
+      const double2 w = cmul(prefactor(v[i], a.frame), c[i]);
+      M.x += w.x;
+      M.y += w.y;
     }
   }
   return M;
 }
 
-// Fused step for 32 dots per block, 128 threads: the gathers in parallel,
-// then warp 0 runs predictor, 11 evaluations and 10 corrections; dots
-// coupled at delay 0 share the block and exchange their iterates through
-// shared memory after each correction.
+__device__ __forceinline__ double2 mid_old(const StepArgs &a, int e, int t, int tslot)
+{
+  const int d = a.mid_delay[e];
+  double2 v[kMaxOrder + 1];
+  mid_old_fetch<true>(a, a.mid_idx[e], d, t, tslot, v);
+  return mid_old_sum(a, d, t, a.mid_coef + (long long)e * (a.q + 1), v);
+}
+
+// M_new of dot idx; prev(b) = rho01 of partner b at step t-1.
+template <class Prev>
+__device__ __forceinline__ double2 mid_new(const StepArgs &a, int idx, const Prev &prev)
+{
+  double2 M = make_double2(0.0, 0.0);
+  for(int j = a.new_ptr[idx]; j < a.new_ptr[idx + 1]; ++j) {
+    const double2 v = cmul(prefactor(prev(a.new_idx[j]), a.frame), a.new_coef[j]);
+    M.x += v.x;
+    M.y += v.y;
+  }
+  return M;
+}
+
+// A dot's delay-0 partners (slot in the block, tap-0 coefficient): the first
+// kNearRegs in registers, any further ones read from the list.
+constexpr int kNearRegs = 2;
+struct NearRegs {
+  int e0, e1;
+  int idx[kNearRegs];
+  double2 coef[kNearRegs];
+};
+
+__device__ __forceinline__ NearRegs near_regs(const StepArgs &a, int idx)
+{
+  NearRegs n;
+  n.e0 = a.near_ptr[idx];
+  n.e1 = a.near_ptr[idx + 1];
+#pragma unroll
+  for(int j = 0; j < kNearRegs; ++j) {
+    const bool has = n.e0 + j < n.e1;
+    n.idx[j] = has ? a.near_idx[n.e0 + j] : 0;
+    n.coef[j] = has ? a.near_coef[n.e0 + j] : make_double2(0.0, 0.0);
+  }
+  return n;
+}
+
+// Predictor, 11 evaluations and 10 corrections of one dot (warp 0, lane =
+// dot); the delay-0 partners' iterates are exchanged through cur[].
+__device__ __forceinline__ void dot_iterate(const StepArgs &a, bool live, bool block_near, const NearRegs &nr,
+                                            double2 *cur, int lane, const double2 (&P)[2], const double2 (&H)[2],
+                                            double2 past, double pul, const DotConst &dc, double2 (&r)[2],
+                                            double2 (&dr)[2])
+{
+  r[0] = P[0];
+  r[1] = P[1];
+  for(int it = 0; it <= kCorrectorSteps; ++it) {
+    if(it > 0 && live) corrector(a, dr, H, r);
+    double2 nf = make_double2(0.0, 0.0);
+    if(block_near) {
+      __syncwarp();
+      cur[lane] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
+      __syncwarp();
+#pragma unroll
+      for(int j = 0; j < kNearRegs; ++j)
+        if(nr.e0 + j < nr.e1) {
+          const double2 v = cmul(cur[nr.idx[j]], nr.coef[j]);
+          nf.x += v.x;
+          nf.y += v.y;
+        }
+      for(int e = nr.e0 + kNearRegs; e < nr.e1; ++e) {
+        const double2 v = cmul(cur[a.near_idx[e]], a.near_coef[e]);
+        nf.x += v.x;
+        nf.y += v.y;
+      }
+    }
+    if(live) {
+      const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
+      liouville(r[0], r[1], om, dc, dr[0], dr[1]);
+    }
+  }
+}
+
+// P = S123 + T, H likewise.
+__device__ __forceinline__ void pc_combine(const double2 (&S)[4], const double2 (&T)[4], double2 (&P)[2],
+                                           double2 (&H)[2])
+{
+  P[0] = make_double2(S[0].x + T[0].x, S[0].y + T[0].y);
+  P[1] = make_double2(S[1].x + T[1].x, S[1].y + T[1].y);
+  H[0] = make_double2(S[2].x + T[2].x, S[2].y + T[2].y);
+  H[1] = make_double2(S[3].x + T[3].x, S[3].y + T[3].y);
+}
+
 template <int NT>
 __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int k)
 {
   constexpr int BS = 32;
-  __shared__ double2 red[kParts][4][BS];
+  __shared__ double2 red[3][4][BS];
   __shared__ double2 midv[kMidChunk];
   __shared__ double2 cur[BS];
   const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
@@ -274,84 +466,61 @@ __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int 
   const int t = *a.far_t0 + k;
   if(t >= a.T) return;  // past this ensemble's last step (uniform per block)
   const bool live = a.user[idx] >= 0;
+  const int nt = NT > 0 ? NT : a.w.n_time;
+  const PcrWindow win{a.pcr, a.n_pad, idx};
 
-  // warp 0's per-dot inputs, requested before the gathers complete
-  double2 past = make_double2(0.0, 0.0);
-  double det = 0, t1 = 1, t2 = 1, pul = 0;
-  if(part == 0 && live) {
-    past = a.far_field[(long long)k * a.n_pad + idx];
-    pul = pulse_rabi(a, idx, t);
-    det = a.laser_freq - a.freq[idx];
-    t1 = a.t1[idx];
-    t2 = a.t2[idx];
-  }
-  if(live) {
-    double2 out[4];
-    pc_part<NT>(a, idx, t, part, out);
+  // warp 0's inputs, requested before the gathers complete
+  double2 F = make_double2(0.0, 0.0), Mn = F, T[4];
+  double pul = 0;
+  DotConst dc{};
+  if(part == 0) {
+    dc = dot_const(a, idx, live);
+    if(live) {
+      F = a.far_field[(long long)k * a.n_pad + idx];
+      pul = pulse_rabi(a, idx, t);
+      pc_newest(a, a.w.ps, a.w.cs, t, nt, win, T);
+      const int slot = ring_slot(t - 1, a.W);
+      Mn = mid_new(a, idx, [&](int b) { return __ldcg(a.ring + (long long)b * a.stride + slot); });
+    }
+  } else if(live) {
+    double2 S[4];
+    pc_partial<NT>(a, a.w.ps, a.w.cs, t, part, win, S);
 #pragma unroll
-    for(int v = 0; v < 4; ++v) red[part][v][lane] = out[v];
+    for(int v = 0; v < 4; ++v) red[part - 1][v][lane] = S[v];
   }
 
-  // mid list of the block's 32 dots: CSR range [E0, E1)
+  // mid list of the block's 32 dots, CSR range [E0, E1): entries staged by
+  // all threads, added per dot in list order by warp 0
   const int E0 = a.mid_ptr[blk * BS], E1 = a.mid_ptr[blk * BS + BS];
   const int my0 = a.mid_ptr[idx], my1 = a.mid_ptr[idx + 1];
-  double2 M = make_double2(0.0, 0.0);
+  double2 Mo = make_double2(0.0, 0.0);
+  const int tslot = ring_slot(t, a.W);
   for(int c0 = E0; c0 < E1; c0 += kMidChunk) {
     const int c1 = min(E1, c0 + kMidChunk);
-    for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_entry(a, e, t);
+    for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_old(a, e, t, tslot);
     __syncthreads();
     if(part == 0)
       for(int e = max(my0, c0); e < min(my1, c1); ++e) {
-        M.x += midv[e - c0].x;
-        M.y += midv[e - c0].y;
+        Mo.x += midv[e - c0].x;
+        Mo.y += midv[e - c0].y;
       }
     __syncthreads();
   }
   if(E0 == E1) __syncthreads();  // the window partials are complete
 
   if(part == 0) {
-    const int nb0 = a.near_ptr[blk * BS];
-    const bool block_near = a.near_ptr[(blk + 1) * BS] > nb0;
-    double2 P[2], H[2], r[2], dr[2];
+    const bool block_near = a.near_ptr[(blk + 1) * BS] > a.near_ptr[blk * BS];
+    double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
     if(live) {
-      double2 sum[4];
+      double2 S[4];
 #pragma unroll
-      for(int v = 0; v < 4; ++v) {
-        sum[v] = red[0][v][lane];
-#pragma unroll
-        for(int p = 1; p < kParts; ++p) {
-          sum[v].x += red[p][v][lane].x;
-          sum[v].y += red[p][v][lane].y;
-        }
-      }
-      P[0] = sum[0];
-      P[1] = sum[1];
-      H[0] = sum[2];
-      H[1] = sum[3];
-      past.x += M.x;
-      past.y += M.y;
-      r[0] = P[0];
-      r[1] = P[1];
+      for(int v = 0; v < 4; ++v)
+        S[v] = make_double2((red[0][v][lane].x + red[1][v][lane].x) + red[2][v][lane].x,
+                            (red[0][v][lane].y + red[1][v][lane].y) + red[2][v][lane].y);
+      pc_combine(S, T, P, H);
+      past = make_double2((F.x + Mo.x) + Mn.x, (F.y + Mo.y) + Mn.y);
     }
-    const int e0 = a.near_ptr[idx], e1 = a.near_ptr[idx + 1];
-    for(int it = 0; it <= kCorrectorSteps; ++it) {
-      if(it > 0 && live) corrector(a, dr, H, r);
-      double2 nf = make_double2(0.0, 0.0);
-      if(block_near) {
-        __syncwarp();
-        cur[lane] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
-        __syncwarp();
-        for(int e = e0; e < e1; ++e) {
-          const double2 v = cmul(cur[a.near_idx[e]], a.near_coef[e]);
-          nf.x += v.x;
-          nf.y += v.y;
-        }
-      }
-      if(live) {
-        const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
-        liouville(r[0], r[1], om, t1, t2, det, dr[0], dr[1]);
-      }
-    }
+    dot_iterate(a, live, block_near, near_regs(a, idx), cur, lane, P, H, past, pul, dc, r, dr);
     if(live) finish_dot(a, idx, t, r, dr);
   }
   publish_next_block(a, blk, k, t);
@@ -393,217 +562,303 @@ void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, in
 }
 
 // ---- one launch for a whole 16-step block ------------------------------------
-// The same step as step_fused_body, repeated for k = k0 .. k1-1 inside one
-// cooperative launch (all blocks resident).  Each block keeps its 32 dots'
-// predictor-corrector window (23 steps of rho and rho-dot) in shared memory,
-// so a step reads only its mid-list partners' history (written by other
-// blocks in the previous step, read through L2).  Steps are separated by a
-// grid barrier: an arrival counter and a bounded wait; a wait that runs out
-// sets *a.d_bad to -2 and the block returns.
-constexpr int kBarrierSpins = 1 << 24;  // x ~64 ns: about a second
+// The steps k0 .. k1-1 of a block in one cooperative launch (every thread
+// block resident), 8 warps per 32 dots.  Each block keeps in shared memory
+// its dots' predictor-corrector window (23 steps of rho and rho-dot), the
+// integrator weights and, when it fits, its part of the mid list.  Warp 0
+// runs step k while warps 1-7 form step k+1's window partials S_p, F + M_old
+// and pulse (double-buffered in shared memory).  M_old reads the partners'
+// history of step k-1 and earlier, so warps 1-7 first wait until every block
+// has finished step k-1.  Blocks count finished steps on one device-wide
+// arrival counter; a block's helper warps post its step k-1 at the start of
+// step k (after the block barrier that follows warp 0's stores), so warp 0
+// never waits on the fence.
+//
+// M_new reads step k-1 of the delay-0/1 partners: with a.lag set every such
+// partner is in the dot's own block and its value comes from shared memory,
+// so no block waits for a step just finished elsewhere (blocks may run one
+// step apart); otherwise warp 0 also waits for every block's step k-1.
+// Every wait is bounded (about a second); a wait that runs out sets
+// *a.d_bad to -2 and the kernel returns.
+constexpr int kBlockWarps = 8;
+constexpr int kHelpers = 32 * (kBlockWarps - 1);  // threads of warps 1..7
+constexpr int kBarrierSpins = 1 << 24;            // x ~64 ns of sleep: about a second
+constexpr int kWeightSlots = 64;                  // 2 x n_time, n_time <= 32
 
-__device__ __forceinline__ bool grid_barrier(unsigned *ctr, unsigned target)
+// Waits until *ctr >= target (thread-level; acquire on success).
+__device__ __forceinline__ bool wait_count(const unsigned *ctr, unsigned target)
 {
-  __syncthreads();
-  int ok = 1;
-  if(threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(ctr, 1u);
-    int spins = 0;
-    while(*(volatile unsigned *)ctr < target) {
-      if(++spins > kBarrierSpins) {
-        ok = 0;
-        break;
-      }
-      __nanosleep(64);
-    }
-    __threadfence();
+  int spins = 0;
+  while(*(volatile const unsigned *)ctr < target) {
+    if(++spins > kBarrierSpins) return false;
+    __nanosleep(64);
   }
-  return __syncthreads_and(threadIdx.x == 0 ? ok : 1) != 0;
+  __threadfence();
+  return true;
 }
 
-// mid_entry for the block kernel: partners' history read through L2, since
-// other blocks of the same launch wrote it after this SM may have cached it.
-__device__ __forceinline__ double2 mid_entry_cg(const StepArgs &a, int e, int t)
+__device__ __forceinline__ void helpers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kHelpers)); }
+
+// S_p of either the predictor sums (HQ = false: rho00, rho01) or the
+// corrector sums (HQ = true), each accumulator with the same operations as
+// pc_partial.
+template <int NT, bool HQ, class Win>
+__device__ __forceinline__ void pc_partial_half(const StepArgs &a, const double *ps, const double *cs, int t, int p,
+                                                const Win &win, double2 (&acc)[2])
 {
-  const int q = a.q;
-  const int b = a.mid_idx[e];
-  const int d = a.mid_delay[e];
-  const double2 *c = a.mid_coef + (long long)e * (q + 1);
-  const double2 *ring = a.ring + (long long)b * a.stride;
-  const int s = t - d;
-  const int base = ring_slot(s - q, a.W);
-  double2 M = make_double2(0.0, 0.0);
+  const int nt = NT > 0 ? NT : a.w.n_time;
+  const double dt = a.dt;
+  acc[0] = acc[1] = make_double2(0.0, 0.0);
 #pragma unroll
-  for(int i = 0; i <= kMaxOrder; ++i) {
-    if(i <= q && s - i >= -kWindow && !(d == 0 && i == 0)) {
-      const double2 v = cmul(prefactor(__ldcg(ring + base + q - i), a.frame), c[i]);
-      M.x += v.x;
-      M.y += v.y;
+  for(int h0 = 0; h0 < (NT > 0 ? NT : 32); h0 += 3) {
+    const int h = h0 + p - 1;
+    if(h <= nt - 2) {
+      const int s = pc_slot(t - nt + h);
+      const double2 x0 = win(s, 0), x1 = win(s, 1), y0 = win(s, 2), y1 = win(s, 3);
+      const double w0 = HQ ? cs[h] : ps[h], w1 = HQ ? cs[nt + h] : ps[nt + h];
+      acc[0].x += x0.x * w0 + (y0.x * w1) * dt;
+      acc[0].y += x0.y * w0 + (y0.y * w1) * dt;
+      acc[1].x += x1.x * w0 + (y1.x * w1) * dt;
+      acc[1].y += x1.y * w0 + (y1.y * w1) * dt;
     }
   }
-  return M;
+}
+
+// Shared-memory layout of the step-block kernel.
+struct BlockSmem {
+  double2 (*win)[4][32];  // [kPcDepth][4][32]
+  double2 *pre_s;         // [2][3][4][32] S_p
+  double2 *pre_f;         // [2][32] F + M_old
+  double2 *midv;          // [kMidChunk] staged entries
+  double2 *cur;           // [32] delay-0 exchange
+  double2 *prev01;        // [32] rho01 of step t-1
+  double *pre_p;          // [2][32] pulse
+  double *ps, *cs;        // [kWeightSlots] each
+  double *pk;             // [4][32] k.r and the dipole, for the pulse
+  double2 *mc_coef;       // [mid_cache][q+1] the block's mid-list coefficients
+  int *mc_idx, *mc_del;   // [mid_cache] partners and delays
+};
+
+__host__ __device__ __forceinline__ size_t block_smem_bytes(int q, int mid_cache)
+{
+  return sizeof(double2) * ((size_t)kPcDepth * 4 * 32 + 2 * 3 * 4 * 32 + 2 * 32 + kMidChunk + 32 + 32 +
+                            (size_t)mid_cache * (q + 1)) +
+         sizeof(double) * (2 * 32 + 2 * kWeightSlots + 4 * 32) + sizeof(int) * 2 * (size_t)mid_cache;
+}
+
+__device__ __forceinline__ BlockSmem block_smem(double2 *base, int q, int mid_cache)
+{
+  BlockSmem m;
+  m.win = reinterpret_cast<double2(*)[4][32]>(base);
+  m.pre_s = base + kPcDepth * 4 * 32;
+  m.pre_f = m.pre_s + 2 * 3 * 4 * 32;
+  m.midv = m.pre_f + 2 * 32;
+  m.cur = m.midv + kMidChunk;
+  m.prev01 = m.cur + 32;
+  m.mc_coef = m.prev01 + 32;
+  m.pre_p = reinterpret_cast<double *>(m.mc_coef + (size_t)mid_cache * (q + 1));
+  m.ps = m.pre_p + 2 * 32;
+  m.cs = m.ps + kWeightSlots;
+  m.pk = m.cs + kWeightSlots;
+  m.mc_idx = reinterpret_cast<int *>(m.pk + 4 * 32);
+  m.mc_del = m.mc_idx + mid_cache;
+  return m;
+}
+
+// Step k's sums by warps 1..7 into buffer `b`: pre_s[b][p-1][v][lane] = S_p
+// of quantity v, pre_f[b] = F + M_old, pre_p[b] = pulse.
+template <int NT>
+__device__ __forceinline__ void block_precompute(const StepArgs &a, const BlockSmem &m, int blk, int k, int t,
+                                                 int b, bool cached)
+{
+  constexpr int BS = 32;
+  const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
+  const int tid = threadIdx.x - 32;
+  const int idx = blk * BS + lane;
+  const bool live = a.user[idx] >= 0;
+  double2 F = make_double2(0.0, 0.0);
+  double pul = 0;
+  if(part == 1 && live) {
+    F = a.far_field[(long long)k * a.n_pad + idx];
+    pul = pulse_at(a, m.pk[lane], m.pk[32 + lane], m.pk[64 + lane], m.pk[96 + lane], t);
+  }
+  // mid-list entries of the block (local index e = entry - E0) staged by
+  // all helper threads, added per dot in list order by warp 1
+  const int E0 = a.mid_ptr[blk * BS], E = a.mid_ptr[blk * BS + BS] - E0;
+  const int my0 = a.mid_ptr[idx] - E0, my1 = a.mid_ptr[idx + 1] - E0;
+  const int tslot = ring_slot(t, a.W), q1 = a.q + 1;
+  double2 Mo = make_double2(0.0, 0.0);
+  for(int c0 = 0; c0 < E; c0 += kMidChunk) {
+    const int c1 = min(E, c0 + kMidChunk);
+    for(int e = c0 + tid; e < c1; e += kHelpers) {
+      const int b = cached ? m.mc_idx[e] : a.mid_idx[E0 + e];
+      const int d = cached ? m.mc_del[e] : a.mid_delay[E0 + e];
+      double2 v[kMaxOrder + 1];
+      mid_old_fetch<false>(a, b, d, t, tslot, v);
+      m.midv[e - c0] = mid_old_sum(a, d, t, cached ? m.mc_coef + e * q1 : a.mid_coef + (long long)(E0 + e) * q1, v);
+    }
+    helpers_sync();
+    if(part == 1)
+      for(int e = max(my0, c0); e < min(my1, c1); ++e) {
+        Mo.x += m.midv[e - c0].x;
+        Mo.y += m.midv[e - c0].y;
+      }
+    helpers_sync();
+  }
+  if(!live) return;
+  if(part == 1) {
+    m.pre_f[b * BS + lane] = make_double2(F.x + Mo.x, F.y + Mo.y);
+    m.pre_p[b * BS + lane] = pul;
+  } else {
+    // warps 2..7: (p, P or H) = (1,P) (1,H) (2,P) (2,H) (3,P) (3,H)
+    const int w = part - 2, p = w / 2 + 1;
+    const SmemWindow src{m.win, lane};
+    double2 S[2];
+    if(w & 1)
+      pc_partial_half<NT, true>(a, m.ps, m.cs, t, p, src, S);
+    else
+      pc_partial_half<NT, false>(a, m.ps, m.cs, t, p, src, S);
+    const int v0 = (w & 1) ? 2 : 0;
+    double2 *ps = m.pre_s + b * 3 * 4 * BS;
+    ps[((p - 1) * 4 + v0) * BS + lane] = S[0];
+    ps[((p - 1) * 4 + v0 + 1) * BS + lane] = S[1];
+  }
 }
 
 template <int NT>
-__global__ void __launch_bounds__(32 * kParts) step_block_kernel(StepArgs a, int k0, int k1, unsigned *bar)
+__global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArgs a, int k0, int k1, unsigned *bar)
 {
   constexpr int BS = 32;
-  // 62.5 KB of dynamic shared memory (above the 48 KB static limit)
-  extern __shared__ double2 smem_block[];
-  auto win = reinterpret_cast<double2(*)[4][BS]>(smem_block);  // rho00, rho01, drho00, drho01 by step slot
-  auto red = reinterpret_cast<double2(*)[4][BS]>(smem_block + kPcDepth * 4 * BS);
-  double2 *midv = smem_block + (kPcDepth + kParts) * 4 * BS;
-  double2 *cur = midv + kMidChunk;
+  extern __shared__ double2 smem_block[];  // dynamic: above the 48 KB static limit
+  const BlockSmem m = block_smem(smem_block, a.q, a.mid_cache);
+  __shared__ int s_abort;
   const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
   const int blk = blockIdx.x;
   const int idx = blk * BS + lane;
   const int t0 = *a.far_t0;
   const bool live = a.user[idx] >= 0;
   const int nt = NT > 0 ? NT : a.w.n_time;
+  const unsigned nb = gridDim.x;
 
-  // the integrator's window: all 23 slots of the predictor-corrector ring
-  for(int sl = part; sl < kPcDepth; sl += kParts)
-    for(int c = 0; c < 4; ++c) win[sl][c][lane] = a.pcr[((long long)sl * 4 + c) * a.n_pad + idx];
-  double det = 0, t1 = 1, t2 = 1;
-  if(live) {
-    det = a.laser_freq - a.freq[idx];
-    t1 = a.t1[idx];
-    t2 = a.t2[idx];
+  // window, weights, prev01, and the block's mid list when it fits
+  for(int sl = part; sl < kPcDepth; sl += kBlockWarps)
+    for(int c = 0; c < 4; ++c) m.win[sl][c][lane] = a.pcr[((long long)sl * 4 + c) * a.n_pad + idx];
+  for(int i = threadIdx.x; i < 2 * nt; i += blockDim.x) {
+    m.ps[i] = a.w.ps[i];
+    m.cs[i] = a.w.cs[i];
   }
-  const int E0 = a.mid_ptr[blk * BS], E1 = a.mid_ptr[blk * BS + BS];
-  const int my0 = a.mid_ptr[idx], my1 = a.mid_ptr[idx + 1];
-  const int nb0 = a.near_ptr[blk * BS];
-  const bool block_near = a.near_ptr[(blk + 1) * BS] > nb0;
-  const int ne0 = a.near_ptr[idx], ne1 = a.near_ptr[idx + 1];
+  const int E0 = a.mid_ptr[blk * BS], E = a.mid_ptr[blk * BS + BS] - E0;
+  const bool cached = E <= a.mid_cache;
+  if(cached) {
+    const int q1 = a.q + 1;
+    for(int i = threadIdx.x; i < E * q1; i += blockDim.x) m.mc_coef[i] = a.mid_coef[(long long)E0 * q1 + i];
+    for(int i = threadIdx.x; i < E; i += blockDim.x) {
+      m.mc_idx[i] = a.mid_idx[E0 + i];
+      m.mc_del[i] = a.mid_delay[E0 + i];
+    }
+  }
+  if(part == 0) m.prev01[lane] = a.ring[(long long)idx * a.stride + ring_slot(t0 + k0 - 1, a.W)];
+  if(part == 1 && live) {
+    m.pk[lane] = pulse_kr(a, idx);
+    for(int c = 0; c < 3; ++c) m.pk[32 * (c + 1) + lane] = a.dip[3 * idx + c];
+  }
+  if(threadIdx.x == 0) s_abort = 0;
+  __syncthreads();
+  if(part > 0 && t0 + k0 < a.T) block_precompute<NT>(a, m, blk, k0, t0 + k0, k0 & 1, cached);
+  const DotConst dc = dot_const(a, idx, live);
+  const bool block_near = a.near_ptr[(blk + 1) * BS] > a.near_ptr[blk * BS];
+  const NearRegs nr = near_regs(a, idx);
   __syncthreads();
 
   for(int k = k0; k < k1; ++k) {
     const int t = t0 + k;
-    if(t >= a.T) break;  // uniform: every block stops at the same k
-    if(live) {
-      double2 P0 = make_double2(0.0, 0.0), P1 = P0, H0 = P0, H1 = P0;
-      const double dt = a.dt;
-#pragma unroll
-      for(int h0 = 0; h0 < (NT > 0 ? NT : 32); h0 += kParts) {
-        const int h = h0 + part;
-        if(h < nt) {
-          const int sl = pc_slot(t - nt + h);
-          const double2 x0 = win[sl][0][lane], x1 = win[sl][1][lane], y0 = win[sl][2][lane], y1 = win[sl][3][lane];
-          const double p0 = a.w.ps[h], p1 = a.w.ps[nt + h];
-          const double c0 = a.w.cs[h], c1 = a.w.cs[nt + h];
-          P0.x += x0.x * p0 + (y0.x * p1) * dt;
-          P0.y += x0.y * p0 + (y0.y * p1) * dt;
-          P1.x += x1.x * p0 + (y1.x * p1) * dt;
-          P1.y += x1.y * p0 + (y1.y * p1) * dt;
-          H0.x += x0.x * c0 + (y0.x * c1) * dt;
-          H0.y += x0.y * c0 + (y0.y * c1) * dt;
-          H1.x += x1.x * c0 + (y1.x * c1) * dt;
-          H1.y += x1.y * c0 + (y1.y * c1) * dt;
-        }
-      }
-      red[part][0][lane] = P0;
-      red[part][1][lane] = P1;
-      red[part][2][lane] = H0;
-      red[part][3][lane] = H1;
-    }
-    double2 M = make_double2(0.0, 0.0);
-    for(int c0 = E0; c0 < E1; c0 += kMidChunk) {
-      const int c1 = min(E1, c0 + kMidChunk);
-      for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_entry_cg(a, e, t);
-      __syncthreads();
-      if(part == 0)
-        for(int e = max(my0, c0); e < min(my1, c1); ++e) {
-          M.x += midv[e - c0].x;
-          M.y += midv[e - c0].y;
-        }
-      __syncthreads();
-    }
-    if(E0 == E1) __syncthreads();
-
+    if(t >= a.T || s_abort) break;  // uniform across the block
+    const int buf = k & 1;
     if(part == 0) {
-      double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
-      double pul = 0;
-      if(live) {
-        double2 sum[4];
-#pragma unroll
-        for(int v = 0; v < 4; ++v) {
-          sum[v] = red[0][v][lane];
-#pragma unroll
-          for(int p = 1; p < kParts; ++p) {
-            sum[v].x += red[p][v][lane].x;
-            sum[v].y += red[p][v][lane].y;
-          }
-        }
-        P[0] = sum[0];
-        P[1] = sum[1];
-        H[0] = sum[2];
-        H[1] = sum[3];
-        past = a.far_field[(long long)k * a.n_pad + idx];
-        past.x += M.x;
-        past.y += M.y;
-        pul = pulse_rabi(a, idx, t);
-        r[0] = P[0];
-        r[1] = P[1];
+      bool ok = true;
+      if(!a.lag && k > k0) {
+        // partners' step t-1 from other blocks: wait for all of them
+        ok = threadIdx.x != 0 || wait_count(bar, (unsigned)(k - k0) * nb);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
       }
-      for(int it = 0; it <= kCorrectorSteps; ++it) {
-        if(it > 0 && live) corrector(a, dr, H, r);
-        double2 nf = make_double2(0.0, 0.0);
-        if(block_near) {
-          __syncwarp();
-          cur[lane] = live ? prefactor(r[1], a.frame) : make_double2(0.0, 0.0);
-          __syncwarp();
-          for(int e = ne0; e < ne1; ++e) {
-            const double2 v = cmul(cur[a.near_idx[e]], a.near_coef[e]);
-            nf.x += v.x;
-            nf.y += v.y;
-          }
-        }
+      if(ok) {
+        double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
+        double pul = 0;
         if(live) {
-          const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
-          liouville(r[0], r[1], om, t1, t2, det, dr[0], dr[1]);
+          double2 S[4], T[4];
+          const double2 *ps = m.pre_s + buf * 3 * 4 * BS;
+#pragma unroll
+          for(int v = 0; v < 4; ++v) {
+            const double2 s1 = ps[(0 * 4 + v) * BS + lane], s2 = ps[(1 * 4 + v) * BS + lane],
+                          s3 = ps[(2 * 4 + v) * BS + lane];
+            S[v] = make_double2((s1.x + s2.x) + s3.x, (s1.y + s2.y) + s3.y);
+          }
+          pc_newest(a, m.ps, m.cs, t, nt, SmemWindow{m.win, lane}, T);
+          pc_combine(S, T, P, H);
+          double2 Mn;
+          if(a.lag) {
+            Mn = mid_new(a, idx, [&](int b) { return m.prev01[b & 31]; });
+          } else {
+            const int slot = ring_slot(t - 1, a.W);
+            Mn = mid_new(a, idx, [&](int b) { return __ldcg(a.ring + (long long)b * a.stride + slot); });
+          }
+          const double2 F = m.pre_f[buf * BS + lane];
+          past = make_double2(F.x + Mn.x, F.y + Mn.y);
+          pul = m.pre_p[buf * BS + lane];
         }
+        dot_iterate(a, live, block_near, nr, m.cur, lane, P, H, past, pul, dc, r, dr);
+        if(live) {
+          finish_dot(a, idx, t, r, dr);
+          const int sl = pc_slot(t);
+          m.win[sl][0][lane] = r[0];
+          m.win[sl][1][lane] = r[1];
+          m.win[sl][2][lane] = dr[0];
+          m.win[sl][3][lane] = dr[1];
+        }
+        __syncwarp();
+        m.prev01[lane] = live ? r[1] : make_double2(0.0, 0.0);
+        if(k == kTimeBlock - 1 && blk == 0 && lane == 0) *a.d_next = t + 1;
+      } else if(lane == 0) {
+        s_abort = 1;
+        atomicMin(a.d_bad, -2);
       }
-      if(live) {
-        finish_dot(a, idx, t, r, dr);
-        const int sl = pc_slot(t);
-        win[sl][0][lane] = r[0];
-        win[sl][1][lane] = r[1];
-        win[sl][2][lane] = dr[0];
-        win[sl][3][lane] = dr[1];
+    } else {
+      // post this block's step k-1 (warp 0's stores precede the block
+      // barrier that ended it; the fence makes them visible device-wide first)
+      if(threadIdx.x == 32 && k > k0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+      }
+      if(k + 1 < k1 && t + 1 < a.T) {
+        // step k+1's sums; M_old needs every block's step k-1
+        if(threadIdx.x == 32 && !wait_count(bar, (unsigned)(k - k0) * nb)) {
+          s_abort = 1;
+          atomicMin(a.d_bad, -2);
+        }
+        helpers_sync();
+        if(!*(volatile int *)&s_abort) block_precompute<NT>(a, m, blk, k + 1, t + 1, buf ^ 1, cached);
       }
     }
-    if(k == kTimeBlock - 1 && blk == 0 && threadIdx.x == 0) *a.d_next = t + 1;
-    if(k + 1 < k1 && !grid_barrier(bar, (unsigned)(k - k0 + 1) * gridDim.x)) {
-      if(threadIdx.x == 0) atomicMin(a.d_bad, -2);
-      return;
-    }
+    __syncthreads();
   }
 }
 
-constexpr size_t kStepBlockSmem = sizeof(double2) * ((kPcDepth + kParts) * 4 * 32 + kMidChunk + 32);
-
-static void step_block_attrs()
+static void step_block_attrs(size_t smem)
 {
-  static int dev_done[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if(dev < 64 && !dev_done[dev]) {
-    cudaFuncSetAttribute(step_block_kernel<22>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStepBlockSmem);
-    cudaFuncSetAttribute(step_block_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStepBlockSmem);
-    dev_done[dev] = 1;
-  }
+  cudaFuncSetAttribute(step_block_kernel<22>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(step_block_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *bar, void *stream)
 {
   cudaStream_t s = (cudaStream_t)stream;
-  step_block_attrs();
+  const size_t smem = block_smem_bytes(a.q, a.mid_cache);
+  step_block_attrs(smem);
   cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
-  cfg.blockDim = dim3(32 * kParts);
-  cfg.dynamicSmemBytes = kStepBlockSmem;
+  cfg.blockDim = dim3(32 * kBlockWarps);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr;
   attr.id = cudaLaunchAttributeCooperative;
@@ -616,13 +871,23 @@ void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned 
     cudaLaunchKernelEx(&cfg, step_block_kernel<0>, a, k0, k1, bar);
 }
 
-int step_block_max_blocks()
+// Thread blocks of the step-block kernel that fit on the device at once
+// with a mid-list cache of `mid_cache` entries (0 when the shared memory
+// does not fit at all).
+int step_block_max_blocks(int q, int mid_cache)
 {
-  int dev = 0, sms = 0, per = 0;
+  const size_t smem = block_smem_bytes(q, mid_cache);
+  int dev = 0, sms = 0, per = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  step_block_attrs();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_block_kernel<22>, 32 * kParts, kStepBlockSmem);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if(smem > (size_t)optin) return 0;
+  step_block_attrs(smem);
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_block_kernel<22>, 32 * kBlockWarps, smem) !=
+     cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
   return sms * per;
 }
 
@@ -667,7 +932,7 @@ __global__ void __launch_bounds__(kStepBlock) step_general_kernel(StepArgs a, in
     const double pul = sc[1].x;
     const double2 om = make_double2((0.0 + pul) + (past.x + nf.x), 0.0 + (past.y + nf.y));
     double2 dr[2];
-    liouville(r[0], r[1], om, a.t1[idx], a.t2[idx], a.laser_freq - a.freq[idx], dr[0], dr[1]);
+    liouville(r[0], r[1], om, dot_const(a, idx, true), dr[0], dr[1]);
     if(it < kCorrectorSteps) {
       const double2 H[2] = {sc[2], sc[3]};
       corrector(a, dr, H, r);
