@@ -80,8 +80,7 @@ struct qg_handle_s {
   double2 *d_new_coef = nullptr;
   bool lag = false;  // every delay-0/1 partner shares the dot's 32-dot block
   // d_ints: 0 step, 1 done, 2 bad, 3 traj_t0, 4 eval_step, 5 max_delay,
-  //         6 far_t0 (run), 7 far block start request, 8 far_t0 (evaluate),
-  //         12 grid-barrier counter of the step-block kernel
+  //         6 far_t0 (run), 7 far block start request, 8 far_t0 (evaluate)
   int *d_ints = nullptr;
   unsigned long long *d_u64 = nullptr;
   double2 *d_traj = nullptr;  // 2 * traj_k steps x N x 2
@@ -96,6 +95,10 @@ struct qg_handle_s {
   // 32-dot block resident at once); otherwise one launch per step
   bool block_step = false, block_step_ok = false;
   int mid_cache = 0;  // mid-list entries per block kept in shared memory by that kernel
+  int hist_cap = 0;   // distinct partners per block whose history that kernel keeps
+  int *d_bp_ptr = nullptr, *d_bp_idx = nullptr, *d_mid_pj = nullptr;
+  int *d_pb_ptr = nullptr, *d_pb_idx = nullptr;
+  unsigned *d_flags = nullptr;  // the step-block kernel's per-block step counts
   int max_delay = 0;
   long long near_pairs = 0, mid_pairs = 0;
   int far_block = -0x7fffffff;  // first step of the far block the partials hold
@@ -185,6 +188,12 @@ struct qg_handle_s {
     a.new_coef = d_new_coef;
     a.lag = lag ? 1 : 0;
     a.mid_cache = mid_cache;
+    a.bp_ptr = d_bp_ptr;
+    a.bp_idx = d_bp_idx;
+    a.mid_pj = d_mid_pj;
+    a.hist_cap = hist_cap;
+    a.pb_ptr = d_pb_ptr;
+    a.pb_idx = d_pb_idx;
     a.pcr = d_pcr;
     a.ring = d_ring;
     a.ring32w = d_ring32w;
@@ -486,15 +495,39 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   h->step_blocks = np / 32;
   // the step-block kernel: all blocks resident, each with its part of the
   // mid list in shared memory when that still fits
-  int max_e = 0;
-  for(int b = 0; b < h->step_blocks; ++b) max_e = std::max(max_e, mptr[32 * (b + 1)] - mptr[32 * b]);
+  // and, again when it fits, the history of each block's distinct partners
+  int max_e = 0, max_p = 0;
+  std::vector<int> bptr(1, 0), bidx, mpj(midx.size()), pbptr(1, 0), pbidx;
+  for(int b = 0; b < h->step_blocks; ++b) {
+    const int e0 = mptr[32 * b], e1 = mptr[32 * (b + 1)];
+    max_e = std::max(max_e, e1 - e0);
+    std::vector<int> parts(midx.begin() + e0, midx.begin() + e1);
+    std::sort(parts.begin(), parts.end());
+    parts.erase(std::unique(parts.begin(), parts.end()), parts.end());
+    for(int e = e0; e < e1; ++e)
+      mpj[e] = (int)(std::lower_bound(parts.begin(), parts.end(), midx[e]) - parts.begin());
+    std::vector<int> blks(1, b);
+    for(int pp : parts) blks.push_back(pp / 32);
+    std::sort(blks.begin(), blks.end());
+    blks.erase(std::unique(blks.begin(), blks.end()), blks.end());
+    pbidx.insert(pbidx.end(), blks.begin(), blks.end());
+    pbptr.push_back((int)pbidx.size());
+    bidx.insert(bidx.end(), parts.begin(), parts.end());
+    bptr.push_back((int)bidx.size());
+    max_p = std::max(max_p, (int)parts.size());
+  }
   h->mid_cache = 0;
+  h->hist_cap = 0;
   h->block_step_ok = false;
   if(h->fused) {
-    if(h->step_blocks <= step_block_max_blocks(h->q, max_e)) {
+    if(h->step_blocks <= step_block_max_blocks(h->q, max_e, max_p)) {
+      h->mid_cache = max_e;
+      h->hist_cap = max_p;
+      h->block_step_ok = true;
+    } else if(h->step_blocks <= step_block_max_blocks(h->q, max_e, 0)) {
       h->mid_cache = max_e;
       h->block_step_ok = true;
-    } else if(h->step_blocks <= step_block_max_blocks(h->q, 0)) {
+    } else if(h->step_blocks <= step_block_max_blocks(h->q, 0, 0)) {
       h->block_step_ok = true;
     }
   }
@@ -524,6 +557,12 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   QG_TRY(upload_i(&h->d_new_ptr, nptr));
   QG_TRY(upload_i(&h->d_new_idx, nidx));
   QG_TRY(upload_c(&h->d_new_coef, ncoef));
+  QG_TRY(upload_i(&h->d_bp_ptr, bptr));
+  QG_TRY(upload_i(&h->d_bp_idx, bidx));
+  QG_TRY(upload_i(&h->d_mid_pj, mpj));
+  QG_TRY(upload_i(&h->d_pb_ptr, pbptr));
+  QG_TRY(upload_i(&h->d_pb_idx, pbidx));
+  QG_TRY(dalloc(h, &h->d_flags, std::max(h->step_blocks, 1)));
   h->lag = h->fused && lag;
   return QG_OK;
 }
@@ -865,7 +904,7 @@ static void enqueue_step_block(qg_handle *h, int k0, int k1, bool traj)
 {
   StepArgs a = h->step_args(false);
   if(traj) a.traj = h->d_traj;
-  launch_step_block(a, k0, k1, h->step_blocks, reinterpret_cast<unsigned *>(h->d_ints + 12), h->stream);
+  launch_step_block(a, k0, k1, h->step_blocks, h->d_flags, h->stream);
 }
 
 static void enqueue_dot_step(qg_handle *h, int k, bool traj)
@@ -1076,7 +1115,7 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   QG_CUDA(cudaGetLastError());
   h->next_step = t_start + n_steps;
   if(bad == -2)
-    return qg_fail(QG_ERR_CUDA, "qg_run: the step-block kernel's grid barrier timed out");
+    return qg_fail(QG_ERR_CUDA, "qg_run: a wait in the step-block kernel timed out");
   if(bad < 0)
     return qg_fail(QG_ERR_CUDA, "qg_run: internal scheduling error (far block or trajectory row)");
   if(bad != kBadNone) {

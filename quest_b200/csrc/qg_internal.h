@@ -109,6 +109,17 @@ struct StepArgs {
   const double2 *new_coef;
   int lag;
   int mid_cache;  // step-block kernel: mid-list entries a block keeps in shared memory
+  // step-block kernel partner history: per 32-dot block its distinct mid-list
+  // partners (CSR by block, internal indices), each entry's partner as an
+  // index into its block's list, and the partners a block can hold (0: off)
+  const int *bp_ptr;
+  const int *bp_idx;
+  const int *mid_pj;
+  int hist_cap;
+  // step-block kernel: per 32-dot block, the blocks holding its mid-list
+  // partners, itself included (CSR by block)
+  const int *pb_ptr;
+  const int *pb_idx;
   double2 *pcr;          // [kPcDepth][4][n_pad]
   double2 *ring;         // [n_pad][stride] rho01 by step slot
   float2 *ring32w;       // mixed: FP32 rho01 by slot (null in FP64)
@@ -148,8 +159,8 @@ void launch_far_step1(const FarArgs &a, void *stream);
 void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
                       int grid, void *stream);
 void launch_ring32_rebuild(const StepArgs &a, void *stream);
-void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *bar, void *stream);
-int step_block_max_blocks(int q, int mid_cache);
+void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *flags, void *stream);
+int step_block_max_blocks(int q, int mid_cache, int hist_cap);
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
                        int k, void *stream);
 

@@ -190,16 +190,10 @@ __device__ __forceinline__ bool finite4(double2 a, double2 b)
   return isfinite(a.x) && isfinite(a.y) && isfinite(b.x) && isfinite(b.y);
 }
 
-// Stores the step's final state: PC window, rho01 ring, trajectory row,
-// and the non-finite flag.
-__device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, const double2 (&r)[2],
-                                           const double2 (&dr)[2])
+// Stores the step's rho01 in the ring (and, in mixed precision, the FP32
+// rings), which other dots read.
+__device__ __forceinline__ void finish_ring(const StepArgs &a, int idx, int t, const double2 (&r)[2])
 {
-  double2 *base = a.pcr + (long long)pc_slot(t) * 4 * a.n_pad + idx;
-  base[0] = r[0];
-  base[a.n_pad] = r[1];
-  base[2 * a.n_pad] = dr[0];
-  base[3 * a.n_pad] = dr[1];
   const int slot = t % a.W;
   double2 *ring = a.ring + (long long)idx * a.stride;
   if(a.ring32w) {
@@ -218,6 +212,18 @@ __device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, co
   }
   ring[slot] = r[1];
   if(slot < kRingMirror) ring[a.W + slot] = r[1];
+}
+
+// Stores the rest of the step's final state: PC window, trajectory row and
+// the non-finite flag.
+__device__ __forceinline__ void finish_state(const StepArgs &a, int idx, int t, const double2 (&r)[2],
+                                             const double2 (&dr)[2])
+{
+  double2 *base = a.pcr + (long long)pc_slot(t) * 4 * a.n_pad + idx;
+  base[0] = r[0];
+  base[a.n_pad] = r[1];
+  base[2 * a.n_pad] = dr[0];
+  base[3 * a.n_pad] = dr[1];
   if(a.traj) {
     const int row = t - *a.traj_t0;
     if(row >= 0 && row < a.traj_rows) {
@@ -229,6 +235,13 @@ __device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, co
     }
   }
   if(!finite4(r[0], r[1]) || !finite4(dr[0], dr[1])) atomicMin(a.d_bad, t);
+}
+
+__device__ __forceinline__ void finish_dot(const StepArgs &a, int idx, int t, const double2 (&r)[2],
+                                           const double2 (&dr)[2])
+{
+  finish_ring(a, idx, t, r);
+  finish_state(a, idx, t, r, dr);
 }
 
 // The step index is the far block's first step plus the launch's offset k;
@@ -326,10 +339,10 @@ __device__ __forceinline__ void pc_newest(const StepArgs &a, const double *ps, c
 // The taps of a mid-list entry at step t that read step t-2 or earlier
 // (taps before step -22 skipped): partner b, delay d < W - q, coefficients
 // c[0..q], tslot = ring_slot(t).  All the taps are fetched before any is
-// used, so their loads are in flight together.  CG: loads through L2 only
-// (the data may have been written by another block since this SM last read
-// the line); otherwise ordinary loads, for callers whose acquire of the
-// writers' release already covers them.
+// used, so their loads are in flight together.  CG: loads through L2 only,
+// for data another block may have written since this SM last read the line
+// (an L1 copy of that line would be stale); otherwise ordinary loads, for
+// data written before the kernel started.
 template <bool CG>
 __device__ __forceinline__ void mid_old_fetch(const StepArgs &a, int b, int d, int t, int tslot,
                                               double2 (&v)[kMaxOrder + 1])
@@ -347,7 +360,7 @@ __device__ __forceinline__ void mid_old_fetch(const StepArgs &a, int b, int d, i
   }
 }
 
-__device__ __forceinline__ double2 mid_old_sum(const StepArgs &a, int d, int t, const double2 *c,
+__device__ __forceinline__ double2 mid_old_sum(const StepArgs &a, int d, int t, const double2 *c, int cstride,
                                                const double2 (&v)[kMaxOrder + 1])
 {
   const int q = a.q;
@@ -356,7 +369,7 @@ __device__ __forceinline__ double2 mid_old_sum(const StepArgs &a, int d, int t, 
 #pragma unroll
   for(int i = 0; i <= kMaxOrder; ++i) {
     if(i <= q && s - i >= -kWindow && d + i >= 2) {
-      const double2 w = cmul(prefactor(v[i], a.frame), c[i]);
+      const double2 w = cmul(prefactor(v[i], a.frame), c[i * cstride]);
       M.x += w.x;
       M.y += w.y;
     }
@@ -369,15 +382,15 @@ __device__ __forceinline__ double2 mid_old(const StepArgs &a, int e, int t, int 
   const int d = a.mid_delay[e];
   double2 v[kMaxOrder + 1];
   mid_old_fetch<true>(a, a.mid_idx[e], d, t, tslot, v);
-  return mid_old_sum(a, d, t, a.mid_coef + (long long)e * (a.q + 1), v);
+  return mid_old_sum(a, d, t, a.mid_coef + (long long)e * (a.q + 1), 1, v);
 }
 
 // M_new of dot idx; prev(b) = rho01 of partner b at step t-1.
 template <class Prev>
-__device__ __forceinline__ double2 mid_new(const StepArgs &a, int idx, const Prev &prev)
+__device__ __forceinline__ double2 mid_new(const StepArgs &a, int j0, int j1, const Prev &prev)
 {
   double2 M = make_double2(0.0, 0.0);
-  for(int j = a.new_ptr[idx]; j < a.new_ptr[idx + 1]; ++j) {
+  for(int j = j0; j < j1; ++j) {
     const double2 v = cmul(prefactor(prev(a.new_idx[j]), a.frame), a.new_coef[j]);
     M.x += v.x;
     M.y += v.y;
@@ -480,7 +493,8 @@ __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int 
       pul = pulse_rabi(a, idx, t);
       pc_newest(a, a.w.ps, a.w.cs, t, nt, win, T);
       const int slot = ring_slot(t - 1, a.W);
-      Mn = mid_new(a, idx, [&](int b) { return __ldcg(a.ring + (long long)b * a.stride + slot); });
+      Mn = mid_new(a, a.new_ptr[idx], a.new_ptr[idx + 1],
+                   [&](int b) { return __ldcg(a.ring + (long long)b * a.stride + slot); });
     }
   } else if(live) {
     double2 S[4];
@@ -565,36 +579,59 @@ void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, in
 // The steps k0 .. k1-1 of a block in one cooperative launch (every thread
 // block resident), 8 warps per 32 dots.  Each block keeps in shared memory
 // its dots' predictor-corrector window (23 steps of rho and rho-dot), the
-// integrator weights and, when it fits, its part of the mid list.  Warp 0
-// runs step k while warps 1-7 form step k+1's window partials S_p, F + M_old
-// and pulse (double-buffered in shared memory).  M_old reads the partners'
-// history of step k-1 and earlier, so warps 1-7 first wait until every block
-// has finished step k-1.  Blocks count finished steps on one device-wide
-// arrival counter; a block's helper warps post its step k-1 at the start of
-// step k (after the block barrier that follows warp 0's stores), so warp 0
-// never waits on the fence.
+// integrator weights, the launch's far-pair field and pulse, and (when they
+// fit) its part of the mid list and the recent rho01 of each distinct
+// mid-list partner.  Warp 0 runs step k on a scheduler of its own (warp 4,
+// which would share it, stays idle) while warps 1-3 and 5-7 form step k+1's
+// window partials S_p and F + M_old (double-buffered).  M_old reads the
+// partners' history of step k-1 and earlier, so the helpers first wait until
+// every block that holds one of the block's mid-list partners (and the block
+// itself) has finished step k-1.  Each block counts its finished steps in
+// flags[block] (zeroed before the launch); warp 0 posts a step as soon as its
+// rho01 is stored.  Blocks wait only for their partners' blocks, so nearby
+// blocks may run a step or two apart and no global barrier is needed.
 //
 // M_new reads step k-1 of the delay-0/1 partners: with a.lag set every such
-// partner is in the dot's own block and its value comes from shared memory,
-// so no block waits for a step just finished elsewhere (blocks may run one
-// step apart); otherwise warp 0 also waits for every block's step k-1.
+// partner is in the dot's own block and its value comes from shared memory;
+// otherwise warp 0 also waits for its partner blocks' step k-1.
 // Every wait is bounded (about a second); a wait that runs out sets
 // *a.d_bad to -2 and the kernel returns.
 constexpr int kBlockWarps = 8;
-constexpr int kHelpers = 32 * (kBlockWarps - 1);  // threads of warps 1..7
-constexpr int kBarrierSpins = 1 << 24;            // x ~64 ns of sleep: about a second
-constexpr int kWeightSlots = 64;                  // 2 x n_time, n_time <= 32
+constexpr int kHelperWarps = 6;                // warps 1, 2, 3, 5, 6, 7
+constexpr int kHelpers = 32 * kHelperWarps;
+constexpr int kBarrierSpins = 1 << 24;         // x ~64 ns of sleep: about a second
+constexpr int kWeightSlots = 64;               // 2 x n_time, n_time <= 32
 
-// Waits until *ctr >= target (thread-level; acquire on success).
-__device__ __forceinline__ bool wait_count(const unsigned *ctr, unsigned target)
+// Partner history: the rho01 samples that mid-list taps read, for each of a
+// block's distinct partners, slot = step mod kHistDepth, rows padded to
+// kHistStride so rows start in different banks.  A step t reads samples
+// t-22 .. t-2 (delay <= K-1, tap <= kMaxOrder, delay + tap >= 2).
+constexpr int kHistDepth = 24;
+constexpr int kHistStride = 25;
+constexpr int kHistSpan = (kTimeBlock - 1) + kMaxOrder;  // t - kHistSpan is the oldest sample read
+
+__device__ __forceinline__ int hist_slot(int s) { return ((s % kHistDepth) + kHistDepth) % kHistDepth; }
+
+// Called by a whole warp: waits until flags[list[i]] >= target for every
+// i < n (the lanes poll in parallel, each wait bounded), then fences so the
+// posting blocks' stores are visible (acquire).  False if a wait ran out.
+__device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *list, int n, unsigned target)
 {
-  int spins = 0;
-  while(*(volatile const unsigned *)ctr < target) {
-    if(++spins > kBarrierSpins) return false;
-    __nanosleep(64);
+  bool ok = true;
+  for(int i = threadIdx.x & 31; i < n && ok; i += 32) {
+    const volatile unsigned *f = flags + __ldg(list + i);
+    int spins = 0;
+    while(*f < target) {
+      if(++spins > kBarrierSpins) {
+        ok = false;
+        break;
+      }
+      __nanosleep(32);
+    }
   }
+  ok = __all_sync(0xffffffffu, ok);
   __threadfence();
-  return true;
+  return ok;
 }
 
 __device__ __forceinline__ void helpers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kHelpers)); }
@@ -629,76 +666,93 @@ struct BlockSmem {
   double2 (*win)[4][32];  // [kPcDepth][4][32]
   double2 *pre_s;         // [2][3][4][32] S_p
   double2 *pre_f;         // [2][32] F + M_old
+  double2 *far;           // [K][32] far-pair field of the launch's steps
   double2 *midv;          // [kMidChunk] staged entries
   double2 *cur;           // [32] delay-0 exchange
   double2 *prev01;        // [32] rho01 of step t-1
-  double *pre_p;          // [2][32] pulse
+  double2 *mc_coef;       // [q+1][mid_cache] the block's mid-list coefficients, tap-major
+  double2 *hist;          // [hist_cap][kHistStride] rho01 of the block's distinct partners
+  double *pul;            // [K][32] pulse of the launch's steps
   double *ps, *cs;        // [kWeightSlots] each
-  double *pk;             // [4][32] k.r and the dipole, for the pulse
-  double2 *mc_coef;       // [mid_cache][q+1] the block's mid-list coefficients
-  int *mc_idx, *mc_del;   // [mid_cache] partners and delays
+  int *mc_idx, *mc_del;   // [mid_cache] partners (with hist: partner slots) and delays
 };
 
-__host__ __device__ __forceinline__ size_t block_smem_bytes(int q, int mid_cache)
+__host__ __device__ __forceinline__ size_t block_smem_bytes(int q, int mid_cache, int hist_cap)
 {
-  return sizeof(double2) * ((size_t)kPcDepth * 4 * 32 + 2 * 3 * 4 * 32 + 2 * 32 + kMidChunk + 32 + 32 +
-                            (size_t)mid_cache * (q + 1)) +
-         sizeof(double) * (2 * 32 + 2 * kWeightSlots + 4 * 32) + sizeof(int) * 2 * (size_t)mid_cache;
+  return sizeof(double2) * ((size_t)kPcDepth * 4 * 32 + 2 * 3 * 4 * 32 + 2 * 32 + kTimeBlock * 32 + kMidChunk + 32 +
+                            32 + (size_t)mid_cache * (q + 1) + (size_t)hist_cap * kHistStride) +
+         sizeof(double) * (kTimeBlock * 32 + 2 * kWeightSlots) + sizeof(int) * 2 * (size_t)mid_cache;
 }
 
-__device__ __forceinline__ BlockSmem block_smem(double2 *base, int q, int mid_cache)
+__device__ __forceinline__ BlockSmem block_smem(double2 *base, int q, int mid_cache, int hist_cap)
 {
   BlockSmem m;
   m.win = reinterpret_cast<double2(*)[4][32]>(base);
   m.pre_s = base + kPcDepth * 4 * 32;
   m.pre_f = m.pre_s + 2 * 3 * 4 * 32;
-  m.midv = m.pre_f + 2 * 32;
+  m.far = m.pre_f + 2 * 32;
+  m.midv = m.far + kTimeBlock * 32;
   m.cur = m.midv + kMidChunk;
   m.prev01 = m.cur + 32;
   m.mc_coef = m.prev01 + 32;
-  m.pre_p = reinterpret_cast<double *>(m.mc_coef + (size_t)mid_cache * (q + 1));
-  m.ps = m.pre_p + 2 * 32;
+  m.hist = m.mc_coef + (size_t)mid_cache * (q + 1);
+  m.pul = reinterpret_cast<double *>(m.hist + (size_t)hist_cap * kHistStride);
+  m.ps = m.pul + kTimeBlock * 32;
   m.cs = m.ps + kWeightSlots;
-  m.pk = m.cs + kWeightSlots;
-  m.mc_idx = reinterpret_cast<int *>(m.pk + 4 * 32);
+  m.mc_idx = reinterpret_cast<int *>(m.cs + kWeightSlots);
   m.mc_del = m.mc_idx + mid_cache;
   return m;
 }
 
-// Step k's sums by warps 1..7 into buffer `b`: pre_s[b][p-1][v][lane] = S_p
-// of quantity v, pre_f[b] = F + M_old, pre_p[b] = pulse.
+// Step k's sums by the helper warps (hw = 0..5) into buffer `b`:
+// pre_s[b][p-1][v][lane] = S_p of quantity v, pre_f[b] = F + M_old.
 template <int NT>
 __device__ __forceinline__ void block_precompute(const StepArgs &a, const BlockSmem &m, int blk, int k, int t,
-                                                 int b, bool cached)
+                                                 int b, bool cached, bool hist, int hw)
 {
   constexpr int BS = 32;
-  const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
-  const int tid = threadIdx.x - 32;
+  const int lane = threadIdx.x & 31;
+  const int tid = hw * 32 + lane;
   const int idx = blk * BS + lane;
   const bool live = a.user[idx] >= 0;
-  double2 F = make_double2(0.0, 0.0);
-  double pul = 0;
-  if(part == 1 && live) {
-    F = a.far_field[(long long)k * a.n_pad + idx];
-    pul = pulse_at(a, m.pk[lane], m.pk[32 + lane], m.pk[64 + lane], m.pk[96 + lane], t);
-  }
-  // mid-list entries of the block (local index e = entry - E0) staged by
-  // all helper threads, added per dot in list order by warp 1
   const int E0 = a.mid_ptr[blk * BS], E = a.mid_ptr[blk * BS + BS] - E0;
   const int my0 = a.mid_ptr[idx] - E0, my1 = a.mid_ptr[idx + 1] - E0;
-  const int tslot = ring_slot(t, a.W), q1 = a.q + 1;
+  const int q1 = a.q + 1, cap = a.mid_cache;
+  if(hist) {
+    // the newest sample the old taps read (step t-2, finished by every
+    // block), one load per distinct partner of the block
+    const int P0 = a.bp_ptr[blk], NP = a.bp_ptr[blk + 1] - P0;
+    const int sa = t - 2, hs = hist_slot(sa), rs = ring_slot(sa, a.W);
+    for(int j = tid; j < NP; j += kHelpers)
+      m.hist[j * kHistStride + hs] = __ldcg(a.ring + (long long)a.bp_idx[P0 + j] * a.stride + rs);
+    helpers_sync();
+  }
+  // mid-list entries of the block (local index e = entry - E0) staged by
+  // the helpers, added per dot in list order by helper warp 0
+  const int tslot = ring_slot(t, a.W);
   double2 Mo = make_double2(0.0, 0.0);
   for(int c0 = 0; c0 < E; c0 += kMidChunk) {
     const int c1 = min(E, c0 + kMidChunk);
     for(int e = c0 + tid; e < c1; e += kHelpers) {
-      const int b = cached ? m.mc_idx[e] : a.mid_idx[E0 + e];
+      const int pb = cached ? m.mc_idx[e] : a.mid_idx[E0 + e];
       const int d = cached ? m.mc_del[e] : a.mid_delay[E0 + e];
       double2 v[kMaxOrder + 1];
-      mid_old_fetch<false>(a, b, d, t, tslot, v);
-      m.midv[e - c0] = mid_old_sum(a, d, t, cached ? m.mc_coef + e * q1 : a.mid_coef + (long long)(E0 + e) * q1, v);
+      if(hist) {
+        const double2 *h = m.hist + pb * kHistStride;
+        const int hb = hist_slot(t - d);
+#pragma unroll
+        for(int i = 0; i <= kMaxOrder; ++i) {
+          const int sl = hb - i < 0 ? hb - i + kHistDepth : hb - i;
+          v[i] = (i <= a.q && t - d - i >= -kWindow && d + i >= 2) ? h[sl] : make_double2(0.0, 0.0);
+        }
+      } else {
+        mid_old_fetch<true>(a, pb, d, t, tslot, v);
+      }
+      m.midv[e - c0] = cached ? mid_old_sum(a, d, t, m.mc_coef + e, cap, v)
+                              : mid_old_sum(a, d, t, a.mid_coef + (long long)(E0 + e) * q1, 1, v);
     }
     helpers_sync();
-    if(part == 1)
+    if(hw == 0)
       for(int e = max(my0, c0); e < min(my1, c1); ++e) {
         Mo.x += m.midv[e - c0].x;
         Mo.y += m.midv[e - c0].y;
@@ -706,68 +760,85 @@ __device__ __forceinline__ void block_precompute(const StepArgs &a, const BlockS
     helpers_sync();
   }
   if(!live) return;
-  if(part == 1) {
+  if(hw == 0) {
+    const double2 F = m.far[k * BS + lane];
     m.pre_f[b * BS + lane] = make_double2(F.x + Mo.x, F.y + Mo.y);
-    m.pre_p[b * BS + lane] = pul;
-  } else {
-    // warps 2..7: (p, P or H) = (1,P) (1,H) (2,P) (2,H) (3,P) (3,H)
-    const int w = part - 2, p = w / 2 + 1;
-    const SmemWindow src{m.win, lane};
-    double2 S[2];
-    if(w & 1)
-      pc_partial_half<NT, true>(a, m.ps, m.cs, t, p, src, S);
-    else
-      pc_partial_half<NT, false>(a, m.ps, m.cs, t, p, src, S);
-    const int v0 = (w & 1) ? 2 : 0;
-    double2 *ps = m.pre_s + b * 3 * 4 * BS;
-    ps[((p - 1) * 4 + v0) * BS + lane] = S[0];
-    ps[((p - 1) * 4 + v0 + 1) * BS + lane] = S[1];
   }
+  // window partials: helper warp hw takes (p, P or H) = (hw/2 + 1, hw odd)
+  const int p = hw / 2 + 1;
+  const SmemWindow src{m.win, lane};
+  double2 S[2];
+  if(hw & 1)
+    pc_partial_half<NT, true>(a, m.ps, m.cs, t, p, src, S);
+  else
+    pc_partial_half<NT, false>(a, m.ps, m.cs, t, p, src, S);
+  const int v0 = (hw & 1) ? 2 : 0;
+  double2 *ps = m.pre_s + b * 3 * 4 * BS;
+  ps[((p - 1) * 4 + v0) * BS + lane] = S[0];
+  ps[((p - 1) * 4 + v0 + 1) * BS + lane] = S[1];
 }
 
 template <int NT>
-__global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArgs a, int k0, int k1, unsigned *bar)
+__global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArgs a, int k0, int k1,
+                                                                          unsigned *flags)
 {
   constexpr int BS = 32;
   extern __shared__ double2 smem_block[];  // dynamic: above the 48 KB static limit
-  const BlockSmem m = block_smem(smem_block, a.q, a.mid_cache);
+  const BlockSmem m = block_smem(smem_block, a.q, a.mid_cache, a.hist_cap);
   __shared__ int s_abort;
   const int lane = threadIdx.x & 31, part = threadIdx.x >> 5;
+  const int hw = part < 4 ? part - 1 : part - 2;  // helper index; warp 0 -> -1, warp 4 -> 2 (unused)
+  const bool helper = part != 0 && part != 4;
   const int blk = blockIdx.x;
   const int idx = blk * BS + lane;
   const int t0 = *a.far_t0;
   const bool live = a.user[idx] >= 0;
   const int nt = NT > 0 ? NT : a.w.n_time;
-  const unsigned nb = gridDim.x;
+  const int B0 = a.pb_ptr[blk], NB = a.pb_ptr[blk + 1] - B0;  // blocks holding this block's partners
 
-  // window, weights, prev01, and the block's mid list when it fits
+  // prologue: window, weights, the launch's far field and pulse, prev01, and
+  // the block's mid list and partner history when they fit
   for(int sl = part; sl < kPcDepth; sl += kBlockWarps)
     for(int c = 0; c < 4; ++c) m.win[sl][c][lane] = a.pcr[((long long)sl * 4 + c) * a.n_pad + idx];
   for(int i = threadIdx.x; i < 2 * nt; i += blockDim.x) {
     m.ps[i] = a.w.ps[i];
     m.cs[i] = a.w.cs[i];
   }
+  for(int kk = k0 + part; kk < k1; kk += kBlockWarps) {
+    m.far[kk * BS + lane] = live ? a.far_field[(long long)kk * a.n_pad + idx] : make_double2(0.0, 0.0);
+    m.pul[kk * BS + lane] = live ? pulse_rabi(a, idx, t0 + kk) : 0.0;
+  }
   const int E0 = a.mid_ptr[blk * BS], E = a.mid_ptr[blk * BS + BS] - E0;
   const bool cached = E <= a.mid_cache;
+  const int P0 = a.bp_ptr[blk], NP = a.bp_ptr[blk + 1] - P0;
+  const bool hist = cached && a.hist_cap > 0 && NP <= a.hist_cap;
   if(cached) {
     const int q1 = a.q + 1;
-    for(int i = threadIdx.x; i < E * q1; i += blockDim.x) m.mc_coef[i] = a.mid_coef[(long long)E0 * q1 + i];
+    for(int i = threadIdx.x; i < E * q1; i += blockDim.x) {
+      const int e = i / q1, tap = i - e * q1;
+      m.mc_coef[tap * a.mid_cache + e] = a.mid_coef[(long long)E0 * q1 + i];
+    }
     for(int i = threadIdx.x; i < E; i += blockDim.x) {
-      m.mc_idx[i] = a.mid_idx[E0 + i];
+      m.mc_idx[i] = hist ? a.mid_pj[E0 + i] : a.mid_idx[E0 + i];
       m.mc_del[i] = a.mid_delay[E0 + i];
     }
   }
-  if(part == 0) m.prev01[lane] = a.ring[(long long)idx * a.stride + ring_slot(t0 + k0 - 1, a.W)];
-  if(part == 1 && live) {
-    m.pk[lane] = pulse_kr(a, idx);
-    for(int c = 0; c < 3; ++c) m.pk[32 * (c + 1) + lane] = a.dip[3 * idx + c];
+  if(hist) {
+    // samples t0+k0-22 .. t0+k0-2; later ones are appended step by step
+    const int first = t0 + k0 - kHistSpan, count = kHistSpan - 1;
+    for(int i = threadIdx.x; i < NP * count; i += blockDim.x) {
+      const int j = i / count, s = first + i % count;
+      m.hist[j * kHistStride + hist_slot(s)] = __ldcg(a.ring + (long long)a.bp_idx[P0 + j] * a.stride + ring_slot(s, a.W));
+    }
   }
+  if(part == 0) m.prev01[lane] = a.ring[(long long)idx * a.stride + ring_slot(t0 + k0 - 1, a.W)];
   if(threadIdx.x == 0) s_abort = 0;
   __syncthreads();
-  if(part > 0 && t0 + k0 < a.T) block_precompute<NT>(a, m, blk, k0, t0 + k0, k0 & 1, cached);
+  if(helper && t0 + k0 < a.T) block_precompute<NT>(a, m, blk, k0, t0 + k0, k0 & 1, cached, hist, hw);
   const DotConst dc = dot_const(a, idx, live);
   const bool block_near = a.near_ptr[(blk + 1) * BS] > a.near_ptr[blk * BS];
   const NearRegs nr = near_regs(a, idx);
+  const int nw0 = a.new_ptr[idx], nw1 = a.new_ptr[idx + 1];
   __syncthreads();
 
   for(int k = k0; k < k1; ++k) {
@@ -776,11 +847,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
     const int buf = k & 1;
     if(part == 0) {
       bool ok = true;
-      if(!a.lag && k > k0) {
-        // partners' step t-1 from other blocks: wait for all of them
-        ok = threadIdx.x != 0 || wait_count(bar, (unsigned)(k - k0) * nb);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-      }
+      if(!a.lag && k > k0) ok = wait_blocks(flags, a.pb_idx + B0, NB, k - k0);  // partners' step t-1
       if(ok) {
         double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
         double pul = 0;
@@ -797,18 +864,25 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
           pc_combine(S, T, P, H);
           double2 Mn;
           if(a.lag) {
-            Mn = mid_new(a, idx, [&](int b) { return m.prev01[b & 31]; });
+            Mn = mid_new(a, nw0, nw1, [&](int b) { return m.prev01[b & 31]; });
           } else {
             const int slot = ring_slot(t - 1, a.W);
-            Mn = mid_new(a, idx, [&](int b) { return __ldcg(a.ring + (long long)b * a.stride + slot); });
+            Mn = mid_new(a, nw0, nw1, [&](int b) { return __ldcg(a.ring + (long long)b * a.stride + slot); });
           }
           const double2 F = m.pre_f[buf * BS + lane];
           past = make_double2(F.x + Mn.x, F.y + Mn.y);
-          pul = m.pre_p[buf * BS + lane];
+          pul = m.pul[k * BS + lane];
         }
         dot_iterate(a, live, block_near, nr, m.cur, lane, P, H, past, pul, dc, r, dr);
+        // rho01 first, then post the step, then the rest of the state
+        if(live) finish_ring(a, idx, t, r);
+        __syncwarp();
+        if(lane == 0) {
+          __threadfence();
+          atomicAdd(flags + blk, 1u);
+        }
         if(live) {
-          finish_dot(a, idx, t, r, dr);
+          finish_state(a, idx, t, r, dr);
           const int sl = pc_slot(t);
           m.win[sl][0][lane] = r[0];
           m.win[sl][1][lane] = r[1];
@@ -822,22 +896,14 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
         s_abort = 1;
         atomicMin(a.d_bad, -2);
       }
-    } else {
-      // post this block's step k-1 (warp 0's stores precede the block
-      // barrier that ended it; the fence makes them visible device-wide first)
-      if(threadIdx.x == 32 && k > k0) {
-        __threadfence();
-        atomicAdd(bar, 1u);
+    } else if(helper && k + 1 < k1 && t + 1 < a.T) {
+      // step k+1's sums; M_old needs the partner blocks' step k-1
+      if(hw == 0 && k > k0 && !wait_blocks(flags, a.pb_idx + B0, NB, k - k0) && lane == 0) {
+        s_abort = 1;
+        atomicMin(a.d_bad, -2);
       }
-      if(k + 1 < k1 && t + 1 < a.T) {
-        // step k+1's sums; M_old needs every block's step k-1
-        if(threadIdx.x == 32 && !wait_count(bar, (unsigned)(k - k0) * nb)) {
-          s_abort = 1;
-          atomicMin(a.d_bad, -2);
-        }
-        helpers_sync();
-        if(!*(volatile int *)&s_abort) block_precompute<NT>(a, m, blk, k + 1, t + 1, buf ^ 1, cached);
-      }
+      helpers_sync();
+      if(!*(volatile int *)&s_abort) block_precompute<NT>(a, m, blk, k + 1, t + 1, buf ^ 1, cached, hist, hw);
     }
     __syncthreads();
   }
@@ -849,12 +915,12 @@ static void step_block_attrs(size_t smem)
   cudaFuncSetAttribute(step_block_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *bar, void *stream)
+void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *flags, void *stream)
 {
   cudaStream_t s = (cudaStream_t)stream;
-  const size_t smem = block_smem_bytes(a.q, a.mid_cache);
+  const size_t smem = block_smem_bytes(a.q, a.mid_cache, a.hist_cap);
   step_block_attrs(smem);
-  cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
+  cudaMemsetAsync(flags, 0, sizeof(unsigned) * nblocks, s);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
   cfg.blockDim = dim3(32 * kBlockWarps);
@@ -866,17 +932,17 @@ void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned 
   cfg.attrs = &attr;
   cfg.numAttrs = 1;
   if(a.w.n_time == 22)
-    cudaLaunchKernelEx(&cfg, step_block_kernel<22>, a, k0, k1, bar);
+    cudaLaunchKernelEx(&cfg, step_block_kernel<22>, a, k0, k1, flags);
   else
-    cudaLaunchKernelEx(&cfg, step_block_kernel<0>, a, k0, k1, bar);
+    cudaLaunchKernelEx(&cfg, step_block_kernel<0>, a, k0, k1, flags);
 }
 
 // Thread blocks of the step-block kernel that fit on the device at once
-// with a mid-list cache of `mid_cache` entries (0 when the shared memory
-// does not fit at all).
-int step_block_max_blocks(int q, int mid_cache)
+// with a mid-list cache of `mid_cache` entries and partner history for
+// `hist_cap` partners per block (0 when the shared memory does not fit).
+int step_block_max_blocks(int q, int mid_cache, int hist_cap)
 {
-  const size_t smem = block_smem_bytes(q, mid_cache);
+  const size_t smem = block_smem_bytes(q, mid_cache, hist_cap);
   int dev = 0, sms = 0, per = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
