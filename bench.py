@@ -14,6 +14,12 @@ this implementation once plus the delay-0 terms per iteration, both credited
 the same N^2 per step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload table|otf|batched|serving] [--precision fp64|mixed]
+
+--workload otf: N = 65536 dots in a 0.5 cube (max delay ~860 steps), same
+distributions, 5000-step run of which a bounded window is timed; the table
+would need 215 GB, so the far-pair kernel computes the coefficients on the
+fly.
 
 For N > 1 (torchrun), every rank advances its own independent ensemble
 (seed + rank) on its GPU: weak scaling, no data-path collective.
@@ -37,6 +43,10 @@ from quest_b200 import inputs as I  # noqa: E402
 
 FALLBACK_HBM_GBS = 6650.0
 TABLE_BYTES_PER_PAIR = lambda q: 4 + 16 * (q + 1)  # noqa: E731  int32 delay + (q+1) complex128
+# FP64 flops of one on-the-fly coefficient evaluation (pair_coef_otf, q = 5):
+# 6 reciprocals + node products and sums (~190), dyad scalars (~30), 6 taps
+# of complex assembly (~90), sqrt / modf / sincos counted as ~40
+OTF_COEF_FLOPS = 350
 
 
 def peaks():
@@ -112,6 +122,8 @@ class ClockSampler:
 
 
 def workload(args, rank: int) -> I.Workload:
+    if args.workload == "otf":
+        return I.mixed_large(seed=3 + rank, n=args.n, steps=5000, pulse_delay=args.pulse_delay)
     wl = I.plain_table(seed=2 + rank, n=args.n, steps=args.warmup + args.steps, pulse_delay=args.pulse_delay)
     if args.dipole_scale != 1.0:
         wl.dots[:, 6:9] *= args.dipole_scale
@@ -206,6 +218,10 @@ def run_reference(args, world, rank):
     steps = max(1, min(args.steps, args.cpu_steps))
     a = argparse.Namespace(**vars(args))
     a.cpu_steps = steps
+    if args.workload == "otf":
+        # the reference needs the full table (215 GB at N = 65536): its CPU
+        # rate is sampled on the table workload's size instead
+        a.n = 4096
     base = cpu_baseline(a)
     line = {"impl": "reference", "metric": "pair-updates/s", "value": base["value"], "unit": "pair-updates/s",
             "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": args.n * args.n / base["value"] * 1e3,
@@ -218,6 +234,13 @@ def run_reference(args, world, rank):
 
 
 def config_dict(args):
+    if args.workload == "otf":
+        return {"workload": f"{args.precision}_otf_N{args.n}_T5000", "N": args.n, "steps_total": 5000,
+                "steps_timed_window": [args.warmup, args.warmup + args.steps], "interpolation_order": 5,
+                "side": 0.5, "dt": 1e-3, "c0": 1.0, "hbar": 1.0, "mu0": 1.0, "laser_frequency": 200.0,
+                "pulse_delay": args.pulse_delay, "precision": args.precision, "coef_mode": "on_the_fly",
+                "l2": "inputs larger than L2 (rho01 ring %.0f MB > 126 MB)" % (args.n * 906 * 16 / 1e6),
+                "parallelism": "1 GPU"}
     return {"workload": f"{args.precision}_table_N{args.n}_T{args.warmup + args.steps}", "N": args.n,
             "steps_total": args.warmup + args.steps, "interpolation_order": 5, "side": 0.2,
             "dt": 1e-3, "c0": 1.0, "hbar": 1.0, "mu0": 1.0, "laser_frequency": 200.0,
@@ -241,7 +264,9 @@ def run_ours(args, world, rank, local):
     # ---- device-resident throughput (value) and the sweep kernel's roofline
     nonfinite = None
     prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
-    sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec)
+    otf = args.workload == "otf"
+    cmode = capi.COEF_ON_THE_FLY if otf else capi.COEF_TABLE
+    sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec, coef_mode=cmode)
     info = sim.info()
     try:
         sim.run(args.warmup, record=False)
@@ -276,7 +301,8 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec) as sim2:
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec,
+                         coef_mode=cmode) as sim2:
         try:
             sim2.run(total, out=rho_host)
         except capi.NonFiniteError:
@@ -301,6 +327,27 @@ def run_ours(args, world, rank, local):
     fp64_tf = flops / (avg_ms / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops("float32" if mixed else "float64")
     traffic = profile_traffic("far_kernel_fp64_N4096")  # ncu dram read+write per launch
+    if otf:
+        # compute-bound: every ordered pair's coefficients (FP64) once per
+        # launch plus the K-step convolution (FP64, or FP32 in mixed)
+        coef_flops = 2 * (info["num_pairs"]) * OTF_COEF_FLOPS
+        d_peak = fp64_peak if not mixed else fp64_peak_tflops("float64")
+        t_s = avg_ms / 1e3
+        # time-weighted peak: coefficient flops at the FP64 rate, convolution
+        # flops at the precision's rate
+        ideal_s = coef_flops / (d_peak * 1e12) + flops / (fp64_peak * 1e12)
+        roof = {"bound": "fp64" if not mixed else "fp64+fp32", "kernel": "far_otf_kernel<5,false,%s>" %
+                ("true" if mixed else "false"),
+                "achieved": (coef_flops + flops) / t_s / 1e12, "unit": "TFLOP/s",
+                "peak": (coef_flops + flops) / ideal_s / 1e12, "peak_source": "measured here: best cuBLAS "
+                "DGEMM%s 8192^3" % (" and SGEMM (no TF32)" if mixed else ""),
+                "frac": ideal_s / t_s, "traffic": None,
+                "coef_flops_per_launch": coef_flops, "conv_flops_per_launch": flops,
+                "coef_flops_per_pair": OTF_COEF_FLOPS, "steps_per_launch": K, "avg_launch_ms": avg_ms,
+                "share_of_timed_region": pair_ms / ms if ms > 0 else None,
+                "step_kernels_ms_per_step": step_ms / max(launches * K, 1),
+                "step_form": {0: "general (12 launches per step)", 1: "fused (1 launch per step)",
+                              2: "block (1 cooperative launch per 16 steps)"}[info["fused_step"]]}
     line = {
         "metric": "pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -308,7 +355,7 @@ def run_ours(args, world, rank, local):
         "dtype": "f32 pair sum + f64 state (mixed)" if mixed else "f64",
         "data": "synthetic (seeded dots and pulse of the stated distributions)",
         "config": config_dict(args),
-        "roofline": {"bound": "hbm", "kernel": "far_kernel<5,false>", "achieved": achieved, "peak": hbm,
+        "roofline": roof if otf else {"bound": "hbm", "kernel": "far_kernel<5,false>", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "steps_per_launch": K,
                      "avg_launch_ms": avg_ms, "share_of_timed_region": pair_ms / ms if ms > 0 else None,
@@ -323,7 +370,8 @@ def run_ours(args, world, rank, local):
                                                                                    else "DGEMM")}},
         "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s,
                 "h2d_bytes_per_step": (n * 72 + 80) / total, "d2h_bytes_per_step": n * 32,
-                "includes": "qg_create (dots upload + table build) + qg_run with every step's rho read back"},
+                "includes": "qg_create (dots upload + %s) + qg_run with every step's rho read back" %
+                            ("max-delay and pair-list kernels" if otf else "table build")},
         "gpu_launches": launches + step_launches,
         "near_pairs": info["near_pairs"], "mid_pairs": info["mid_pairs"], "max_delay": info["max_delay"],
         "nonfinite_from_step": nonfinite,
@@ -332,7 +380,7 @@ def run_ours(args, world, rank, local):
     cs = clocks.summary()
     if cs is not None:
         line["clocks"] = cs
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not otf:
         line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -416,17 +464,17 @@ def run_serving(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=19950)
-    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--pulse-delay", type=float, default=5.0)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-t0", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dipole-scale", type=float, default=1.0)
     ap.add_argument("--far-variant", type=int, default=0)
-    ap.add_argument("--workload", choices=["table", "batched", "serving"], default="table")
+    ap.add_argument("--workload", choices=["table", "otf", "batched", "serving"], default="table")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--ensembles", type=int, default=256)
     ap.add_argument("--blocks-per-round", type=int, default=8)
@@ -435,6 +483,13 @@ def main():
     ap.add_argument("--serve-nmax", type=int, default=16384)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     args = ap.parse_args()
+    otf = args.workload == "otf"
+    if args.n is None:
+        args.n = 65536 if otf else 4096
+    if args.steps is None:
+        args.steps = 160 if otf else 19950
+    if args.warmup is None:
+        args.warmup = 16 if otf else 50
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_setup(args)

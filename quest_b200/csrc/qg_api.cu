@@ -65,6 +65,8 @@ struct qg_handle_s {
   float2 *d_coef32 = nullptr;              // mixed precision table
   float2 *d_ring32w = nullptr, *d_ring32d = nullptr;
   bool mixed = false;
+  bool otf = false;  // coefficients computed in the far kernel (no table)
+  int group = kTileGroup;  // source tiles per far-kernel warp
   double2 *d_ring = nullptr;
   int W = 0, stride = 0;
   double2 *d_pcr = nullptr, *d_partial = nullptr, *d_field = nullptr, *d_scratch = nullptr;
@@ -147,6 +149,18 @@ struct qg_handle_s {
     s.d_t0 = d_t0;
     s.far_t0_out = far_t0_out;
     s.variant = far_variant;
+    s.otf = otf ? 1 : 0;
+    s.group = group;
+    s.pos = d_pos;
+    s.dip = d_dip;
+    s.user = d_user;
+    s.cp.c0 = params.c0;
+    s.cp.dt = params.dt;
+    s.cp.mu0 = params.mu0;
+    s.cp.hbar = params.hbar;
+    s.cp.omega = params.laser_frequency;
+    s.cp.q = q;
+    s.cp.frame = params.frame;
     return s;
   }
 
@@ -338,9 +352,7 @@ static qg_status validate(const qg_dot *dots, int n, const qg_pulse *pulse, cons
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown frame %d", p->frame);
   if(p->precision != QG_PREC_FP64 && p->precision != QG_PREC_MIXED)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown precision %d", p->precision);
-  if(p->coef_mode == QG_COEF_ON_THE_FLY)
-    return qg_fail(QG_ERR_UNSUPPORTED, "qg_create: on-the-fly coefficients use qg_otf_* handles");
-  if(p->coef_mode != QG_COEF_AUTO && p->coef_mode != QG_COEF_TABLE)
+  if(p->coef_mode != QG_COEF_AUTO && p->coef_mode != QG_COEF_TABLE && p->coef_mode != QG_COEF_ON_THE_FLY)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown coef_mode %d", p->coef_mode);
   return QG_OK;
 }
@@ -420,6 +432,7 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
     mid[a].push_back({b, d, k});
     mid[b].push_back({a, d, k});
     if(d == 0) {
+      if(h->otf) ++h->near_pairs;
       adj[a].push_back({b, mc[k * q1]});
       adj[b].push_back({a, mc[k * q1]});
       dsu.unite(a, b);
@@ -761,18 +774,27 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaMemset(h->d_ints, 0, sizeof(int) * 16));
   QG_CUDA(cudaMemset(h->d_u64, 0, sizeof(unsigned long long) * 4));
 
-  // coefficient table
+  // coefficients: a table when asked for, or (auto) when it takes at most
+  // half of the free device memory; otherwise computed in the far kernel
   h->mixed = p->precision == QG_PREC_MIXED;
   const size_t tb = table_bytes(h->nT, h->q, h->mixed);
   size_t free_b = 0, total_b = 0;
   QG_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  if(tb > free_b * 0.9)
+  h->otf = p->coef_mode == QG_COEF_ON_THE_FLY || (p->coef_mode == QG_COEF_AUTO && tb > free_b / 2);
+  if(!h->otf && tb > free_b * 0.9)
     return qg_fail(QG_ERR_OOM, "qg_create: coefficient table needs %zu bytes, %zu free", tb, free_b);
-  QG_TRY(dalloc(h, &h->d_delay, (size_t)h->nT * h->nT * kTilePairs));
-  if(h->mixed)
-    QG_TRY(dalloc(h, &h->d_coef32, (size_t)h->nT * h->nT * kTilePairs * (h->q + 2)));
-  else
-    QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nT * h->nT * kTilePairs * (h->q + 1)));
+  if(h->otf) {
+    // about 16 source groups per target tile: enough warps for the device,
+    // partial sums of K x 16 x n_pad
+    h->group = (h->nT + 15) / 16;
+    h->nG = (h->nT + h->group - 1) / h->group;
+  } else {
+    QG_TRY(dalloc(h, &h->d_delay, (size_t)h->nT * h->nT * kTilePairs));
+    if(h->mixed)
+      QG_TRY(dalloc(h, &h->d_coef32, (size_t)h->nT * h->nT * kTilePairs * (h->q + 2)));
+    else
+      QG_TRY(dalloc(h, &h->d_coef, (size_t)h->nT * h->nT * kTilePairs * (h->q + 1)));
+  }
   TableArgs ta{};
   ta.pos = h->d_pos;
   ta.dip = h->d_dip;
@@ -798,7 +820,10 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaEventCreate(&e0));
   QG_CUDA(cudaEventCreate(&e1));
   QG_CUDA(cudaEventRecord(e0, h->stream));
-  launch_table_build(ta, h->q, h->stream);
+  if(h->otf)
+    launch_max_delay(h->d_pos, h->d_user, h->n_pad, p->c0 * p->dt, h->d_ints + 5, h->stream);
+  else
+    launch_table_build(ta, h->q, h->stream);
   QG_CUDA(cudaGetLastError());
   QG_CUDA(cudaEventRecord(e1, h->stream));
   int md = 0;
@@ -815,7 +840,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: floor delay %d out of range (non-finite positions?)",
                    md);
   h->max_delay = md;
-  h->near_pairs = (long long)nn[0];
+  h->near_pairs = (long long)nn[0];  // on the fly: counted from the mid list below
   h->mid_pairs = (long long)nn[1];
 
   // rings and scratch.  W covers the oldest sample a far block reads
@@ -1198,6 +1223,9 @@ extern "C" qg_status qg_batch_add(qg_batch *b, qg_handle *h)
   if(!h->fused)
     return qg_fail(QG_ERR_UNSUPPORTED,
                    "qg_batch_add: a group of dots coupled at delay 0 exceeds 32; run this handle alone");
+  if(h->otf)
+    return qg_fail(QG_ERR_UNSUPPORTED,
+                   "qg_batch_add: the handle computes its coefficients on the fly; run it alone");
   if(h->next_step % kTimeBlock != 0)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_add: next step %d is not a multiple of %d", h->next_step,
                    kTimeBlock);
@@ -1375,6 +1403,10 @@ extern "C" qg_status qg_history_evaluate_noalloc(qg_handle *h, int step, const d
     return qg_fail(QG_ERR_INVALID_ARG, "qg_history_evaluate_noalloc: NULL handle or output");
   if(step < 0 || step >= std::max(h->T, 1))
     return qg_fail(QG_ERR_INVALID_ARG, "qg_history_evaluate_noalloc: step %d outside [0, %d)", step, h->T);
+  if(h->otf)
+    return qg_fail(QG_ERR_UNSUPPORTED,
+                   "qg_history_evaluate_noalloc: the handle computes its coefficients on the fly; "
+                   "use qg_history_evaluate");
   if(h->n_pad > kNoAllocMaxDots)
     return qg_fail(QG_ERR_INVALID_ARG,
                    "qg_history_evaluate_noalloc: %d dots (%d padded) exceed the fixed scratch, "
@@ -1459,7 +1491,7 @@ extern "C" qg_status qg_get_info(const qg_handle *h, qg_info *info)
   info->near_pairs = h->near_pairs;
   info->mid_pairs = h->mid_pairs;
   info->time_block = kTimeBlock;
-  info->coef_mode = QG_COEF_TABLE;
+  info->coef_mode = h->otf ? QG_COEF_ON_THE_FLY : QG_COEF_TABLE;
   info->precision = h->mixed ? QG_PREC_MIXED : QG_PREC_FP64;
   info->fused_step = h->fused ? (h->block_step ? 2 : 1) : 0;
   info->device_bytes = h->bytes;
@@ -1471,12 +1503,14 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
 {
   if(!p || !bytes || n < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_footprint: bad argument");
   const int nT = (n + kTile - 1) / kTile, n_pad = nT * kTile;
-  const int nG = (nT + kTileGroup - 1) / kTileGroup;
+  const bool otf = p->coef_mode == QG_COEF_ON_THE_FLY;
+  const int group = otf ? (nT + 15) / 16 : kTileGroup;
+  const int nG = (nT + group - 1) / group;
   const int q = p->interpolation_order;
   const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
   const int W = ring_depth(md, q);
   const bool mixed = p->precision == QG_PREC_MIXED;
-  size_t b = table_bytes(nT, q, mixed);
+  size_t b = otf ? 0 : table_bytes(nT, q, mixed);
   b += sizeof(double2) * (size_t)n_pad * (W + kRingMirror) * (mixed ? 2 : 1);
   b += sizeof(double2) * (size_t)kPcDepth * 4 * n_pad;
   b += sizeof(double2) * (size_t)kTimeBlock * (nG + 1) * n_pad + sizeof(unsigned) * nT;

@@ -152,4 +152,90 @@ __device__ __forceinline__ int pair_coef_ref(const double (&psrc)[3], const doub
   return fd;
 }
 
+// The same pair's floor delay and coefficients for the on-the-fly path,
+// in an algebraically equal but cheaper form (about 400 instead of about
+// 5000 instructions per pair):
+//   Lagrange weights   one reciprocal r_m = 1/(x-m) per node, then for node b
+//                      w0 = prod_{m!=b} (x-m) / prod_{m!=b} (b-m),
+//                      w1 = w0 d1 / dt, w2 = w0 (d2 + d1^2) / dt^2 with
+//                      d1 = -sum_{m!=b} r_m, d2 = -sum_{m!=b} r_m^2
+//                      (the reference's w0 d2 + w1^2 / w0 with w1 = w0 d1);
+//   dyads              contracted with the dipoles first: d_obs.(I - 3 rr).d_src
+//                      = dd - 3 (d_obs.r)(d_src.r)/r^2 and d_obs.(I - rr).d_src
+//                      = dd - (d_obs.r)(d_src.r)/r^2, so each tap needs three
+//                      real scalars G0 = (dd - 3ab/r^2) c^2/r^3,
+//                      G1 = (dd - 3ab/r^2) c/r^2, G2 = (dd - ab/r^2)/r;
+//   rotating frame     coef_i = s (G0 w0 + G1 (w1 + i om w0) + G2 (w2 + 2 i om w1
+//                      - om^2 w0)), s = -mu0/(4 pi hbar) e^{-i om r/c};
+//   lab frame          coef_i = mu0/(4 pi hbar) (G0 w0 + G1 w1 + G2 w2).
+// The floor delay uses exactly the operations of pair_coef_ref (and of the
+// near-pair search), so the far / mid split is the same as the table's; the
+// coefficients agree with the reference's to rounding.
+template <int Q>
+__device__ __forceinline__ int pair_coef_otf(const double (&psrc)[3], const double (&pobs)[3],
+                                             const double (&dsrc)[3], const double (&dobs)[3],
+                                             const CoefParams &p, double2 (&coef)[Q + 1])
+{
+  double dr[3];
+#pragma unroll
+  for(int k = 0; k < 3; ++k) dr[k] = pobs[k] - psrc[k];
+  const double sq = (dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2];
+  const double nrm = sqrt(sq);
+  double idelay;
+  const double x = modf(nrm / (p.c0 * p.dt), &idelay);
+  const int fd = (int)idelay;
+
+  double xm[Q + 1], rm[Q + 1];
+#pragma unroll
+  for(int m = 0; m <= Q; ++m) {
+    xm[m] = x - m;
+    rm[m] = 1.0 / xm[m];
+  }
+  const double inv_dt = 1.0 / p.dt, inv_dt2 = inv_dt * inv_dt;
+  double w0[Q + 1], w1[Q + 1], w2[Q + 1];
+#pragma unroll
+  for(int b = 0; b <= Q; ++b) {
+    double num = 1.0, den = 1.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+    for(int m = 0; m <= Q; ++m) {
+      if(m == b) continue;
+      num *= xm[m];
+      den *= (double)(b - m);
+      d1 -= rm[m];
+      d2 -= rm[m] * rm[m];
+    }
+    w0[b] = num / den;
+    w1[b] = (w0[b] * d1) * inv_dt;
+    w2[b] = (w0[b] * (d2 + d1 * d1)) * inv_dt2;
+  }
+
+  const double dd = (dobs[0] * dsrc[0] + dobs[1] * dsrc[1]) + dobs[2] * dsrc[2];
+  const double ar = (dobs[0] * dr[0] + dobs[1] * dr[1]) + dobs[2] * dr[2];
+  const double br = (dsrc[0] * dr[0] + dsrc[1] * dr[1]) + dsrc[2] * dr[2];
+  const double inv_r = 1.0 / nrm, inv_sq = 1.0 / sq;
+  const double ab = (ar * br) * inv_sq;
+  const double g3 = dd - 3.0 * ab, g1 = dd - ab;
+  const double G0 = (g3 * (p.c0 * p.c0)) * (inv_sq * inv_r);
+  const double G1 = (g3 * p.c0) * inv_sq;
+  const double G2 = g1 * inv_r;
+  const double A = p.mu0 / (4 * M_PI * p.hbar);
+  if(p.frame == 0) {
+    const double om = p.omega;
+    double sn, cs;
+    sincos((-om * nrm) / p.c0, &sn, &cs);
+    const double2 s = make_double2(-A * cs, -A * sn);
+    const double om2 = om * om;
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) {
+      const double re = (G0 * w0[i] + G1 * w1[i]) + G2 * (w2[i] - om2 * w0[i]);
+      const double im = om * (G1 * w0[i] + 2.0 * (G2 * w1[i]));
+      coef[i] = cmul(s, make_double2(re, im));
+    }
+  } else {
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) coef[i] = make_double2(A * ((G0 * w0[i] + G1 * w1[i]) + G2 * w2[i]), 0.0);
+  }
+  return fd;
+}
+
 }  // namespace qg

@@ -81,6 +81,14 @@ struct FarArgs {
   const int *d_t0;      // first step of the block
   int *far_t0_out;      // receives *d_t0 (read by the dot-step kernels)
   int variant;          // kernel variant (same results), see qg_far.cu
+  // on-the-fly coefficients (no table): dot data, constants, and the source
+  // tiles per warp (nG = ceil(nT / group) groups)
+  int otf;
+  int group;
+  const double *pos;    // [n_pad][3]
+  const double *dip;    // [n_pad][3]
+  const int *user;      // internal -> user index, -1 for padding
+  CoefParams cp;
 };
 
 // Arguments of the per-dot step kernels.
@@ -167,6 +175,8 @@ void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, in
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);
 void launch_far(const FarArgs &a, void *stream);
+void launch_far_otf(const FarArgs &a, void *stream);
+void launch_max_delay(const double *pos, const int *user, int n_pad, double c0dt, int *max_delay, void *stream);
 void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int below, int *out_pairs,
                       unsigned long long *counter, unsigned long long cap, void *stream);
 void launch_pair_list_coef(const TableArgs &a, int q, const int *pairs, long long m, double2 *out, void *stream);

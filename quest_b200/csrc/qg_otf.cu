@@ -1,0 +1,145 @@
+// Far-pair kernel with on-the-fly coefficients: the same K-step sum as the
+// table path (qg_far.cu) for ensembles whose coefficient table does not fit
+// in device memory (N = 65536 needs 215 GB in FP64).  Each warp owns a
+// target tile (lane = target dot) and a group of `group` source tiles; for
+// every source the 32 lanes compute their pair's floor delay and q+1
+// coefficients (pair_coef_otf, in the reference's orientation: src = larger
+// user index) and, for pairs with delay >= K, apply them to the source's
+// K + q window exactly as the table path does.  The coefficients are
+// computed once per pair per K steps, so about 400 instructions of
+// coefficient work are shared by K = 16 steps of (q+1)-tap convolution.
+//
+// FP64: FP64 coefficients and convolution.  Mixed: FP64 coefficients,
+// rounded to FP32 with their sum as the table build does, and the FP32
+// difference-form convolution of the mixed table path.
+//
+// Compiled with -fmad=false (the delay arithmetic must match the near-pair
+// search bit for bit); the convolution's products are explicit fused
+// multiply-adds, so they round as in the table path.
+#include <cuda_runtime.h>
+
+#include "qg_coef.cuh"
+#include "qg_conv.cuh"
+
+namespace qg {
+
+template <int Q, bool LAB, bool MIXED, int K = kTimeBlock>
+__device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
+{
+  const int lane = threadIdx.x & 31;
+  if(task >= a.nT * a.nG) return;  // uniform per warp
+  const int I = task / a.nG, g = task % a.nG;
+  const int J0 = g * a.group;
+  const int nJ = min(a.group, a.nT - J0);
+  const int t0 = *a.d_t0;
+  if(task == 0 && lane == 0) *a.far_t0_out = t0;
+  const int W = a.W;
+  const int ia = I * kTile + lane;
+  const int ua = a.user[ia];
+  double pa[3], da[3];
+#pragma unroll
+  for(int k = 0; k < 3; ++k) {
+    pa[k] = a.pos[3 * ia + k];
+    da[k] = a.dip[3 * ia + k];
+  }
+
+  double2 acc[K];
+  float2 accf[K];
+#pragma unroll
+  for(int k = 0; k < K; ++k) {
+    acc[k] = make_double2(0.0, 0.0);
+    accf[k] = make_float2(0.f, 0.f);
+  }
+
+  const int iters = nJ * kTile;
+  for(int it = 0; it < iters; ++it) {
+    const int ib = J0 * kTile + it;
+    const int ub = __ldg(a.user + ib);  // the same source for all lanes
+    const bool valid = ia != ib && ua >= 0 && ub >= 0;
+    if(!__any_sync(0xffffffffu, valid)) continue;
+    double pb[3], db[3];
+#pragma unroll
+    for(int k = 0; k < 3; ++k) {
+      pb[k] = __ldg(a.pos + 3 * ib + k);
+      db[k] = __ldg(a.dip + 3 * ib + k);
+    }
+    // reference orientation: src = larger user index
+    const bool a_src = ua > ub;
+    double ps[3], po[3], ds[3], dob[3];
+#pragma unroll
+    for(int k = 0; k < 3; ++k) {
+      ps[k] = a_src ? pa[k] : pb[k];
+      po[k] = a_src ? pb[k] : pa[k];
+      ds[k] = a_src ? da[k] : db[k];
+      dob[k] = a_src ? db[k] : da[k];
+    }
+    double2 c[Q + 1];
+    const int d = pair_coef_otf<Q>(ps, po, ds, dob, a.cp, c);
+    if(valid && d >= kTimeBlock) {
+      const int tau0 = t0 - d - Q;
+      int slot0 = tau0 % W;
+      if(slot0 < 0) slot0 += W;
+      if(MIXED) {
+        float2 cf[Q + 2];
+        double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+        for(int i = 0; i <= Q; ++i) {
+          cf[i] = make_float2((float)c[i].x, (float)c[i].y);
+          sum.x += c[i].x;
+          sum.y += c[i].y;
+        }
+        cf[Q + 1] = make_float2((float)sum.x, (float)sum.y);
+        window_conv_mixed<Q, LAB, K>(a.ring32w + (long long)ib * a.stride, a.ring32d + (long long)ib * a.stride,
+                                     slot0, tau0, cf, accf);
+      } else {
+        window_conv<Q, LAB, K>(a.ring + (long long)ib * a.stride, slot0, tau0, c, acc);
+      }
+    }
+  }
+  if(MIXED) {
+#pragma unroll
+    for(int k = 0; k < K; ++k) acc[k] = make_double2((double)accf[k].x, (double)accf[k].y);
+  }
+  group_partials_reduce<K>(a, I, g, acc);
+}
+
+template <int Q, bool LAB, bool MIXED>
+__global__ void __launch_bounds__(128) far_otf_kernel(FarArgs a)
+{
+  far_body_otf<Q, LAB, MIXED>(a, blockIdx.x * 4 + (threadIdx.x >> 5));
+}
+
+template <bool LAB, bool MIXED>
+static void launch_otf_q(const FarArgs &a, cudaStream_t s)
+{
+  const unsigned blocks = (unsigned)(((long long)a.nT * a.nG + 3) / 4);
+  switch(a.q) {
+    case 1: far_otf_kernel<1, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    case 2: far_otf_kernel<2, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    case 3: far_otf_kernel<3, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    case 4: far_otf_kernel<4, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    case 5: far_otf_kernel<5, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    case 6: far_otf_kernel<6, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    case 7: far_otf_kernel<7, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    default: break;
+  }
+}
+
+void launch_far_otf(const FarArgs &a, void *stream)
+{
+  if(a.nT <= 0) return;
+  cudaStream_t s = (cudaStream_t)stream;
+  if(a.frame == 0) {
+    if(a.mixed)
+      launch_otf_q<false, true>(a, s);
+    else
+      launch_otf_q<false, false>(a, s);
+  } else {
+    if(a.mixed)
+      launch_otf_q<true, true>(a, s);
+    else
+      launch_otf_q<true, false>(a, s);
+  }
+}
+
+}  // namespace qg

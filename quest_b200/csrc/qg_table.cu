@@ -163,6 +163,45 @@ __global__ void near_find_kernel(const double *pos, const int *user, int n_pad, 
   out_pairs[3 * slot + 2] = (int)idelay;
 }
 
+// The largest floor delay over all pairs (for the ring depth when no table
+// is built), with the delay arithmetic of pair_coef_ref.
+__global__ void __launch_bounds__(256) max_delay_kernel(const double *pos, const int *user, int n_pad, double c0dt,
+                                                        int *out)
+{
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nt = (n_pad + kTile - 1) / kTile;
+  const long long nblk = nt * (nt + 1) / 2;
+  int v = -1;
+  if(gid < nblk * kTilePairs) {
+    int I, J;
+    decode_block(gid / kTilePairs, I, J);
+    const int e = (int)(gid % kTilePairs);
+    const int la = e / kTile, lb = e % kTile;
+    const int ia = I * kTile + la, ib = J * kTile + lb;
+    if(!(I == J && la <= lb) && ia < n_pad && ib < n_pad && user[ia] >= 0 && user[ib] >= 0) {
+      const int ua = user[ia], ub = user[ib];
+      const int is = ua > ub ? ia : ib, io = ua > ub ? ib : ia;
+      double dr[3];
+#pragma unroll
+      for(int k = 0; k < 3; ++k) dr[k] = pos[3 * io + k] - pos[3 * is + k];
+      const double nrm = sqrt((dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2]);
+      double idelay;
+      modf(nrm / c0dt, &idelay);
+      v = (int)idelay;
+    }
+  }
+  v = __reduce_max_sync(0xffffffffu, v);
+  if((threadIdx.x & 31) == 0 && v >= 0) atomicMax(out, v);
+}
+
+void launch_max_delay(const double *pos, const int *user, int n_pad, double c0dt, int *max_delay, void *stream)
+{
+  const long long nt = (n_pad + kTile - 1) / kTile;
+  const long long total = nt * (nt + 1) / 2 * kTilePairs;
+  const unsigned blocks = (unsigned)((total + 255) / 256);
+  max_delay_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(pos, user, n_pad, c0dt, max_delay);
+}
+
 // FP64 coefficients of listed pairs (the per-step mid list), computed as the
 // table build computes them.
 template <int Q>

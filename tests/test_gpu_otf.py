@@ -1,0 +1,149 @@
+"""On-the-fly coefficients (no table): the far-pair kernel computes every
+pair's floor delay and q+1 coefficients in registers each K-step block, in
+an algebraically equal form of the reference's table build.
+
+Checks: the interaction-level sum (HistoryInteraction::evaluate) against the
+oracle's reference-order table on random histories, whole runs against the
+oracle at the FP64 tolerance (1e-10), against the table path, in the lab
+frame and at other interpolation orders, mixed precision against FP64, and
+the N = 65536 workload (whose table would need 215 GB) for a few blocks."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from quest_b200 import capi, inputs as I
+from tests.conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def run(wl, weights, steps, **kw):
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, **kw) as sim:
+        rho = sim.run(steps)
+        info = sim.info()
+    return rho, info
+
+
+def parity(hist, rho):
+    ref = O.rho_trajectory(hist)[: rho.shape[0]]
+    return rel_err(ref[..., 0], rho[..., 0]), rel_err(ref[..., 1], rho[..., 1])
+
+
+def stable(n, steps, pulse_delay, side=0.2, seed=2):
+    wl = I.plain_small(n=n, steps=steps, pulse_delay=pulse_delay)
+    wl.dots[:, 8] = 2e-4
+    return wl
+
+
+def test_otf_info_matches_table(golden_weights):
+    wl = stable(700, 32, 0.1)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights,
+                         coef_mode=capi.COEF_TABLE) as a, \
+            capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights,
+                            coef_mode=capi.COEF_ON_THE_FLY) as b:
+        ia, ib = a.info(), b.info()
+    assert ib["coef_mode"] == capi.COEF_ON_THE_FLY and ia["coef_mode"] == capi.COEF_TABLE
+    for key in ("max_delay", "ring_depth", "near_pairs", "mid_pairs", "num_pairs"):
+        assert ia[key] == ib[key], key
+    assert ib["device_bytes"] < ia["device_bytes"]
+
+
+def test_otf_history_evaluate_matches_reference_table(golden_weights):
+    wl = I.plain_small(n=150, steps=400)
+    c = wl.constants
+    n = wl.n
+    rng = np.random.default_rng(11)
+    T = 400
+    hist = np.zeros((n, T + O.WINDOW, 2, 2), dtype=np.complex128)
+    hist[:, :, 0, 1] = rng.normal(size=(n, T + O.WINDOW)) + 1j * rng.normal(size=(n, T + O.WINDOW))
+    delays, coefs = O.build_table(wl.dots, c)
+    with capi.Simulation(wl.dots, wl.pulse, c, weights=golden_weights, coef_mode=capi.COEF_ON_THE_FLY) as sim:
+        W = sim.info()["ring_depth"]
+        for step in [0, 60, 250, 399]:
+            lo = max(-O.WINDOW, step - W + 1)
+            sim.set_history(lo, hist[:, lo + O.WINDOW: step + O.WINDOW, 0, 1].T)
+            got = sim.history_evaluate(step, hist[:, step + O.WINDOW, 0, 1])
+            ref = O.history_evaluate(wl.dots, c, delays, coefs, hist, step)
+            assert rel_err(ref, got) < 1e-12, step
+
+
+def test_otf_against_oracle(golden_weights, oracle_weights):
+    wl = I.plain_small(n=60, steps=350, pulse_delay=0.2)
+    hist, bad = O.run_faithful(wl.dots, wl.pulse, wl.constants, oracle_weights, 350)
+    assert bad is None
+    rho, info = run(wl, golden_weights, 350, coef_mode=capi.COEF_ON_THE_FLY)
+    assert info["coef_mode"] == capi.COEF_ON_THE_FLY
+    e00, e01 = parity(hist, rho)
+    assert e00 <= TOL and e01 <= TOL, (e00, e01)
+    assert np.abs(rho[..., 1]).max() > 1e-6
+
+
+def test_otf_stable_run_against_oracle_and_table(golden_weights, oracle_weights):
+    wl = stable(1000, 600, 0.1)
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, 600)
+    assert bad is None
+    got, _ = run(wl, golden_weights, 600, coef_mode=capi.COEF_ON_THE_FLY)
+    e00, e01 = parity(hist, got)
+    assert e00 <= TOL and e01 <= TOL, (e00, e01)
+    tab, _ = run(wl, golden_weights, 600, coef_mode=capi.COEF_TABLE)
+    assert rel_err(tab[..., 1], got[..., 1]) <= 1e-11
+    assert rel_err(tab[..., 0], got[..., 0]) <= 1e-11
+
+
+@pytest.mark.parametrize("q,frame,steps", [(3, 0, 300), (7, 0, 200), (5, 1, 300)])
+def test_otf_orders_and_lab_frame(golden_weights, oracle_weights, q, frame, steps):
+    """Horizons as in the table path's tests: order 7 amplifies rounding
+    differences (here: coefficient rounding) faster than order 5."""
+    wl = I.plain_small(n=90, steps=steps, pulse_delay=0.15)
+    wl.constants.interpolation_order = q
+    wl.constants.frame = frame
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, steps)
+    assert bad is None
+    rho, _ = run(wl, golden_weights, steps, coef_mode=capi.COEF_ON_THE_FLY)
+    e00, e01 = parity(hist, rho)
+    assert e00 <= TOL and e01 <= TOL, (e00, e01)
+
+
+def test_otf_mixed_matches_fp64(golden_weights):
+    wl = stable(1000, 600, 0.1)
+    ref, _ = run(wl, golden_weights, 600, coef_mode=capi.COEF_ON_THE_FLY)
+    got, info = run(wl, golden_weights, 600, coef_mode=capi.COEF_ON_THE_FLY, precision=capi.PREC_MIXED)
+    assert info["precision"] == capi.PREC_MIXED and info["coef_mode"] == capi.COEF_ON_THE_FLY
+    assert rel_err(ref[..., 0], got[..., 0]) <= 1e-6
+    assert rel_err(ref[..., 1], got[..., 1]) <= 1e-6
+
+
+def test_otf_rejected_where_a_table_is_needed(golden_weights):
+    import ctypes
+    import torch
+
+    wl = stable(100, 32, 0.1)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights,
+                         coef_mode=capi.COEF_ON_THE_FLY) as sim:
+        out = torch.empty((wl.n,), dtype=torch.complex128, device="cuda")
+        rc = capi.lib().qg_history_evaluate_noalloc(sim.h, 0, None, ctypes.c_void_p(out.data_ptr()), None)
+        assert rc == capi.QG_ERR_UNSUPPORTED
+        assert "on the fly" in capi.lib().qg_last_error().decode()
+        b = capi.Batch(2)
+        try:
+            with pytest.raises(capi.QuestError):
+                b.add(sim)
+        finally:
+            b.close()
+
+
+def test_otf_n65536_blocks(golden_weights):
+    """The N = 65536, 0.5-cube workload (table: 215 GB): creation, two
+    16-step blocks in mixed precision and FP64, finite states, the far
+    field nonzero once the history is."""
+    wl = I.mixed_large(n=65536, steps=5000)
+    for prec in (capi.PREC_MIXED, capi.PREC_FP64):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights, precision=prec) as sim:
+            info = sim.info()
+            assert info["coef_mode"] == capi.COEF_ON_THE_FLY
+            assert 850 <= info["max_delay"] <= 870
+            sim.run(32, record=False)
+            st = sim.state()
+            assert np.all(np.isfinite(st))
