@@ -272,7 +272,8 @@ def run_ours(args, world, rank, local):
         sim.run(args.warmup, record=False)
     except capi.NonFiniteError as e:
         nonfinite = e.step
-    sim.set_option("far_variant", args.far_variant)
+    if args.far_variant is not None:
+        sim.set_option("far_variant", args.far_variant)
     sim.set_option("profile", 1)
     sim.kernel_time(reset=True)
     stream = torch.cuda.ExternalStream(capi.lib().qg_stream(sim.h))
@@ -355,14 +356,15 @@ def run_ours(args, world, rank, local):
         "dtype": "f32 pair sum + f64 state (mixed)" if mixed else "f64",
         "data": "synthetic (seeded dots and pulse of the stated distributions)",
         "config": config_dict(args),
-        "roofline": roof if otf else {"bound": "hbm", "kernel": "far_kernel<5,false>", "achieved": achieved, "peak": hbm,
+        "roofline": roof if otf else {"bound": "hbm", "kernel": "far_kernel_mixed<5,false>" if mixed else
+                                      "far_kernel_async<5,false,0>", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "steps_per_launch": K,
                      "avg_launch_ms": avg_ms, "share_of_timed_region": pair_ms / ms if ms > 0 else None,
                      "step_kernels_ms_per_step": step_ms / max(launches * K, 1),
                      "step_form": {0: "general (12 launches per step)", 1: "fused (1 launch per step)",
                                    2: "block (1 cooperative launch per 16 steps)"}[info["fused_step"]],
-                     "far_variant": args.far_variant,
+                     "far_variant": 3 if args.far_variant is None else args.far_variant,
                      ("fp32" if mixed else "fp64"): {
                          "achieved": fp64_tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": fp64_tf / fp64_peak,
                          "flops_per_launch": flops,
@@ -473,7 +475,7 @@ def main():
     ap.add_argument("--cpu-t0", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dipole-scale", type=float, default=1.0)
-    ap.add_argument("--far-variant", type=int, default=0)
+    ap.add_argument("--far-variant", type=int, default=None)
     ap.add_argument("--workload", choices=["table", "otf", "batched", "serving"], default="table")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--ensembles", type=int, default=256)

@@ -67,6 +67,7 @@ struct qg_handle_s {
   bool mixed = false;
   bool otf = false;  // coefficients computed in the far kernel (no table)
   int group = kTileGroup;  // source tiles per far-kernel warp
+  int max_groups = 0;      // source groups the partial buffer holds
   double2 *d_ring = nullptr;
   int W = 0, stride = 0;
   double2 *d_pcr = nullptr, *d_partial = nullptr, *d_field = nullptr, *d_scratch = nullptr;
@@ -118,7 +119,7 @@ struct qg_handle_s {
   bool pev_ready = false, pending[kProfRing] = {};
   int prof_next = 0;
   bool use_graph = true;
-  int far_variant = 0;
+  int far_variant = 3;  // cp.async-staged table (see qg_far.cu)
   bool profile = false;
   cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
   bool events_ready = false;
@@ -740,7 +741,10 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_TRY(order_for_near_groups(h, dots, morton_order(dots, n), order));
   h->n_pad = (int)order.size();
   h->nT = h->n_pad / kTile;
-  h->nG = (h->nT + kTileGroup - 1) / kTileGroup;
+  // source tiles per far-kernel warp: 2 for the mixed path (twice as many
+  // warps balance its shorter per-source work better), 4 in FP64
+  h->group = p->precision == QG_PREC_MIXED ? 2 : kTileGroup;
+  h->nG = (h->nT + h->group - 1) / h->group;
   h->nblk = (long long)h->nT * (h->nT + 1) / 2;
   std::vector<double> pos((size_t)h->n_pad * 3, 0.0), dip((size_t)h->n_pad * 3, 0.0);
   std::vector<double> fr(h->n_pad, 0.0), t1(h->n_pad, 1.0), t2(h->n_pad, 1.0);
@@ -854,7 +858,9 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
     QG_TRY(dalloc(h, &h->d_ring32d, (size_t)h->n_pad * h->stride));
   }
   QG_TRY(dalloc(h, &h->d_pcr, (size_t)kPcDepth * 4 * h->n_pad));
-  QG_TRY(dalloc(h, &h->d_partial, (size_t)kTimeBlock * h->nG * h->n_pad));
+  // partials for the smallest group size the "far_group" option allows
+  h->max_groups = h->otf ? h->nG : (h->nT <= 512 ? h->nT : h->nG);
+  QG_TRY(dalloc(h, &h->d_partial, (size_t)kTimeBlock * h->max_groups * h->n_pad));
   QG_TRY(dalloc(h, &h->d_field, (size_t)kTimeBlock * h->n_pad));
   QG_TRY(dalloc(h, &h->d_tile_done, (size_t)h->nT));
   QG_TRY(dalloc(h, &h->d_scratch, (size_t)h->n_pad * 8));
@@ -1427,6 +1433,8 @@ extern "C" qg_status qg_history_evaluate_noalloc(qg_handle *h, int step, const d
   QG_CUDA(cudaMemsetAsync(sc.tile_done, 0, sc.tile_bytes, s));
   launch_set_int(sc.ints + 0, step, s);
   FarArgs fa = h->far_args(sc.ints + 0, sc.ints + 1);
+  fa.group = kTileGroup;  // the fixed scratch holds the partials of this group size
+  fa.nG = (h->nT + kTileGroup - 1) / kTileGroup;
   fa.partial = sc.partial;
   fa.field = sc.field;
   fa.tile_done = sc.tile_done;
@@ -1504,8 +1512,8 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
   if(!p || !bytes || n < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_footprint: bad argument");
   const int nT = (n + kTile - 1) / kTile, n_pad = nT * kTile;
   const bool otf = p->coef_mode == QG_COEF_ON_THE_FLY;
-  const int group = otf ? (nT + 15) / 16 : kTileGroup;
-  const int nG = (nT + group - 1) / group;
+  const int group = otf ? (nT + 15) / 16 : (p->precision == QG_PREC_MIXED ? 2 : kTileGroup);
+  const int nG = otf ? (nT + group - 1) / group : (nT <= 512 ? nT : (nT + group - 1) / group);
   const int q = p->interpolation_order;
   const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
   const int W = ring_depth(md, q);
@@ -1547,9 +1555,16 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
   } else if(!std::strcmp(key, "profile")) {
     if(value) QG_TRY(ensure_events(h));
     h->profile = value != 0;
-  } else if(!std::strcmp(key, "far_variant") || !std::strcmp(key, "block_step")) {
-    if(!std::strcmp(key, "far_variant")) {
-      if(value < 0 || value > 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..2");
+  } else if(!std::strcmp(key, "far_variant") || !std::strcmp(key, "block_step") ||
+            !std::strcmp(key, "far_group")) {
+    if(!std::strcmp(key, "far_group")) {
+      if(h->otf || value < 1 || (h->nT + value - 1) / value > h->max_groups)
+        return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_group %d not available (table handles, "
+                       "at least %d)", value, (h->nT + h->max_groups - 1) / std::max(h->max_groups, 1));
+      h->group = value;
+      h->nG = (h->nT + value - 1) / value;
+    } else if(!std::strcmp(key, "far_variant")) {
+      if(value < 0 || value > 4) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..4");
       h->far_variant = value;
     } else {
       if(value && !h->block_step_ok)

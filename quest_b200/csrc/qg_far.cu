@@ -21,7 +21,7 @@
 // only the K accumulators and the q+1 coefficients stay in registers.
 //
 // Schedule.  One warp owns a target tile I (lane l = dot 32 I + l) and a
-// group of kTileGroup source tiles.  At each step all 32 lanes take the same
+// group of a.group source tiles.  At each step all 32 lanes take the same
 // source b, so their windows, at the 32 different delays d(a_l, b), fall in
 // one short stretch of b's history row: a handful of cache lines per load
 // instead of 32.  The sums over the group are written as partials; the last
@@ -84,8 +84,8 @@ __device__ __forceinline__ void far_body(const FarArgs &a, int task)
   static_assert(VEC == 0 || VEC == 1, "VEC");
   if(task >= a.nT * a.nG) return;  // uniform per warp
   const int I = task / a.nG, g = task % a.nG;
-  const int J0 = g * kTileGroup;
-  const int nJ = min(kTileGroup, a.nT - J0);
+  const int J0 = g * a.group;
+  const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
   if(task == 0 && lane == 0) *a.far_t0_out = t0;
   const int W = a.W;
@@ -135,10 +135,113 @@ __device__ __forceinline__ void far_body(const FarArgs &a, int task)
   group_partials_reduce<K>(a, I, g, acc);
 }
 
+__device__ __forceinline__ int warp_task() { return blockIdx.x * 4 + (threadIdx.x >> 5); }
+
+// Table entries staged in shared memory by asynchronous copies (cp.async),
+// P sources ahead of the convolution: each lane copies its own delay and
+// q+1 coefficients of source it + P - 1 while it convolves source it, so the
+// HBM latency of the table stream is covered without holding prefetched
+// values in registers.  The copies carry an L2 evict-first policy (the table
+// is streamed once per launch; the history ring should stay in L2).
+template <int Q, int P>
+struct FarStage {
+  double2 coef[P][Q + 1][32];
+  int delay[P][32];
+};
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, unsigned long long pol)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "l"(pol));
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, unsigned long long pol)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "l"(pol));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+template <int Q, bool LAB, int P, int VEC, int K = kTimeBlock>
+__device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarStage<Q, P> &st)
+{
+  const int lane = threadIdx.x & 31;
+  if(task >= a.nT * a.nG) return;  // uniform per warp
+  const int I = task / a.nG, g = task % a.nG;
+  const int J0 = g * a.group;
+  const int nJ = min(a.group, a.nT - J0);
+  const int t0 = *a.d_t0;
+  if(task == 0 && lane == 0) *a.far_t0_out = t0;
+  const int W = a.W;
+  unsigned long long pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+
+  double2 acc[K];
+#pragma unroll
+  for(int k = 0; k < K; ++k) acc[k] = make_double2(0.0, 0.0);
+
+  const long long tile0 = (long long)I * a.nT + J0;
+  const int iters = nJ * kTile;
+  auto issue = [&](int it) {
+    const int slot = it % P;
+    const long long tile = tile0 + it / kTile;
+    const int e = (it % kTile) * kTile + lane;
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) cp_async16(&st.coef[slot][i][lane], a.coef + (tile * (Q + 1) + i) * kTilePairs + e, pol);
+    cp_async4(&st.delay[slot][lane], a.delay + tile * kTilePairs + e, pol);
+  };
+#pragma unroll
+  for(int p = 0; p < P - 1; ++p) {
+    if(p < iters) issue(p);
+    cp_async_commit();
+  }
+  for(int it = 0; it < iters; ++it) {
+    if(it + P - 1 < iters) issue(it + P - 1);
+    cp_async_commit();
+    cp_async_wait<P - 1>();  // the group holding source `it` has landed
+    const int slot = it % P;
+    const int d = st.delay[slot][lane];
+    if(d >= kTimeBlock) {
+      double2 c[Q + 1];
+#pragma unroll
+      for(int i = 0; i <= Q; ++i) c[i] = st.coef[slot][i][lane];
+      const int ib = (J0 + it / kTile) * kTile + (it % kTile);
+      const int tau0 = t0 - d - Q;
+      int slot0 = tau0 % W;
+      if(slot0 < 0) slot0 += W;
+      const double2 *row = a.ring + (long long)ib * a.stride;
+      if(VEC) {
+        if(slot0 & 1)
+          window_conv2<Q, LAB, 1, K>(row, slot0 - 1, tau0, c, acc);
+        else
+          window_conv2<Q, LAB, 0, K>(row, slot0, tau0, c, acc);
+      } else {
+        window_conv<Q, LAB, K>(row, slot0, tau0, c, acc);
+      }
+    }
+  }
+  cp_async_wait<0>();
+  group_partials_reduce<K>(a, I, g, acc);
+}
+
+constexpr int kFarStages = 3;
+static_assert(4 * sizeof(FarStage<kMaxOrder, kFarStages>) <= 227 * 1024, "far stage buffers");
+
+template <int Q, bool LAB, int VEC>
+__global__ void __launch_bounds__(128) far_kernel_async(FarArgs a)
+{
+  extern __shared__ double2 far_smem[];
+  FarStage<Q, kFarStages> *st = reinterpret_cast<FarStage<Q, kFarStages> *>(far_smem);
+  far_body_async<Q, LAB, kFarStages, VEC>(a, warp_task(), st[threadIdx.x >> 5]);
+}
+
 // Variants of the same kernel (identical arithmetic and results):
-//   far_kernel      3 blocks of 4 warps per SM, one sample per load
-//   far_kernel_r4   registers capped for 4 blocks per SM
-//   far_kernel_v2   capped, two samples per 32-byte load
+//   far_kernel        3 blocks of 4 warps per SM, one sample per load
+//   far_kernel_r4     registers capped for 4 blocks per SM
+//   far_kernel_v2     capped, two samples per 32-byte load
+//   far_kernel_async  table staged in shared memory by cp.async, 3 sources
+//                     ahead; one sample (variant 3) or two (variant 4) per load
 // ---- mixed precision ---------------------------------------------------------
 // The tap sum of one pair, sum_i c_i w_i, is formed as
 //     (sum_i c_i) w_0 + sum_i c_i (w_i - w_0),
@@ -153,8 +256,8 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
   const int lane = threadIdx.x & 31;
   if(task >= a.nT * a.nG) return;  // uniform per warp
   const int I = task / a.nG, g = task % a.nG;
-  const int J0 = g * kTileGroup;
-  const int nJ = min(kTileGroup, a.nT - J0);
+  const int J0 = g * a.group;
+  const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
   if(task == 0 && lane == 0) *a.far_t0_out = t0;
   const int W = a.W;
@@ -198,7 +301,6 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
   group_partials_reduce<K>(a, I, g, acc64);
 }
 
-__device__ __forceinline__ int warp_task() { return blockIdx.x * 4 + (threadIdx.x >> 5); }
 
 template <int Q, bool LAB>
 __global__ void __launch_bounds__(128) far_kernel(FarArgs a) { far_body<Q, LAB, 0>(a, warp_task()); }
@@ -276,6 +378,22 @@ static void launch_far_q(const FarArgs &a, cudaStream_t s)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
+  else if(a.variant == 3 || a.variant == 4) {
+    // 38 KB at q = 5, 51 KB at q = 7 (above the 48 KB default: opt in)
+    const size_t smem = 4 * sizeof(FarStage<Q, kFarStages>);
+    static bool attr_set[64] = {};  // the attribute is per function and device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if(dev >= 64 || !attr_set[dev]) {
+      cudaFuncSetAttribute(far_kernel_async<Q, LAB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(far_kernel_async<Q, LAB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if(dev < 64) attr_set[dev] = true;
+    }
+    if(a.variant == 3)
+      far_kernel_async<Q, LAB, 0><<<blocks, 128, smem, s>>>(a);
+    else
+      far_kernel_async<Q, LAB, 1><<<blocks, 128, smem, s>>>(a);
+  }
   else
     far_kernel<Q, LAB><<<blocks, 128, 0, s>>>(a);
 }
