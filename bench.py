@@ -327,7 +327,8 @@ def run_ours(args, world, rank, local):
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     fp64_tf = flops / (avg_ms / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops("float32" if mixed else "float64")
-    traffic = profile_traffic("far_kernel_fp64_N4096")  # ncu dram read+write per launch
+    # ncu dram read + write per launch of the same kernel on the same workload
+    traffic = profile_traffic("far_kernel_mixed_N4096" if mixed else "far_kernel_async_fp64_N4096")
     if otf:
         # compute-bound: every ordered pair's coefficients (FP64) once per
         # launch plus the K-step convolution (FP64, or FP32 in mixed)
