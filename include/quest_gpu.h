@@ -191,6 +191,17 @@ qg_status qg_get_state(qg_handle *h, double *rho_out);
 /* First step at which a non-finite value appeared, or -1. */
 qg_status qg_bad_step(qg_handle *h, int *bad_step);
 
+/* Checkpoint / resume (no reference counterpart; the reference keeps the
+ * whole history in host memory).  A checkpoint holds the device state after
+ * step next_step - 1: the rho01 history ring (plus the FP32 rings in mixed
+ * precision), the 23-step predictor-corrector window, the next step and the
+ * first non-finite step.  Load it into a handle created from the same dots,
+ * pulse and parameters; the resumed run is bit-identical to an uninterrupted
+ * one.  qg_checkpoint_size gives the buffer size (host memory). */
+qg_status qg_checkpoint_size(const qg_handle *h, size_t *bytes);
+qg_status qg_checkpoint_save(qg_handle *h, void *buf, size_t bytes);
+qg_status qg_checkpoint_load(qg_handle *h, const void *buf, size_t bytes);
+
 /* Batches: many independent ensembles (handles) advanced together, one
  * persistent far-pair launch and one step launch per step for all of them,
  * driven by an (ensemble, target tile, source-tile group) work list, the

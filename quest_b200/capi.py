@@ -74,7 +74,7 @@ EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_dest
            "qg_get_history", "qg_get_info", "qg_footprint", "qg_stream", "qg_kernel_time",
            "qg_set_option", "qg_history_evaluate_noalloc", "qg_get_state", "qg_bad_step",
            "qg_batch_create", "qg_batch_destroy", "qg_batch_add", "qg_batch_remove", "qg_batch_run",
-           "qg_batch_size"]
+           "qg_batch_size", "qg_checkpoint_size", "qg_checkpoint_save", "qg_checkpoint_load"]
 
 _lib = None
 
@@ -110,6 +110,9 @@ def lib():
         L.qg_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.qg_history_evaluate_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp]
         L.qg_get_state.argtypes = [vp, dp]
+        L.qg_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+        L.qg_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
+        L.qg_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
         L.qg_bad_step.argtypes = [vp, ip]
         L.qg_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
         L.qg_batch_destroy.argtypes = [vp]
@@ -261,6 +264,19 @@ class Simulation:
         out = np.empty((self.n, 2), dtype=np.complex128)
         _check(lib().qg_get_state(self.h, _dp(out.view(np.float64))))
         return out
+
+    def checkpoint(self) -> bytes:
+        """The device state after the last computed step (qg_checkpoint_save)."""
+        size = ctypes.c_size_t()
+        _check(lib().qg_checkpoint_size(self.h, ctypes.byref(size)))
+        buf = ctypes.create_string_buffer(size.value)
+        _check(lib().qg_checkpoint_save(self.h, buf, size.value))
+        return buf.raw
+
+    def restore(self, data: bytes) -> None:
+        """Continue from a checkpoint of a simulation with the same inputs."""
+        buf = ctypes.create_string_buffer(data, len(data))
+        _check(lib().qg_checkpoint_load(self.h, buf, len(data)))
 
     def bad_step(self) -> int:
         b = ctypes.c_int()

@@ -1354,6 +1354,115 @@ extern "C" qg_status qg_get_state(qg_handle *h, double *rho_out)
   return QG_OK;
 }
 
+// ---- checkpoint / resume ------------------------------------------------------
+// A checkpoint is the integrator's device state after step next_step - 1:
+// the rho01 ring (and, in mixed precision, the FP32 rings), the 23-step
+// predictor-corrector window, the next step and the first non-finite step.
+// The coefficient table and lists are not part of it: they follow from the
+// inputs, so a checkpoint is loaded into a handle created from the same
+// dots, pulse and parameters.  Resuming gives the same bits as not stopping
+// (a far block is recomputed from history that the steps after its start do
+// not touch).
+struct CheckpointHeader {
+  char magic[8];
+  int version, n, n_pad, q, W, stride, mixed, next_step, T, bad;
+  double dt, c0;
+  unsigned long long ring_bytes, ring32_bytes, pcr_bytes;
+};
+
+static void checkpoint_header(const qg_handle *h, CheckpointHeader &hd)
+{
+  std::memset(&hd, 0, sizeof hd);
+  std::memcpy(hd.magic, "QGCKPT\0", 8);
+  hd.version = 1;
+  hd.n = h->n;
+  hd.n_pad = h->n_pad;
+  hd.q = h->q;
+  hd.W = h->W;
+  hd.stride = h->stride;
+  hd.mixed = h->mixed ? 1 : 0;
+  hd.next_step = h->next_step;
+  hd.T = h->T;
+  hd.dt = h->params.dt;
+  hd.c0 = h->params.c0;
+  hd.ring_bytes = sizeof(double2) * (unsigned long long)h->n_pad * h->stride;
+  hd.ring32_bytes = h->mixed ? sizeof(float2) * (unsigned long long)h->n_pad * h->stride : 0;
+  hd.pcr_bytes = sizeof(double2) * (unsigned long long)kPcDepth * 4 * h->n_pad;
+}
+
+extern "C" qg_status qg_checkpoint_size(const qg_handle *h, size_t *bytes)
+{
+  if(!h || !bytes) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_size: NULL argument");
+  CheckpointHeader hd;
+  checkpoint_header(h, hd);
+  *bytes = sizeof hd + hd.ring_bytes + 2 * hd.ring32_bytes + hd.pcr_bytes;
+  return QG_OK;
+}
+
+extern "C" qg_status qg_checkpoint_save(qg_handle *h, void *buf, size_t bytes)
+{
+  if(!h || !buf) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_save: NULL argument");
+  size_t need = 0;
+  QG_TRY(qg_checkpoint_size(h, &need));
+  if(bytes < need) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_save: buffer of %zu bytes, need %zu", bytes, need);
+  QG_CUDA(cudaSetDevice(h->device));
+  CheckpointHeader hd;
+  checkpoint_header(h, hd);
+  QG_CUDA(cudaMemcpyAsync(&hd.bad, h->d_ints + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  char *p = static_cast<char *>(buf) + sizeof hd;
+  QG_CUDA(cudaMemcpyAsync(p, h->d_ring, hd.ring_bytes, cudaMemcpyDeviceToHost, h->stream));
+  p += hd.ring_bytes;
+  if(h->mixed) {
+    QG_CUDA(cudaMemcpyAsync(p, h->d_ring32w, hd.ring32_bytes, cudaMemcpyDeviceToHost, h->stream));
+    p += hd.ring32_bytes;
+    QG_CUDA(cudaMemcpyAsync(p, h->d_ring32d, hd.ring32_bytes, cudaMemcpyDeviceToHost, h->stream));
+    p += hd.ring32_bytes;
+  }
+  QG_CUDA(cudaMemcpyAsync(p, h->d_pcr, hd.pcr_bytes, cudaMemcpyDeviceToHost, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  std::memcpy(buf, &hd, sizeof hd);
+  return QG_OK;
+}
+
+extern "C" qg_status qg_checkpoint_load(qg_handle *h, const void *buf, size_t bytes)
+{
+  if(!h || !buf) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: NULL argument");
+  CheckpointHeader hd, mine;
+  if(bytes < sizeof hd) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: buffer too small");
+  std::memcpy(&hd, buf, sizeof hd);
+  checkpoint_header(h, mine);
+  if(std::memcmp(hd.magic, mine.magic, 8) != 0 || hd.version != 1)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: not a checkpoint of this library");
+  if(hd.n != mine.n || hd.n_pad != mine.n_pad || hd.q != mine.q || hd.W != mine.W || hd.stride != mine.stride ||
+     hd.mixed != mine.mixed || hd.T != mine.T || hd.dt != mine.dt || hd.c0 != mine.c0)
+    return qg_fail(QG_ERR_INVALID_ARG,
+                   "qg_checkpoint_load: checkpoint of another configuration (N %d, q %d, W %d, precision %d, T %d; "
+                   "this handle: N %d, q %d, W %d, precision %d, T %d)",
+                   hd.n, hd.q, hd.W, hd.mixed, hd.T, mine.n, mine.q, mine.W, mine.mixed, mine.T);
+  if(hd.next_step < 0 || hd.next_step > hd.T)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: step %d outside [0, %d]", hd.next_step, hd.T);
+  const size_t need = sizeof hd + hd.ring_bytes + 2 * hd.ring32_bytes + hd.pcr_bytes;
+  if(bytes < need) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: buffer of %zu bytes, need %zu", bytes, need);
+  QG_CUDA(cudaSetDevice(h->device));
+  for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
+  const char *p = static_cast<const char *>(buf) + sizeof hd;
+  QG_CUDA(cudaMemcpyAsync(h->d_ring, p, hd.ring_bytes, cudaMemcpyHostToDevice, h->stream));
+  p += hd.ring_bytes;
+  if(h->mixed) {
+    QG_CUDA(cudaMemcpyAsync(h->d_ring32w, p, hd.ring32_bytes, cudaMemcpyHostToDevice, h->stream));
+    p += hd.ring32_bytes;
+    QG_CUDA(cudaMemcpyAsync(h->d_ring32d, p, hd.ring32_bytes, cudaMemcpyHostToDevice, h->stream));
+    p += hd.ring32_bytes;
+  }
+  QG_CUDA(cudaMemcpyAsync(h->d_pcr, p, hd.pcr_bytes, cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(h->d_ints + 2, &hd.bad, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  h->next_step = hd.next_step;
+  h->far_block = -0x7fffffff;
+  h->eval_cached = -0x7fffffff;
+  return QG_OK;
+}
+
 extern "C" qg_status qg_next_step(const qg_handle *h, int *step)
 {
   if(!h || !step) return qg_fail(QG_ERR_INVALID_ARG, "qg_next_step: NULL argument");

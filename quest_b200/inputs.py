@@ -228,6 +228,19 @@ def write_input_cfg(path: str, c: Constants, num_particles: int, qd_path="dots.c
         f.write(f"  laser_frequency = {c.laser_frequency:.17g}\n")
 
 
+def read_output_dat(path: str) -> np.ndarray:
+    """output.dat as History::write_history writes it (src/history.cpp:17-34):
+    one line per step, each dot's rho00 and rho01 as "(re,im)".  Returns
+    (T, N, 2) complex."""
+    rows = []
+    for line in open(path):
+        toks = line.replace("(", " ").replace(")", " ").split()
+        vals = [complex(float(a), float(b)) for a, b in (t.split(",") for t in toks)]
+        rows.append(vals)
+    arr = np.array(rows, dtype=np.complex128)
+    return arr.reshape(arr.shape[0], -1, 2)
+
+
 def load_pc_weights(path: str) -> tuple[np.ndarray, np.ndarray, float]:
     """Read a weight table: n_time, ps rows 0-1, cs rows 0-1, future_coef."""
     rows = [ln for ln in open(path) if ln.strip() and not ln.startswith("#")]

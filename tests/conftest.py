@@ -20,7 +20,8 @@ def pytest_configure(config):
 def _ensure_built():
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
-    if not os.path.exists(os.path.join(ROOT, "quest_b200", "libquest_gpu.so")):
+    if not (os.path.exists(os.path.join(ROOT, "quest_b200", "libquest_gpu.so")) and
+            os.path.exists(os.path.join(ROOT, "quest_b200", "quest-gpu"))):
         subprocess.run(["make", "-s", "-j4", "-C", os.path.join(ROOT, "quest_b200", "csrc")], check=True)
 
 
