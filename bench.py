@@ -155,7 +155,9 @@ def fp64_peak_tflops(dtype="float64") -> float:
     return 2 * n ** 3 / (best / 1e3) / 1e12
 
 
-def dist_setup(args):
+def dist_setup(args, backend: str = "nccl"):
+    """One process per GPU (torchrun): RANK / WORLD_SIZE / LOCAL_RANK from
+    the environment; NCCL on GPUs, gloo for the CPU tests of this logic."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -164,9 +166,15 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
+
+
+def _collective_device():
+    import torch.distributed as dist
+    return "cpu" if dist.get_backend() == "gloo" else "cuda"
 
 
 def max_over_ranks(x: float, world: int) -> float:
@@ -174,9 +182,15 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_collective_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(world: int, n: int, steps: int, ms_max: float) -> float:
+    """Whole-job pair-updates/s: every rank advances its own N-dot ensemble
+    `steps` steps; the job takes as long as the slowest rank."""
+    return world * n * n * steps / (ms_max / 1e3)
 
 
 def barrier(world: int):
@@ -294,7 +308,7 @@ def run_ours(args, world, rank, local):
     pair_ms, launches, step_ms, step_launches = sim.kernel_times()
     sim.close()
     ms_max = max_over_ranks(ms, world)
-    value = world * n * n * args.steps / (ms_max / 1e3)
+    value = job_throughput(world, n, args.steps, ms_max)
 
     # ---- end to end through the C ABI with host buffers: create (dots
     # upload + table build), every step's rho (N x 2 complex) copied back
