@@ -439,7 +439,8 @@ def run_batched(args, world, rank, local):
     ns = np.array([r.n for r in reqs])
     line = {"metric": "pair-updates/s", "value": world * total / wall, "unit": "pair-updates/s",
             "n_gpus": world, "steps": int(blocks * 16), "warmup": 0, "ms_per_step": wall * 1e3 / (blocks * 16),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair sum + f64 state (mixed)" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded ensembles)",
             "config": {"workload": f"batched_{args.ensembles}_ensembles", "ensembles": args.ensembles,
                        "N_min": int(ns.min()), "N_max": int(ns.max()), "sum_N2T": total,
@@ -469,7 +470,8 @@ def run_serving(args, world, rank, local):
     srv.close()
     stats["pair_updates_per_s"] = max_over_ranks(stats["pair_updates_per_s"], world)
     line = {"metric": "pair-updates/s", "value": world * stats["pair_updates_per_s"], "unit": "pair-updates/s",
-            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair sum + f64 state (mixed)" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded Poisson request stream)",
             "config": {"workload": "serving", "requests": args.requests, "rate_per_s": args.rate,
                        "N_max": args.serve_nmax, "budget_gb": args.budget_gb, "precision": args.precision},
