@@ -256,7 +256,7 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "profile" (1 = CUDA events around the far-pair kernel and the step
  * kernels: event nodes inside the block graphs, or around each launch when
  * "graph" is 0),
- * "far_variant" (0..4: resource shape of the far-pair kernel, same results),
+ * "far_variant" (0..5: resource shape of the far-pair kernel, same results),
  * "far_group" (source tiles each far-kernel warp sums before writing its
  *   partial, table handles; default 4; changes the summation grouping, so
  *   results change in the last bits),

@@ -1198,7 +1198,7 @@ extern "C" qg_status qg_batch_create(int capacity, qg_batch **out)
                         cudaGetErrorString(e)));
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  per_sm = 3;  // far kernel: 168 registers x 128 threads -> 3 blocks per SM
+  per_sm = 3;  // persistent far grid: 3 blocks of 4 warps per SM (measured best)
   b->far_grid = std::max(1, sms * per_sm);
   *out = b;
   return QG_OK;
@@ -1673,7 +1673,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
       h->group = value;
       h->nG = (h->nT + value - 1) / value;
     } else if(!std::strcmp(key, "far_variant")) {
-      if(value < 0 || value > 4) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..4");
+      if(value < 0 || value > 5) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..5");
       h->far_variant = value;
     } else {
       if(value && !h->block_step_ok)

@@ -35,6 +35,7 @@
 // (green_function.h:23-27).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "qg_conv.cuh"
@@ -121,7 +122,7 @@ __device__ __forceinline__ void far_body(const FarArgs &a, int task)
       int slot0 = tau0 % W;
       if(slot0 < 0) slot0 += W;
       const double2 *row = a.ring + (long long)ib * a.stride;
-      if(VEC) {
+      if(VEC == 1) {
         if(slot0 & 1)
           window_conv2<Q, LAB, 1, K>(row, slot0 - 1, tau0, c, acc);
         else
@@ -199,7 +200,25 @@ __device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarSt
   for(int it = 0; it < iters; ++it) {
     if(it + P - 1 < iters) issue(it + P - 1);
     cp_async_commit();
-    cp_async_wait<P - 1>();  // the group holding source `it` has landed
+    if(VEC == 2) {
+      // sources it and it+1 have landed; pull it+1's history window into L1
+      // while `it` is convolved (its lanes' windows span a few lines)
+      cp_async_wait<P - 2>();
+      if(it + 1 < iters) {
+        const int d1 = st.delay[(it + 1) % P][lane];
+        if(d1 >= kTimeBlock) {
+          int s1 = (t0 - d1 - Q) % W;
+          if(s1 < 0) s1 += W;
+          const char *p1 = reinterpret_cast<const char *>(
+              a.ring + (long long)((J0 + (it + 1) / kTile) * kTile + ((it + 1) % kTile)) * a.stride + s1);
+#pragma unroll
+          for(int b = 0; b < 3; ++b) asm volatile("prefetch.global.L1 [%0];" ::"l"(p1 + 128 * b));
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(p1 + 16 * (K + Q) - 1));
+        }
+      }
+    } else {
+      cp_async_wait<P - 1>();  // the group holding source `it` has landed
+    }
     const int slot = it % P;
     const int d = st.delay[slot][lane];
     if(d >= kTimeBlock) {
@@ -211,7 +230,7 @@ __device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarSt
       int slot0 = tau0 % W;
       if(slot0 < 0) slot0 += W;
       const double2 *row = a.ring + (long long)ib * a.stride;
-      if(VEC) {
+      if(VEC == 1) {
         if(slot0 & 1)
           window_conv2<Q, LAB, 1, K>(row, slot0 - 1, tau0, c, acc);
         else
@@ -232,8 +251,9 @@ template <int Q, bool LAB, int VEC>
 __global__ void __launch_bounds__(128) far_kernel_async(FarArgs a)
 {
   extern __shared__ double2 far_smem[];
-  FarStage<Q, kFarStages> *st = reinterpret_cast<FarStage<Q, kFarStages> *>(far_smem);
-  far_body_async<Q, LAB, kFarStages, VEC>(a, warp_task(), st[threadIdx.x >> 5]);
+  constexpr int P = VEC == 2 ? kFarStages + 1 : kFarStages;
+  FarStage<Q, P> *st = reinterpret_cast<FarStage<Q, P> *>(far_smem);
+  far_body_async<Q, LAB, P, VEC>(a, warp_task(), st[threadIdx.x >> 5]);
 }
 
 // Variants of the same kernel (identical arithmetic and results):
@@ -241,7 +261,9 @@ __global__ void __launch_bounds__(128) far_kernel_async(FarArgs a)
 //   far_kernel_r4     registers capped for 4 blocks per SM
 //   far_kernel_v2     capped, two samples per 32-byte load
 //   far_kernel_async  table staged in shared memory by cp.async, 3 sources
-//                     ahead; one sample (variant 3) or two (variant 4) per load
+//                     ahead; one sample (variant 3) or two (variant 4) per
+//                     load; variant 5: 4 stages and the next source's history
+//                     window prefetched into L1
 // ---- mixed precision ---------------------------------------------------------
 // The tap sum of one pair, sum_i c_i w_i, is formed as
 //     (sum_i c_i) w_0 + sum_i c_i (w_i - w_0),
@@ -250,7 +272,7 @@ __global__ void __launch_bounds__(128) far_kernel_async(FarArgs a)
 // interpolation weights (w1 ~ 1/dt, w2 ~ 1/dt^2) multiply only differences,
 // and sum_i c_i carries no such factor, so FP32 storage loses no more than a
 // few units in the last place of the pair's contribution.
-template <int Q, bool LAB, int K = kTimeBlock>
+template <int Q, bool LAB, int K = kTimeBlock, bool PACKED = false>
 __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
 {
   const int lane = threadIdx.x & 31;
@@ -289,8 +311,8 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
       const int tau0 = t0 - d - Q;
       int slot0 = tau0 % W;
       if(slot0 < 0) slot0 += W;
-      window_conv_mixed<Q, LAB, K>(a.ring32w + (long long)ib * a.stride, a.ring32d + (long long)ib * a.stride,
-                                   slot0, tau0, c, acc);
+      window_conv_mixed<Q, LAB, K, PACKED>(a.ring32w + (long long)ib * a.stride,
+                                           a.ring32d + (long long)ib * a.stride, slot0, tau0, c, acc);
     }
   }
 
@@ -328,12 +350,32 @@ __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restric
       else
         hi = mid - 1;
     }
-    const FarArgs a = args[lo];
-    if(MIXED)
+    const FarArgs a = args[lo];  // a copy: the bodies read its fields in their inner loops
+    if(MIXED) {
       far_body_mixed<Q, LAB>(a, task - task_off[lo]);
-    else
-      far_body<Q, LAB, 0>(a, task - task_off[lo]);
+    } else {
+      extern __shared__ double2 far_smem[];
+      FarStage<Q, kFarStages> *st = reinterpret_cast<FarStage<Q, kFarStages> *>(far_smem);
+      far_body_async<Q, LAB, kFarStages, 0>(a, task - task_off[lo], st[threadIdx.x >> 5]);
+    }
   }
+}
+
+// FP64 members stage their table entries in shared memory (as far_kernel_async)
+template <int Q, bool LAB, bool MIXED>
+static void launch_far_batch_q(const FarArgs *args, const int *task_off, int n_ens, int grid, cudaStream_t s)
+{
+  const size_t smem = MIXED ? 0 : 4 * sizeof(FarStage<Q, kFarStages>);
+  if(smem > 48 * 1024) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if(dev >= 64 || !attr_set[dev]) {
+      cudaFuncSetAttribute(far_batch_kernel<Q, LAB, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if(dev < 64) attr_set[dev] = true;
+    }
+  }
+  far_batch_kernel<Q, LAB, MIXED><<<grid, 128, smem, s>>>(args, task_off, n_ens);
 }
 
 template <bool LAB, bool MIXED>
@@ -341,13 +383,13 @@ static void launch_far_batch_frame(const FarArgs *args, const int *task_off, int
                                    cudaStream_t s)
 {
   switch(q) {
-    case 1: far_batch_kernel<1, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 2: far_batch_kernel<2, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 3: far_batch_kernel<3, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 4: far_batch_kernel<4, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 5: far_batch_kernel<5, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 6: far_batch_kernel<6, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
-    case 7: far_batch_kernel<7, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens); break;
+    case 1: launch_far_batch_q<1, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 2: launch_far_batch_q<2, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 3: launch_far_batch_q<3, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 4: launch_far_batch_q<4, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 5: launch_far_batch_q<5, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 6: launch_far_batch_q<6, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 7: launch_far_batch_q<7, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
     default: break;
   }
 }
@@ -366,7 +408,10 @@ void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q
 }
 
 template <int Q, bool LAB>
-__global__ void __launch_bounds__(128) far_kernel_mixed(FarArgs a) { far_body_mixed<Q, LAB>(a, warp_task()); }
+__global__ void __launch_bounds__(128) far_kernel_mixed(FarArgs a)
+{
+  far_body_mixed<Q, LAB, kTimeBlock, true>(a, warp_task());
+}
 
 template <int Q, bool LAB>
 static void launch_far_q(const FarArgs &a, cudaStream_t s)
@@ -378,21 +423,25 @@ static void launch_far_q(const FarArgs &a, cudaStream_t s)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
-  else if(a.variant == 3 || a.variant == 4) {
-    // 38 KB at q = 5, 51 KB at q = 7 (above the 48 KB default: opt in)
-    const size_t smem = 4 * sizeof(FarStage<Q, kFarStages>);
+  else if(a.variant >= 3 && a.variant <= 5) {
+    // 38 KB at q = 5, 51 KB at q = 7 (above the 48 KB default: opt in);
+    // variant 5 keeps one more stage
+    const size_t smem = 4 * sizeof(FarStage<Q, kFarStages>), smem5 = 4 * sizeof(FarStage<Q, kFarStages + 1>);
     static bool attr_set[64] = {};  // the attribute is per function and device
     int dev = 0;
     cudaGetDevice(&dev);
     if(dev >= 64 || !attr_set[dev]) {
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(far_kernel_async<Q, LAB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem5);
       if(dev < 64) attr_set[dev] = true;
     }
     if(a.variant == 3)
       far_kernel_async<Q, LAB, 0><<<blocks, 128, smem, s>>>(a);
-    else
+    else if(a.variant == 4)
       far_kernel_async<Q, LAB, 1><<<blocks, 128, smem, s>>>(a);
+    else
+      far_kernel_async<Q, LAB, 2><<<blocks, 128, smem5, s>>>(a);
   }
   else
     far_kernel<Q, LAB><<<blocks, 128, 0, s>>>(a);
