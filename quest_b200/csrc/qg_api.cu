@@ -119,7 +119,8 @@ struct qg_handle_s {
   bool pev_ready = false, pending[kProfRing] = {};
   int prof_next = 0;
   bool use_graph = true;
-  int far_variant = 3;  // cp.async-staged table (see qg_far.cu)
+  int far_variant = 3;  // cp.async-staged table (see qg_far.cu); the autotuner may change it
+  float tuned_far_ms = 0;  // far-kernel time of the autotuner's choice
   bool profile = false;
   cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
   bool events_ready = false;
@@ -875,6 +876,51 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 
   QG_TRY(build_lists(h, ta));
   QG_TRY(reset_state(h));
+  QG_TRY(autotune_far(h));
+  QG_TRY(reset_state(h));
+  return QG_OK;
+}
+
+// The far-kernel autotuner.  The FP64 table path has several kernels with
+// identical arithmetic (and so identical results) but different resource
+// shapes; which one is fastest depends on N and on the device.  One launch of
+// each, at a block start past the largest delay (every tap live, as in the
+// steady state), after one untimed launch; the fastest is kept.  The history
+// is whatever the handle holds (its values do not change the work), and the
+// far field and partials are recomputed by the next run.
+static qg_status autotune_far(qg_handle *h)
+{
+  if(h->otf || h->mixed || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
+  static const int candidates[] = {3, 0, 5};
+  const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
+  cudaEvent_t e0, e1;
+  QG_CUDA(cudaEventCreate(&e0));
+  QG_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_v = h->far_variant;
+  for(int v : candidates) {
+    h->far_variant = v;
+    launch_set_int(h->d_ints + 7, t_test, h->stream);
+    const FarArgs fa = h->far_args(h->d_ints + 7, h->d_ints + 6);
+    launch_far(fa, h->stream);  // untimed: first use of the kernel
+    QG_CUDA(cudaEventRecord(e0, h->stream));
+    launch_far(fa, h->stream);
+    QG_CUDA(cudaEventRecord(e1, h->stream));
+    QG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if(ms < best) {
+      best = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  QG_CUDA(cudaGetLastError());
+  h->far_variant = best_v;
+  h->tuned_far_ms = best;
+  h->far_block = -0x7fffffff;
+  h->eval_cached = -0x7fffffff;
   return QG_OK;
 }
 
@@ -1695,6 +1741,27 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
         }
   } else if(!std::strcmp(key, "reset")) {
     return reset_state(h);
+  } else if(!std::strcmp(key, "autotune")) {
+    // clobbers the far field and partials: only between runs on a block
+    // boundary (the next run recomputes them)
+    if(h->next_step % kTimeBlock != 0)
+      return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: autotune only at a block boundary (next step %d)",
+                     h->next_step);
+    if(value) {
+      for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
+      QG_TRY(autotune_far(h));
+      for(auto &g : h->graph)
+        if(g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+      for(auto &row : h->gprof)
+        for(auto &g : row)
+          if(g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+          }
+    }
   } else {
     return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: unknown key '%s'", key);
   }

@@ -294,6 +294,21 @@ def test_far_kernel_variants_agree_bitwise(golden_weights):
         np.testing.assert_array_equal(outs[0], outs[v])
 
 
+def test_autotuned_variant_changes_nothing(golden_weights):
+    """The autotuner (at creation, and on request) chooses among far-kernel
+    variants with identical arithmetic, so the trajectory does not depend on
+    its choice."""
+    wl = stable_small(600, 160, 0.06)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        a = sim.run(64)
+        sim.set_option("autotune", 1)
+        a = np.concatenate([a, sim.run(96)])
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        sim.set_option("far_variant", 0)
+        b = sim.run(160)
+    np.testing.assert_array_equal(a, b)
+
+
 def test_coincident_dots_raise_at_step_zero(golden_weights):
     dots = I.make_dots(5, 0.1, 3)
     dots[3, :3] = dots[1, :3]
