@@ -706,6 +706,8 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
   return QG_OK;
 }
 
+static qg_status autotune_far(qg_handle *h);
+
 static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, const qg_params *p,
                              const qg_weights *weights, qg_handle *h)
 {
