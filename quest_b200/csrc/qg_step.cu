@@ -360,21 +360,41 @@ __device__ __forceinline__ void mid_old_fetch(const StepArgs &a, int b, int d, i
   }
 }
 
+// The taps' products are independent and summed as a fixed pairwise tree
+// over the eight tap slots (absent taps contribute exact zeros), so the
+// dependent chain is three adds deep instead of q+1.
 __device__ __forceinline__ double2 mid_old_sum(const StepArgs &a, int d, int t, const double2 *c, int cstride,
                                                const double2 (&v)[kMaxOrder + 1])
 {
   const int q = a.q;
   const int s = t - d;
-  double2 M = make_double2(0.0, 0.0);
+  double2 p[kMaxOrder + 1];
 #pragma unroll
-  for(int i = 0; i <= kMaxOrder; ++i) {
-    if(i <= q && s - i >= -kWindow && d + i >= 2) {
-      const double2 w = cmul(prefactor(v[i], a.frame), c[i * cstride]);
-      M.x += w.x;
-      M.y += w.y;
+  for(int i = 0; i <= kMaxOrder; ++i)
+    p[i] = (i <= q && s - i >= -kWindow && d + i >= 2) ? cmul(prefactor(v[i], a.frame), c[i * cstride])
+                                                        : make_double2(0.0, 0.0);
+  static_assert(kMaxOrder + 1 == 8, "tree over 8 tap slots");
+  const double2 s01 = make_double2(p[0].x + p[1].x, p[0].y + p[1].y);
+  const double2 s23 = make_double2(p[2].x + p[3].x, p[2].y + p[3].y);
+  const double2 s45 = make_double2(p[4].x + p[5].x, p[4].y + p[5].y);
+  const double2 s67 = make_double2(p[6].x + p[7].x, p[6].y + p[7].y);
+  return make_double2((s01.x + s23.x) + (s45.x + s67.x), (s01.y + s23.y) + (s45.y + s67.y));
+}
+
+// A dot's staged mid-list entries [lo, hi) of one chunk: even and odd
+// positions in two running sums, then their sum (half the dependent chain).
+__device__ __forceinline__ double2 entry_sum(const double2 *v, int lo, int hi)
+{
+  double2 e = make_double2(0.0, 0.0), o = e;
+  for(int j = lo; j < hi; j += 2) {
+    e.x += v[j].x;
+    e.y += v[j].y;
+    if(j + 1 < hi) {
+      o.x += v[j + 1].x;
+      o.y += v[j + 1].y;
     }
   }
-  return M;
+  return make_double2(e.x + o.x, e.y + o.y);
 }
 
 __device__ __forceinline__ double2 mid_old(const StepArgs &a, int e, int t, int tslot)
@@ -513,11 +533,11 @@ __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int 
     const int c1 = min(E1, c0 + kMidChunk);
     for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_old(a, e, t, tslot);
     __syncthreads();
-    if(part == 0)
-      for(int e = max(my0, c0); e < min(my1, c1); ++e) {
-        Mo.x += midv[e - c0].x;
-        Mo.y += midv[e - c0].y;
-      }
+    if(part == 0) {
+      const double2 cs = entry_sum(midv, max(my0, c0) - c0, min(my1, c1) - c0);
+      Mo.x += cs.x;
+      Mo.y += cs.y;
+    }
     __syncthreads();
   }
   if(E0 == E1) __syncthreads();  // the window partials are complete
@@ -612,16 +632,30 @@ constexpr int kHistSpan = (kTimeBlock - 1) + kMaxOrder;  // t - kHistSpan is the
 
 __device__ __forceinline__ int hist_slot(int s) { return ((s % kHistDepth) + kHistDepth) % kHistDepth; }
 
+// Step flags: a block posts a finished step with a release add (its rho01
+// stores become visible before the count), and readers poll with acquire
+// loads (the posting block's stores are visible once the count is seen).
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void post_step(unsigned *p)
+{
+  asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
+
 // Called by a whole warp: waits until flags[list[i]] >= target for every
-// i < n (the lanes poll in parallel, each wait bounded), then fences so the
-// posting blocks' stores are visible (acquire).  False if a wait ran out.
+// i < n (the lanes poll in parallel, each wait bounded).  False if a wait
+// ran out.
 __device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *list, int n, unsigned target)
 {
   bool ok = true;
   for(int i = threadIdx.x & 31; i < n && ok; i += 32) {
-    const volatile unsigned *f = flags + __ldg(list + i);
+    const unsigned *f = flags + __ldg(list + i);
     int spins = 0;
-    while(*f < target) {
+    while(ld_acquire(f) < target) {
       if(++spins > kBarrierSpins) {
         ok = false;
         break;
@@ -629,9 +663,7 @@ __device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *li
       __nanosleep(32);
     }
   }
-  ok = __all_sync(0xffffffffu, ok);
-  __threadfence();
-  return ok;
+  return __all_sync(0xffffffffu, ok);
 }
 
 __device__ __forceinline__ void helpers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kHelpers)); }
@@ -675,13 +707,22 @@ struct BlockSmem {
   double *pul;            // [K][32] pulse of the launch's steps
   double *ps, *cs;        // [kWeightSlots] each
   int *mc_idx, *mc_del;   // [mid_cache] partners (with hist: partner slots) and delays
+  int *bp;                // [hist_cap] the distinct partners' internal indices
+};
+
+// Per-thread constants of the helpers' step work, read once per launch.
+struct BlockConst {
+  bool live;
+  int E0, E, my0, my1;  // the block's mid-list range; this lane's dot's sub-range (local)
+  int NP;               // distinct partners (partner history)
 };
 
 __host__ __device__ __forceinline__ size_t block_smem_bytes(int q, int mid_cache, int hist_cap)
 {
   return sizeof(double2) * ((size_t)kPcDepth * 4 * 32 + 2 * 3 * 4 * 32 + 2 * 32 + kTimeBlock * 32 + kMidChunk + 32 +
                             32 + (size_t)mid_cache * (q + 1) + (size_t)hist_cap * kHistStride) +
-         sizeof(double) * (kTimeBlock * 32 + 2 * kWeightSlots) + sizeof(int) * 2 * (size_t)mid_cache;
+         sizeof(double) * (kTimeBlock * 32 + 2 * kWeightSlots) + sizeof(int) * 2 * (size_t)mid_cache +
+         sizeof(int) * (size_t)hist_cap;
 }
 
 __device__ __forceinline__ BlockSmem block_smem(double2 *base, int q, int mid_cache, int hist_cap)
@@ -701,30 +742,28 @@ __device__ __forceinline__ BlockSmem block_smem(double2 *base, int q, int mid_ca
   m.cs = m.ps + kWeightSlots;
   m.mc_idx = reinterpret_cast<int *>(m.cs + kWeightSlots);
   m.mc_del = m.mc_idx + mid_cache;
+  m.bp = m.mc_del + mid_cache;
   return m;
 }
 
 // Step k's sums by the helper warps (hw = 0..5) into buffer `b`:
 // pre_s[b][p-1][v][lane] = S_p of quantity v, pre_f[b] = F + M_old.
 template <int NT>
-__device__ __forceinline__ void block_precompute(const StepArgs &a, const BlockSmem &m, int blk, int k, int t,
-                                                 int b, bool cached, bool hist, int hw)
+__device__ __forceinline__ void block_precompute(const StepArgs &a, const BlockSmem &m, const BlockConst &bc,
+                                                 int k, int t, int b, bool cached, bool hist, int hw)
 {
   constexpr int BS = 32;
   const int lane = threadIdx.x & 31;
   const int tid = hw * 32 + lane;
-  const int idx = blk * BS + lane;
-  const bool live = a.user[idx] >= 0;
-  const int E0 = a.mid_ptr[blk * BS], E = a.mid_ptr[blk * BS + BS] - E0;
-  const int my0 = a.mid_ptr[idx] - E0, my1 = a.mid_ptr[idx + 1] - E0;
+  const bool live = bc.live;
+  const int E0 = bc.E0, E = bc.E, my0 = bc.my0, my1 = bc.my1;
   const int q1 = a.q + 1, cap = a.mid_cache;
   if(hist) {
-    // the newest sample the old taps read (step t-2, finished by every
-    // block), one load per distinct partner of the block
-    const int P0 = a.bp_ptr[blk], NP = a.bp_ptr[blk + 1] - P0;
+    // the newest sample the old taps read (step t-2, finished by the
+    // partners' blocks), one L2 load per distinct partner of the block
     const int sa = t - 2, hs = hist_slot(sa), rs = ring_slot(sa, a.W);
-    for(int j = tid; j < NP; j += kHelpers)
-      m.hist[j * kHistStride + hs] = __ldcg(a.ring + (long long)a.bp_idx[P0 + j] * a.stride + rs);
+    for(int j = tid; j < bc.NP; j += kHelpers)
+      m.hist[j * kHistStride + hs] = __ldcg(a.ring + (long long)m.bp[j] * a.stride + rs);
     helpers_sync();
   }
   // mid-list entries of the block (local index e = entry - E0) staged by
@@ -752,11 +791,11 @@ __device__ __forceinline__ void block_precompute(const StepArgs &a, const BlockS
                               : mid_old_sum(a, d, t, a.mid_coef + (long long)(E0 + e) * q1, 1, v);
     }
     helpers_sync();
-    if(hw == 0)
-      for(int e = max(my0, c0); e < min(my1, c1); ++e) {
-        Mo.x += m.midv[e - c0].x;
-        Mo.y += m.midv[e - c0].y;
-      }
+    if(hw == 0) {
+      const double2 cs = entry_sum(m.midv, max(my0, c0) - c0, min(my1, c1) - c0);
+      Mo.x += cs.x;
+      Mo.y += cs.y;
+    }
     helpers_sync();
   }
   if(!live) return;
@@ -823,6 +862,8 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
       m.mc_del[i] = a.mid_delay[E0 + i];
     }
   }
+  if(hist)
+    for(int i = threadIdx.x; i < NP; i += blockDim.x) m.bp[i] = a.bp_idx[P0 + i];
   if(hist) {
     // samples t0+k0-22 .. t0+k0-2; later ones are appended step by step
     const int first = t0 + k0 - kHistSpan, count = kHistSpan - 1;
@@ -833,8 +874,15 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
   }
   if(part == 0) m.prev01[lane] = a.ring[(long long)idx * a.stride + ring_slot(t0 + k0 - 1, a.W)];
   if(threadIdx.x == 0) s_abort = 0;
+  BlockConst bc;
+  bc.live = live;
+  bc.E0 = E0;
+  bc.E = E;
+  bc.my0 = a.mid_ptr[idx] - E0;
+  bc.my1 = a.mid_ptr[idx + 1] - E0;
+  bc.NP = NP;
   __syncthreads();
-  if(helper && t0 + k0 < a.T) block_precompute<NT>(a, m, blk, k0, t0 + k0, k0 & 1, cached, hist, hw);
+  if(helper && t0 + k0 < a.T) block_precompute<NT>(a, m, bc, k0, t0 + k0, k0 & 1, cached, hist, hw);
   const DotConst dc = dot_const(a, idx, live);
   const bool block_near = a.near_ptr[(blk + 1) * BS] > a.near_ptr[blk * BS];
   const NearRegs nr = near_regs(a, idx);
@@ -877,10 +925,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
         // rho01 first, then post the step, then the rest of the state
         if(live) finish_ring(a, idx, t, r);
         __syncwarp();
-        if(lane == 0) {
-          __threadfence();
-          atomicAdd(flags + blk, 1u);
-        }
+        if(lane == 0) post_step(flags + blk);
         if(live) {
           finish_state(a, idx, t, r, dr);
           const int sl = pc_slot(t);
@@ -903,7 +948,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
         atomicMin(a.d_bad, -2);
       }
       helpers_sync();
-      if(!*(volatile int *)&s_abort) block_precompute<NT>(a, m, blk, k + 1, t + 1, buf ^ 1, cached, hist, hw);
+      if(!*(volatile int *)&s_abort) block_precompute<NT>(a, m, bc, k + 1, t + 1, buf ^ 1, cached, hist, hw);
     }
     __syncthreads();
   }
