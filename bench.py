@@ -265,6 +265,32 @@ def config_dict(args):
             else "1 GPU"}
 
 
+def accuracy_vs_fp64(args, weights) -> dict:
+    """Max relative error in rho of the mixed form against the FP64 form
+    (which matches the oracle to 1e-10, tests/test_gpu_parity.py) on an
+    excited, stable variant of the workload: dipoles x 0.1, pulse delay 0.3,
+    700 steps (N = 4096 table) or 400 steps at N = 16384 in the 0.5 cube
+    (on the fly).  max |d rho| / max |rho| per component."""
+    from quest_b200 import capi
+    otf = args.workload == "otf"
+    if otf:
+        wl = I.mixed_large(seed=3, n=16384, steps=400, pulse_delay=0.3)
+        steps, cmode = 400, capi.COEF_ON_THE_FLY
+    else:
+        wl = I.plain_table(seed=2, n=args.n, steps=700, pulse_delay=0.3)
+        steps, cmode = 700, capi.COEF_TABLE
+    wl.dots[:, 6:9] *= 0.1
+    out = {}
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec,
+                             coef_mode=cmode) as sim:
+            out[prec] = sim.run(steps)
+    a, b = out[capi.PREC_FP64], out[capi.PREC_MIXED]
+    err = [float(np.abs(a[..., k] - b[..., k]).max() / np.abs(a[..., k]).max()) for k in range(2)]
+    return {"rho00": err[0], "rho01": err[1],
+            "probe": f"N={wl.n}, {steps} steps, dipoles x0.1, pulse delay 0.3 ({'on the fly' if otf else 'table'})"}
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -399,6 +425,8 @@ def run_ours(args, world, rank, local):
         line["clocks"] = cs
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not otf:
         line["cpu_baseline"] = cpu_baseline(args)
+    if mixed and rank == 0:
+        line["max_rel_err_vs_fp64"] = accuracy_vs_fp64(args, weights)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -462,22 +490,24 @@ def run_serving(args, world, rank, local):
 
     from quest_b200 import capi, serving
     torch.cuda.set_device(local)
-    reqs = serving.serving_requests(args.requests, args.rate, seed=70 + rank, n_range=(32, args.serve_nmax))
-    srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=capi.pc_weights(),
-                         precision=capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64)
-    barrier(world)
-    stats = srv.serve(reqs)
-    srv.close()
-    stats["pair_updates_per_s"] = max_over_ranks(stats["pair_updates_per_s"], world)
-    line = {"metric": "pair-updates/s", "value": world * stats["pair_updates_per_s"], "unit": "pair-updates/s",
-            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 pair sum + f64 state (mixed)" if args.precision == "mixed" else "f64",
-            "data": "synthetic (seeded Poisson request stream)",
-            "config": {"workload": "serving", "requests": args.requests, "rate_per_s": args.rate,
-                       "N_max": args.serve_nmax, "budget_gb": args.budget_gb, "precision": args.precision},
-            "serving": stats}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    rates = [float(r) for r in args.rate_sweep.split(",")] if args.rate_sweep else [args.rate]
+    for rate in rates:
+        reqs = serving.serving_requests(args.requests, rate, seed=70 + rank, n_range=(32, args.serve_nmax))
+        srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=capi.pc_weights(),
+                             precision=capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64)
+        barrier(world)
+        stats = srv.serve(reqs)
+        srv.close()
+        stats["pair_updates_per_s"] = max_over_ranks(stats["pair_updates_per_s"], world)
+        line = {"metric": "pair-updates/s", "value": world * stats["pair_updates_per_s"], "unit": "pair-updates/s",
+                "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 pair sum + f64 state (mixed)" if args.precision == "mixed" else "f64",
+                "data": "synthetic (seeded Poisson request stream)",
+                "config": {"workload": "serving", "requests": args.requests, "rate_per_s": rate,
+                           "N_max": args.serve_nmax, "budget_gb": args.budget_gb, "precision": args.precision},
+                "serving": stats}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
 
 
 def main():
@@ -499,6 +529,7 @@ def main():
     ap.add_argument("--blocks-per-round", type=int, default=8)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--rate-sweep", default="", help="comma-separated arrival rates (one line each)")
     ap.add_argument("--serve-nmax", type=int, default=16384)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     args = ap.parse_args()

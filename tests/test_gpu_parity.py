@@ -294,6 +294,50 @@ def test_far_kernel_variants_agree_bitwise(golden_weights):
         np.testing.assert_array_equal(outs[0], outs[v])
 
 
+def line_of_dots(n, spacing, seed=5):
+    """n dots on a line along x, `spacing` apart (c dt = 1e-3): neighbours at
+    floor delay 1, none at delay 0, so the groups coupled at delay <= 1 are
+    the whole line and the step-block kernel waits on other blocks."""
+    wl = I.plain_small(n=n, steps=300, pulse_delay=0.02)
+    # jittered spacing: an exactly regular line puts some delays on integers,
+    # where the reference's Lagrange weights are NaN (tested separately)
+    jitter = 1.0 + 0.2 * (np.random.default_rng(seed).random(n) - 0.5)
+    wl.dots[:, 0] = np.cumsum(spacing * jitter) - 0.5 * n * spacing
+    wl.dots[:, 1] = 0.0
+    wl.dots[:, 2] = 0.0
+    wl.dots[:, 8] = 2e-4
+    return wl
+
+
+@pytest.mark.parametrize("case", ["delay1_chain", "dense_mid_list"])
+def test_step_block_paths_against_oracle(golden_weights, oracle_weights, case):
+    """Paths of the step-block kernel the random workloads rarely reach:
+    delay-1 partners in other blocks (warp 0 waits for their previous step),
+    and blocks whose mid list does not fit the shared-memory cache (entries
+    read from the lists in HBM, several staging chunks)."""
+    if case == "delay1_chain":
+        wl = line_of_dots(256, 1.5e-3)
+        steps = 300
+    else:
+        wl = I.plain_small(n=1024, steps=200, pulse_delay=0.02)
+        wl.dots[:, 0:3] *= 0.03 / 0.2
+        wl.dots[:, 8] = 2e-5
+        steps = 200
+    hist, bad = O.run_fast(wl.dots, wl.pulse, wl.constants, oracle_weights, steps)
+    assert bad is None
+    outs = []
+    for block in (1, 0):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+            info = sim.info()
+            if block:
+                assert info["fused_step"] == 2, info
+            sim.set_option("block_step", block)
+            outs.append(sim.run(steps))
+    np.testing.assert_array_equal(outs[0], outs[1])
+    assert_parity(hist, outs[0])
+    assert np.abs(outs[0][..., 1]).max() > 1e-8
+
+
 def test_autotuned_variant_changes_nothing(golden_weights):
     """The autotuner (at creation, and on request) chooses among far-kernel
     variants with identical arithmetic, so the trajectory does not depend on
