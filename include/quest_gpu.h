@@ -256,8 +256,8 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "profile" (1 = CUDA events around the far-pair kernel and the step
  * kernels: event nodes inside the block graphs, or around each launch when
  * "graph" is 0),
- * "far_variant" (0..5: resource shape of the far-pair kernel, same results;
- *   qg_create picks the fastest of 0, 3 and 5 for FP64 table handles of
+ * "far_variant" (0..6: resource shape of the far-pair kernel, same results;
+ *   qg_create picks the fastest of 0, 3, 5 and 6 for FP64 table handles of
  *   512 dots or more by timing one launch of each),
  * "autotune" (1 = time the far-kernel variants again now; at a block
  *   boundary between runs),

@@ -893,7 +893,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 static qg_status autotune_far(qg_handle *h)
 {
   if(h->otf || h->mixed || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
-  static const int candidates[] = {3, 0, 5};
+  static const int candidates[] = {6, 3, 0, 5};
   const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
   cudaEvent_t e0, e1;
   QG_CUDA(cudaEventCreate(&e0));
@@ -1721,7 +1721,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
       h->group = value;
       h->nG = (h->nT + value - 1) / value;
     } else if(!std::strcmp(key, "far_variant")) {
-      if(value < 0 || value > 5) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..5");
+      if(value < 0 || value > 6) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..6");
       h->far_variant = value;
     } else {
       if(value && !h->block_step_ok)

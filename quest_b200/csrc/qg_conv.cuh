@@ -50,6 +50,56 @@ __device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int 
   }
 }
 
+// Two samples per 32-byte load (ld.global.nc.v4.f64).  Ring rows start on
+// 32-byte boundaries (even row stride, 16-byte samples), so a load must start
+// at an even slot.
+template <bool LAB>
+__device__ __forceinline__ void ld_pair(const double2 *p, double2 &x, double2 &y)
+{
+  double a0, a1, a2, a3;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a0), "=d"(a1), "=d"(a2), "=d"(a3) : "l"(p));
+  x = LAB ? make_double2(2 * a0, 0.0) : make_double2(a0, a1);
+  y = LAB ? make_double2(2 * a2, 0.0) : make_double2(a2, a3);
+}
+
+__device__ __forceinline__ double2 sel2(bool odd, double2 a, double2 b) { return odd ? a : b; }
+
+// window_conv's result from 32-byte loads, for windows whose samples are all
+// live (tau0 >= -22).  The 32 lanes of a warp read windows at different
+// delays, so their first slots have different parities; a branch on the
+// parity would run the convolution twice.  Every lane instead loads
+// (K+Q+1)/2 rounded up pairs from the even slot at or below its first one,
+// L[0 ..], and takes sample m as L[m + par] by a select: the same products
+// in the same order as window_conv, hence the same result bit for bit, with
+// half the load instructions (each warp load touches about as many cache
+// lines as a 16-byte one, so the L1 wavefronts halve too).  The last sample
+// read is at slot0 + K + Q, inside the row's kRingMirror mirrored slots.
+template <int Q, bool LAB, int K>
+__device__ __forceinline__ void window_conv_pairs(const double2 *ring, int slot0, const double2 (&c)[Q + 1],
+                                                  double2 (&acc)[K])
+{
+  constexpr int M = K + Q;             // window samples
+  constexpr int NV = (M + 1 + 1) / 2;  // pairs loaded: L[0 .. M] (and one more when M is odd)
+  const bool odd = slot0 & 1;
+  const double2 *p = ring + (slot0 - (odd ? 1 : 0));
+  double2 prev = make_double2(0.0, 0.0);
+#pragma unroll
+  for(int v = 0; v < NV; ++v) {
+    double2 x, y;  // L[2v], L[2v+1]
+    ld_pair<LAB>(p + 2 * v, x, y);
+    // sample m = 2v-1 is L[2v] (odd) or L[2v-1] (even); sample 2v is L[2v+1] or L[2v]
+#pragma unroll
+    for(int e = 0; e < 2; ++e) {
+      const int m = 2 * v - 1 + e;
+      if(m < 0 || m >= M) continue;
+      const double2 w = e == 0 ? sel2(odd, x, prev) : sel2(odd, y, x);
+#pragma unroll
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfma(acc[k], c[k + Q - m], w);
+    }
+    prev = y;
+  }
+}
+
 __device__ __forceinline__ void cfmaf(float2 &acc, float2 c, float2 r)
 {
   acc.x = fmaf(c.x, r.x, acc.x);

@@ -235,6 +235,8 @@ __device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarSt
           window_conv2<Q, LAB, 1, K>(row, slot0 - 1, tau0, c, acc);
         else
           window_conv2<Q, LAB, 0, K>(row, slot0, tau0, c, acc);
+      } else if(VEC == 3 && tau0 >= -kWindow) {
+        window_conv_pairs<Q, LAB, K>(row, slot0, c, acc);
       } else {
         window_conv<Q, LAB, K>(row, slot0, tau0, c, acc);
       }
@@ -247,8 +249,10 @@ __device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarSt
 constexpr int kFarStages = 3;
 static_assert(4 * sizeof(FarStage<kMaxOrder, kFarStages>) <= 227 * 1024, "far stage buffers");
 
+// Variant 6 is held to 128 registers (4 blocks, 16 warps per SM); uncapped
+// it takes 132 and fits 3 blocks.
 template <int Q, bool LAB, int VEC>
-__global__ void __launch_bounds__(128) far_kernel_async(FarArgs a)
+__global__ void __launch_bounds__(128, VEC == 3 ? 4 : 1) far_kernel_async(FarArgs a)
 {
   extern __shared__ double2 far_smem[];
   constexpr int P = VEC == 2 ? kFarStages + 1 : kFarStages;
@@ -261,9 +265,11 @@ __global__ void __launch_bounds__(128) far_kernel_async(FarArgs a)
 //   far_kernel_r4     registers capped for 4 blocks per SM
 //   far_kernel_v2     capped, two samples per 32-byte load
 //   far_kernel_async  table staged in shared memory by cp.async, 3 sources
-//                     ahead; one sample (variant 3) or two (variant 4) per
-//                     load; variant 5: 4 stages and the next source's history
-//                     window prefetched into L1
+//                     ahead; one sample (variant 3) or two (variant 4, a
+//                     branch on each lane's window parity) per load; variant
+//                     5: 4 stages and the next source's history window
+//                     prefetched into L1; variant 6: two samples per load
+//                     with the parity taken by selects (window_conv_pairs)
 // ---- mixed precision ---------------------------------------------------------
 // The tap sum of one pair, sum_i c_i w_i, is formed as
 //     (sum_i c_i) w_0 + sum_i c_i (w_i - w_0),
@@ -423,7 +429,7 @@ static void launch_far_q(const FarArgs &a, cudaStream_t s)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
-  else if(a.variant >= 3 && a.variant <= 5) {
+  else if(a.variant >= 3 && a.variant <= 6) {
     // 38 KB at q = 5, 51 KB at q = 7 (above the 48 KB default: opt in);
     // variant 5 keeps one more stage
     const size_t smem = 4 * sizeof(FarStage<Q, kFarStages>), smem5 = 4 * sizeof(FarStage<Q, kFarStages + 1>);
@@ -434,12 +440,15 @@ static void launch_far_q(const FarArgs &a, cudaStream_t s)
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem5);
+      cudaFuncSetAttribute(far_kernel_async<Q, LAB, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if(dev < 64) attr_set[dev] = true;
     }
     if(a.variant == 3)
       far_kernel_async<Q, LAB, 0><<<blocks, 128, smem, s>>>(a);
     else if(a.variant == 4)
       far_kernel_async<Q, LAB, 1><<<blocks, 128, smem, s>>>(a);
+    else if(a.variant == 6)
+      far_kernel_async<Q, LAB, 3><<<blocks, 128, smem, s>>>(a);
     else
       far_kernel_async<Q, LAB, 2><<<blocks, 128, smem5, s>>>(a);
   }
