@@ -155,8 +155,16 @@ def fp64_peak_tflops(dtype="float64") -> float:
     return 2 * n ** 3 / (best / 1e3) / 1e12
 
 
-def table_roofline(mixed, achieved, hbm, src, traffic, alg_bytes, pipe_tf, pipe_peak, flops, K, avg_ms, pair_ms, ms,
-                   step_ms, launches, info, args):
+# far-pair kernel variants (qg_set_option "far_variant"; qg_create keeps the
+# fastest of 0, 3, 5 and 6): kernel name and the ncu summary of its traffic
+FAR_VARIANTS = {0: ("far_kernel<5,false>", "far_kernel_fp64_N4096"), 1: ("far_kernel_r4<5,false>", None),
+                2: ("far_kernel_v2<5,false>", None), 3: ("far_kernel_async<5,false,0>", "far_kernel_async_fp64_N4096"),
+                4: ("far_kernel_async<5,false,1>", None), 5: ("far_kernel_async<5,false,2>", None),
+                6: ("far_kernel_async<5,false,3>", "far_kernel_async_pairs_fp64_N4096")}
+
+
+def table_roofline(mixed, kname, variant, achieved, hbm, src, traffic, alg_bytes, pipe_tf, pipe_peak, flops, K,
+                   avg_ms, pair_ms, ms, step_ms, launches, info):
     """Roofline of the far-pair table kernel.  Its two ceilings are the
     table stream (algorithmic bytes / HBM copy bandwidth) and the
     convolution's multiply-adds (flops / cuBLAS GEMM rate of the same type);
@@ -172,7 +180,7 @@ def table_roofline(mixed, achieved, hbm, src, traffic, alg_bytes, pipe_tf, pipe_
                 "peak_source": "measured here: best cuBLAS %s 8192^3" % ("SGEMM (no TF32)" if mixed else "DGEMM")}
     main = pipe_obj if t_pipe >= t_hbm else hbm_obj
     r = {"bound": pipe if t_pipe >= t_hbm else "hbm",
-         "kernel": "far_kernel_mixed<5,false>" if mixed else "far_kernel_async<5,false,0>",
+         "kernel": kname,
          "achieved": main["achieved"], "peak": main["peak"], "unit": main["unit"], "frac": main["frac"],
          "peak_source": main["peak_source"], "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
          "steps_per_launch": K, "avg_launch_ms": avg_ms,
@@ -180,7 +188,7 @@ def table_roofline(mixed, achieved, hbm, src, traffic, alg_bytes, pipe_tf, pipe_
          "step_kernels_ms_per_step": step_ms / max(launches * K, 1),
          "step_form": {0: "general (12 launches per step)", 1: "fused (1 launch per step)",
                        2: "block (1 cooperative launch per 16 steps)"}[info["fused_step"]],
-         "far_variant": 3 if args.far_variant is None else args.far_variant,
+         "far_variant": variant,
          "hbm": hbm_obj, pipe: pipe_obj}
     return r
 
@@ -362,6 +370,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ms = e0.elapsed_time(e1)
     pair_ms, launches, step_ms, step_launches = sim.kernel_times()
+    variant = sim.get_option("far_variant")
     sim.close()
     ms_max = max_over_ranks(ms, world)
     value = job_throughput(world, n, args.steps, ms_max)
@@ -398,7 +407,8 @@ def run_ours(args, world, rank, local):
     fp64_tf = flops / (avg_ms / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops("float32" if mixed else "float64")
     # ncu dram read + write per launch of the same kernel on the same workload
-    traffic = profile_traffic("far_kernel_mixed_N4096" if mixed else "far_kernel_async_fp64_N4096")
+    kname, prof = ("far_kernel_mixed<5,false>", "far_kernel_mixed_N4096") if mixed else FAR_VARIANTS[variant]
+    traffic = profile_traffic(prof) if prof else None
     if otf:
         # compute-bound: every ordered pair's coefficients (FP64) once per
         # launch plus the K-step convolution (FP64, or FP32 in mixed)
@@ -427,9 +437,9 @@ def run_ours(args, world, rank, local):
         "dtype": "f32 pair sum + f64 state (mixed)" if mixed else "f64",
         "data": "synthetic (seeded dots and pulse of the stated distributions)",
         "config": config_dict(args),
-        "roofline": roof if otf else table_roofline(mixed, achieved, hbm, src, traffic, alg_bytes, fp64_tf,
-                                                    fp64_peak, flops, K, avg_ms, pair_ms, ms, step_ms, launches,
-                                                    info, args),
+        "roofline": roof if otf else table_roofline(mixed, kname, variant, achieved, hbm, src, traffic, alg_bytes,
+                                                    fp64_tf, fp64_peak, flops, K, avg_ms, pair_ms, ms, step_ms,
+                                                    launches, info),
         "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s,
                 "h2d_bytes_per_step": (n * 72 + 80) / total, "d2h_bytes_per_step": n * 32,
                 "includes": "qg_create (dots upload + %s) + qg_run with every step's rho read back" %

@@ -270,6 +270,11 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "reset" (restart the history at step 0, main.cpp:30-36). */
 qg_status qg_set_option(qg_handle *h, const char *key, int value);
 
+/* Reads an option back: "graph", "profile", "far_variant" (the variant in
+ * use, which after qg_create is the autotuner's choice), "block_step",
+ * "far_group".  No reference counterpart (the reference has no options). */
+qg_status qg_get_option(const qg_handle *h, const char *key, int *value);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,7 +72,7 @@ class QgInfo(ctypes.Structure):
 EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_destroy", "qg_run",
            "qg_next_step", "qg_history_evaluate", "qg_pulse_evaluate", "qg_set_history",
            "qg_get_history", "qg_get_info", "qg_footprint", "qg_stream", "qg_kernel_time",
-           "qg_set_option", "qg_history_evaluate_noalloc", "qg_get_state", "qg_bad_step",
+           "qg_set_option", "qg_get_option", "qg_history_evaluate_noalloc", "qg_get_state", "qg_bad_step",
            "qg_batch_create", "qg_batch_destroy", "qg_batch_add", "qg_batch_remove", "qg_batch_run",
            "qg_batch_size", "qg_checkpoint_size", "qg_checkpoint_save", "qg_checkpoint_load"]
 
@@ -108,6 +108,7 @@ def lib():
         L.qg_stream.restype = vp
         L.qg_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip, dp, ip]
         L.qg_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.qg_get_option.argtypes = [vp, ctypes.c_char_p, ip]
         L.qg_history_evaluate_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp]
         L.qg_get_state.argtypes = [vp, dp]
         L.qg_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
@@ -290,6 +291,11 @@ class Simulation:
 
     def set_option(self, key: str, value: int) -> None:
         _check(lib().qg_set_option(self.h, key.encode(), int(value)))
+
+    def get_option(self, key: str) -> int:
+        v = ctypes.c_int()
+        _check(lib().qg_get_option(self.h, key.encode(), ctypes.byref(v)))
+        return v.value
 
     def kernel_time(self, reset: bool = False) -> tuple[float, int]:
         """(far-pair kernel ms, launches) accumulated in profile mode."""

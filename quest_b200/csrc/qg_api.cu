@@ -577,7 +577,7 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   QG_TRY(upload_i(&h->d_mid_pj, mpj));
   QG_TRY(upload_i(&h->d_pb_ptr, pbptr));
   QG_TRY(upload_i(&h->d_pb_idx, pbidx));
-  QG_TRY(dalloc(h, &h->d_flags, std::max(h->step_blocks, 1)));
+  QG_TRY(dalloc(h, &h->d_flags, (size_t)std::max(h->step_blocks, 1) * kFlagStride));
   h->lag = h->fused && lag;
   return QG_OK;
 }
@@ -885,9 +885,10 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 
 // The far-kernel autotuner.  The FP64 table path has several kernels with
 // identical arithmetic (and so identical results) but different resource
-// shapes; which one is fastest depends on N and on the device.  One launch of
-// each, at a block start past the largest delay (every tap live, as in the
-// steady state), after one untimed launch; the fastest is kept.  The history
+// shapes; which one is fastest depends on N and on the device.  Each is
+// launched once untimed, then timed in two rounds (candidates interleaved,
+// best of the two kept), at a block start past the largest delay (every tap
+// live, as in the steady state); the fastest is kept.  The history
 // is whatever the handle holds (its values do not change the work), and the
 // far field and partials are recomputed by the next run.
 static qg_status autotune_far(qg_handle *h)
@@ -898,24 +899,32 @@ static qg_status autotune_far(qg_handle *h)
   cudaEvent_t e0, e1;
   QG_CUDA(cudaEventCreate(&e0));
   QG_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int best_v = h->far_variant;
-  for(int v : candidates) {
-    h->far_variant = v;
-    launch_set_int(h->d_ints + 7, t_test, h->stream);
-    const FarArgs fa = h->far_args(h->d_ints + 7, h->d_ints + 6);
-    launch_far(fa, h->stream);  // untimed: first use of the kernel
-    QG_CUDA(cudaEventRecord(e0, h->stream));
-    launch_far(fa, h->stream);
-    QG_CUDA(cudaEventRecord(e1, h->stream));
-    QG_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if(ms < best) {
-      best = ms;
-      best_v = v;
+  constexpr int nc = sizeof(candidates) / sizeof(candidates[0]);
+  float t_best[nc];
+  launch_set_int(h->d_ints + 7, t_test, h->stream);
+  for(int round = 0; round < 3; ++round)
+    for(int c = 0; c < nc; ++c) {
+      h->far_variant = candidates[c];
+      const FarArgs fa = h->far_args(h->d_ints + 7, h->d_ints + 6);
+      if(round == 0) {
+        launch_far(fa, h->stream);  // untimed: first use of the kernel
+        continue;
+      }
+      QG_CUDA(cudaEventRecord(e0, h->stream));
+      launch_far(fa, h->stream);
+      QG_CUDA(cudaEventRecord(e1, h->stream));
+      QG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      t_best[c] = round == 1 ? ms : std::min(t_best[c], ms);
     }
-  }
+  float best = 1e30f;
+  int best_v = candidates[0];
+  for(int c = 0; c < nc; ++c)
+    if(t_best[c] < best) {
+      best = t_best[c];
+      best_v = candidates[c];
+    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   QG_CUDA(cudaGetLastError());
@@ -1767,5 +1776,23 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
   } else {
     return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: unknown key '%s'", key);
   }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_get_option(const qg_handle *h, const char *key, int *value)
+{
+  if(!h || !key || !value) return qg_fail(QG_ERR_INVALID_ARG, "qg_get_option: NULL argument");
+  if(!std::strcmp(key, "graph"))
+    *value = h->use_graph ? 1 : 0;
+  else if(!std::strcmp(key, "profile"))
+    *value = h->profile ? 1 : 0;
+  else if(!std::strcmp(key, "far_variant"))
+    *value = h->far_variant;
+  else if(!std::strcmp(key, "block_step"))
+    *value = h->block_step ? 1 : 0;
+  else if(!std::strcmp(key, "far_group"))
+    *value = h->group;
+  else
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_get_option: unknown key '%s'", key);
   return QG_OK;
 }

@@ -167,6 +167,9 @@ void launch_far_step1(const FarArgs &a, void *stream);
 void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
                       int grid, void *stream);
 void launch_ring32_rebuild(const StepArgs &a, void *stream);
+// The step-block kernel's per-block step counts, one per 128-byte line (so
+// the polls on one block's count do not queue behind those on another's).
+constexpr int kFlagStride = 32;
 void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *flags, void *stream);
 int step_block_max_blocks(int q, int mid_cache, int hist_cap);
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
