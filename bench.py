@@ -346,12 +346,12 @@ def run_ours(args, world, rank, local):
     cmode = capi.COEF_ON_THE_FLY if otf else capi.COEF_TABLE
     sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec, coef_mode=cmode)
     info = sim.info()
+    if args.far_variant is not None:
+        sim.set_option("far_variant", args.far_variant)
     try:
         sim.run(args.warmup, record=False)
     except capi.NonFiniteError as e:
         nonfinite = e.step
-    if args.far_variant is not None:
-        sim.set_option("far_variant", args.far_variant)
     sim.set_option("profile", 1)
     sim.kernel_time(reset=True)
     stream = torch.cuda.ExternalStream(capi.lib().qg_stream(sim.h))
@@ -383,6 +383,8 @@ def run_ours(args, world, rank, local):
     t0 = time.perf_counter()
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec,
                          coef_mode=cmode) as sim2:
+        if args.far_variant is not None:
+            sim2.set_option("far_variant", args.far_variant)
         try:
             sim2.run(total, out=rho_host)
         except capi.NonFiniteError:

@@ -886,15 +886,16 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 // The far-kernel autotuner.  The FP64 table path has several kernels with
 // identical arithmetic (and so identical results) but different resource
 // shapes; which one is fastest depends on N and on the device.  Each is
-// launched once untimed, then timed in two rounds (candidates interleaved,
-// best of the two kept), at a block start past the largest delay (every tap
-// live, as in the steady state); the fastest is kept.  The history
+// launched twice untimed (first use, clocks settling), then timed in three
+// rounds (candidates interleaved, best of the three kept), at a block start
+// past the largest delay (every tap live, as in the steady state); the
+// fastest is kept.  The history
 // is whatever the handle holds (its values do not change the work), and the
 // far field and partials are recomputed by the next run.
 static qg_status autotune_far(qg_handle *h)
 {
   if(h->otf || h->mixed || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
-  static const int candidates[] = {6, 3, 0, 5};
+  static const int candidates[] = {0, 3, 5, 6};
   const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
   cudaEvent_t e0, e1;
   QG_CUDA(cudaEventCreate(&e0));
@@ -902,12 +903,12 @@ static qg_status autotune_far(qg_handle *h)
   constexpr int nc = sizeof(candidates) / sizeof(candidates[0]);
   float t_best[nc];
   launch_set_int(h->d_ints + 7, t_test, h->stream);
-  for(int round = 0; round < 3; ++round)
+  for(int round = 0; round < 5; ++round)
     for(int c = 0; c < nc; ++c) {
       h->far_variant = candidates[c];
       const FarArgs fa = h->far_args(h->d_ints + 7, h->d_ints + 6);
-      if(round == 0) {
-        launch_far(fa, h->stream);  // untimed: first use of the kernel
+      if(round < 2) {
+        launch_far(fa, h->stream);  // untimed: first use of the kernel, clocks settling
         continue;
       }
       QG_CUDA(cudaEventRecord(e0, h->stream));
@@ -916,7 +917,7 @@ static qg_status autotune_far(qg_handle *h)
       QG_CUDA(cudaEventSynchronize(e1));
       float ms = 0;
       QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      t_best[c] = round == 1 ? ms : std::min(t_best[c], ms);
+      t_best[c] = round == 2 ? ms : std::min(t_best[c], ms);
     }
   float best = 1e30f;
   int best_v = candidates[0];

@@ -602,16 +602,18 @@ void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, in
 // integrator weights, the launch's far-pair field and pulse, and (when they
 // fit) its part of the mid list and the recent rho01 of each distinct
 // mid-list partner.  Warp 0 runs step k on a scheduler of its own (warp 4,
-// which shares it, only posts finished steps) while warps 1-3 and 5-7 form
-// step k+1's window partials S_p and F + M_old (double-buffered).  M_old
-// reads the partners' history of step k-1 and earlier, so the helpers first
-// wait until every block that holds one of the block's mid-list partners (and
-// the block itself) has finished step k-1.  Each block counts its finished
-// steps in flags[block * kFlagStride] (zeroed before the launch); as soon as warp 0 has
-// stored a step's rho01 it hands the step to warp 4, which posts it (the
-// release waits for the stores; warp 0 goes on meanwhile).  Blocks wait only
-// for their partners' blocks, so nearby blocks may run a step or two apart
-// and no global barrier is needed.
+// which would share it, stays idle) while warps 1-3 and 5-7 form step k+1's
+// window partials S_p and F + M_old (double-buffered).  M_old reads the
+// partners' history of step k-1 and earlier, so the helpers first wait until
+// every block that holds one of the block's mid-list partners (and the block
+// itself) has finished step k-1.  Each block counts its finished steps in
+// flags[block * kFlagStride] (zeroed before the launch); warp 0 posts a step
+// as soon as its rho01 is stored.  The post is on the critical path between
+// blocks (a partner's post, then the helpers' work, bounds the step), so
+// warp 0 posts it itself: handing it to another warp through a barrier
+// delays it by that warp's wake-up and fence.  Blocks wait only for their
+// partners' blocks, so nearby blocks may run a step or two apart and no
+// global barrier is needed.
 //
 // M_new reads step k-1 of the delay-0/1 partners: with a.lag set every such
 // partner is in the dot's own block and its value comes from shared memory;
@@ -649,9 +651,9 @@ __device__ __forceinline__ void post_step(unsigned *p)
   asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
 }
 
-// Called by a whole warp: waits until flags[list[i] * kFlagStride] >= target for every
-// i < n (the lanes poll in parallel, each wait bounded).  False if a wait
-// ran out.
+// Called by a whole warp: waits until flags[list[i] * kFlagStride] >= target
+// for every i < n (the lanes poll in parallel, each wait bounded).  False if
+// a wait ran out.
 __device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *list, int n, unsigned target)
 {
   bool ok = true;
@@ -670,15 +672,6 @@ __device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *li
 }
 
 __device__ __forceinline__ void helpers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kHelpers)); }
-
-// Hand-off of a finished step from warp 0 to warp 4 (named barrier 2, 64
-// threads): warp 0 arrives once its rho01 stores are issued and goes on;
-// warp 4 waits, then posts the step.  The arrival orders warp 0's stores
-// before warp 4's release (barrier synchronisation, then a cumulative
-// release), so a block that sees the count sees the stores, while the
-// release's wait for the stores to complete is off warp 0's path.
-__device__ __forceinline__ void post_arrive() { asm volatile("bar.arrive 2, 64;" ::: "memory"); }
-__device__ __forceinline__ void post_wait() { asm volatile("bar.sync 2, 64;" ::: "memory"); }
 
 // S_p of either the predictor sums (HQ = false: rho00, rho01) or the
 // corrector sums (HQ = true), each accumulator with the same operations as
@@ -934,10 +927,10 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
           pul = m.pul[k * BS + lane];
         }
         dot_iterate(a, live, block_near, nr, m.cur, lane, P, H, past, pul, dc, r, dr);
-        // rho01 first, then hand the post to warp 4, then the rest of the state
+        // rho01 first, then post the step, then the rest of the state
         if(live) finish_ring(a, idx, t, r);
         __syncwarp();
-        post_arrive();
+        if(lane == 0) post_step(flags + (long long)blk * kFlagStride);
         if(live) {
           finish_state(a, idx, t, r, dr);
           const int sl = pc_slot(t);
@@ -949,17 +942,10 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
         __syncwarp();
         m.prev01[lane] = live ? r[1] : make_double2(0.0, 0.0);
         if(k == kTimeBlock - 1 && blk == 0 && lane == 0) *a.d_next = t + 1;
-      } else {
-        if(lane == 0) {
-          s_abort = 1;
-          atomicMin(a.d_bad, -2);
-        }
-        __syncwarp();
-        post_arrive();  // warp 4 sees s_abort and posts nothing
+      } else if(lane == 0) {
+        s_abort = 1;
+        atomicMin(a.d_bad, -2);
       }
-    } else if(part == 4) {
-      post_wait();
-      if(lane == 0 && !*(volatile int *)&s_abort) post_step(flags + (long long)blk * kFlagStride);
     } else if(helper && k + 1 < k1 && t + 1 < a.T) {
       // step k+1's sums; M_old needs the partner blocks' step k-1
       if(hw == 0 && k > k0 && !wait_blocks(flags, a.pb_idx + B0, NB, k - k0) && lane == 0) {
