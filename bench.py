@@ -47,6 +47,12 @@ TABLE_BYTES_PER_PAIR = lambda q: 4 + 16 * (q + 1)  # noqa: E731  int32 delay + (
 # 6 reciprocals + node products and sums (~190), dyad scalars (~30), 6 taps
 # of complex assembly (~90), sqrt / modf / sincos counted as ~40
 OTF_COEF_FLOPS = 350
+# Mixed precision (pair_coef_otf_mixed, q = 5): FP64 for the distance, the
+# delay split, 1/r and the phase reduction (~80, sqrt and divisions counted
+# as ~20 each); FP32 for the weights (6 nodes x (5 subtractions + 15 FMA of
+# the symmetric-polynomial recurrence + 6 products) ~ 250), the dyad scalars
+# (~35) and the 6 taps with their sum (~120)
+OTF_COEF_FLOPS_MIXED = (80, 400)  # (FP64, FP32)
 
 
 def peaks():
@@ -412,14 +418,16 @@ def run_ours(args, world, rank, local):
     kname, prof = ("far_kernel_mixed<5,false>", "far_kernel_mixed_N4096") if mixed else FAR_VARIANTS[variant]
     traffic = profile_traffic(prof) if prof else None
     if otf:
-        # compute-bound: every ordered pair's coefficients (FP64) once per
-        # launch plus the K-step convolution (FP64, or FP32 in mixed)
-        coef_flops = 2 * (info["num_pairs"]) * OTF_COEF_FLOPS
+        # compute-bound: every ordered pair's coefficients once per launch
+        # (FP64; in mixed precision mostly FP32) plus the K-step convolution
+        # (FP64, or FP32 in mixed)
+        c64, c32 = OTF_COEF_FLOPS_MIXED if mixed else (OTF_COEF_FLOPS, 0)
+        coef_flops = 2 * (info["num_pairs"]) * (c64 + c32)
         d_peak = fp64_peak if not mixed else fp64_peak_tflops("float64")
         t_s = avg_ms / 1e3
-        # time-weighted peak: coefficient flops at the FP64 rate, convolution
-        # flops at the precision's rate
-        ideal_s = coef_flops / (d_peak * 1e12) + flops / (fp64_peak * 1e12)
+        # time-weighted peak: each kind of flop at its type's measured rate
+        ideal_s = (2 * info["num_pairs"] * c64) / (d_peak * 1e12) + \
+            (2 * info["num_pairs"] * c32 + flops) / (fp64_peak * 1e12)
         roof = {"bound": "fp64" if not mixed else "fp64+fp32", "kernel": "far_otf_kernel<5,false,%s>" %
                 ("true" if mixed else "false"),
                 "achieved": (coef_flops + flops) / t_s / 1e12, "unit": "TFLOP/s",
@@ -427,7 +435,7 @@ def run_ours(args, world, rank, local):
                 "DGEMM%s 8192^3" % (" and SGEMM (no TF32)" if mixed else ""),
                 "frac": ideal_s / t_s, "traffic": None,
                 "coef_flops_per_launch": coef_flops, "conv_flops_per_launch": flops,
-                "coef_flops_per_pair": OTF_COEF_FLOPS, "steps_per_launch": K, "avg_launch_ms": avg_ms,
+                "coef_flops_per_pair": {"fp64": c64, "fp32": c32}, "steps_per_launch": K, "avg_launch_ms": avg_ms,
                 "share_of_timed_region": pair_ms / ms if ms > 0 else None,
                 "step_kernels_ms_per_step": step_ms / max(launches * K, 1),
                 "step_form": {0: "general (12 launches per step)", 1: "fused (1 launch per step)",

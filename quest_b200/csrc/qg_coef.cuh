@@ -238,4 +238,107 @@ __device__ __forceinline__ int pair_coef_otf(const double (&psrc)[3], const doub
   return fd;
 }
 
+// Mixed-precision coefficients of one pair for the on-the-fly kernel.  FP64
+// is kept for the distance and the split of r / (c dt) into the floor delay
+// and the fraction x (the operations of pair_coef_otf, so the far / mid split
+// is the same), and for reducing the phase argument -omega r / c to
+// [-pi, pi]; the Lagrange weights, the dyad factors and the taps are FP32.
+//
+// Weights: with f_m = x - m and e_k the elementary symmetric polynomials of
+// {f_m : m != b}, the reference's w0 = prod f_m / den, w1 = w0 sum(-1/f_m) / dt
+// and w2 = w0 (sum(-1/f_m^2) + (sum 1/f_m)^2) / dt^2 (lagrange_set.cpp:17-41)
+// are w0 = e_Q / den, w1 = -e_{Q-1} / (den dt), w2 = 2 e_{Q-2} / (den dt^2):
+// no reciprocals, so no cancellation between 1/x-sized terms as x -> 0.
+//
+// cf[0..Q] are the taps and cf[Q+1] their sum, taken from the identities
+// sum w0 = 1, sum w1 = sum w2 = 0 as the w0-only coefficient: the
+// difference-form convolution multiplies the sum by the window's first
+// sample and each tap by a step difference, so the sum must be accurate to
+// FP32 rounding while the taps (each ~1e-7 relative) only meet differences.
+// An integer delay (x = 0) gives NaN taps, as the reference's weights do.
+template <int Q>
+__device__ __forceinline__ int pair_coef_otf_mixed(const double (&psrc)[3], const double (&pobs)[3],
+                                                   const double (&dsrc)[3], const double (&dobs)[3],
+                                                   const CoefParams &p, float2 (&cf)[Q + 2])
+{
+  double dr[3];
+#pragma unroll
+  for(int k = 0; k < 3; ++k) dr[k] = pobs[k] - psrc[k];
+  const double sq = (dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2];
+  const double nrm = sqrt(sq);
+  double idelay;
+  const double xd = modf(nrm / (p.c0 * p.dt), &idelay);
+  const int fd = (int)idelay;
+
+  const float x = (float)xd;
+  const float inv_dt = (float)(1.0 / p.dt);
+  float w0[Q + 1], w1[Q + 1], w2[Q + 1];
+#pragma unroll
+  for(int b = 0; b <= Q; ++b) {
+    float e[Q + 1];
+    e[0] = 1.f;
+#pragma unroll
+    for(int k = 1; k <= Q; ++k) e[k] = 0.f;
+    int n = 0;
+#pragma unroll
+    for(int m = 0; m <= Q; ++m) {
+      if(m == b) continue;
+      const float f = x - (float)m;
+      ++n;
+#pragma unroll
+      for(int k = Q; k >= 1; --k)
+        if(k <= n) e[k] = fmaf(f, e[k - 1], e[k]);
+    }
+    float den = 1.f;
+#pragma unroll
+    for(int m = 0; m <= Q; ++m)
+      if(m != b) den *= (float)(b - m);  // an exact integer (|den| <= 7!)
+    const float id = 1.f / den;
+    w0[b] = e[Q] * id;
+    w1[b] = -(e[Q - 1] * id) * inv_dt;
+    w2[b] = Q >= 2 ? (2.f * (e[Q >= 2 ? Q - 2 : 0] * id)) * (inv_dt * inv_dt) : 0.f;
+  }
+
+  const float drf[3] = {(float)dr[0], (float)dr[1], (float)dr[2]};
+  const float df_s[3] = {(float)dsrc[0], (float)dsrc[1], (float)dsrc[2]};
+  const float df_o[3] = {(float)dobs[0], (float)dobs[1], (float)dobs[2]};
+  const float dd = fmaf(df_o[2], df_s[2], fmaf(df_o[1], df_s[1], df_o[0] * df_s[0]));
+  const float ar = fmaf(df_o[2], drf[2], fmaf(df_o[1], drf[1], df_o[0] * drf[0]));
+  const float br = fmaf(df_s[2], drf[2], fmaf(df_s[1], drf[1], df_s[0] * drf[0]));
+  const float inv_r = (float)(1.0 / nrm), inv_sq = inv_r * inv_r;
+  const float ab = (ar * br) * inv_sq;
+  const float g3 = fmaf(-3.f, ab, dd), g1 = dd - ab;
+  const float c0 = (float)p.c0;
+  const float G0 = (g3 * (c0 * c0)) * (inv_sq * inv_r);
+  const float G1 = (g3 * c0) * inv_sq;
+  const float G2 = g1 * inv_r;
+  const float A = (float)(p.mu0 / (4 * M_PI * p.hbar));
+  if(p.frame == 0) {
+    const double om = p.omega;
+    const double ph = (-om * nrm) / p.c0;
+    const double red = ph - 6.283185307179586 * rint(ph * 0.15915494309189535);
+    float sn, cs;
+    sincosf((float)red, &sn, &cs);
+    const float2 sc = make_float2(-A * cs, -A * sn);
+    const float omf = (float)om, om2 = omf * omf;
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) {
+      const float re = fmaf(G2, fmaf(-om2, w0[i], w2[i]), fmaf(G0, w0[i], G1 * w1[i]));
+      const float im = omf * fmaf(G1, w0[i], 2.f * (G2 * w1[i]));
+      cf[i] = make_float2(fmaf(sc.x, re, -sc.y * im), fmaf(sc.x, im, sc.y * re));
+    }
+    const float rs = fmaf(-om2, G2, G0), is = omf * G1;
+    cf[Q + 1] = make_float2(fmaf(sc.x, rs, -sc.y * is), fmaf(sc.x, is, sc.y * rs));
+  } else {
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) cf[i] = make_float2(A * fmaf(G2, w2[i], fmaf(G0, w0[i], G1 * w1[i])), 0.f);
+    cf[Q + 1] = make_float2(A * G0, 0.f);
+  }
+  if(xd == 0.0) {
+#pragma unroll
+    for(int i = 0; i <= Q + 1; ++i) cf[i] = make_float2(__int_as_float(0x7fc00000), 0.f);
+  }
+  return fd;
+}
+
 }  // namespace qg

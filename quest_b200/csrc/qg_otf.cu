@@ -9,8 +9,9 @@
 // computed once per pair per K steps, so about 400 instructions of
 // coefficient work are shared by K = 16 steps of (q+1)-tap convolution.
 //
-// FP64: FP64 coefficients and convolution.  Mixed: FP64 coefficients,
-// rounded to FP32 with their sum as the table build does, and the FP32
+// FP64: FP64 coefficients and convolution.  Mixed: FP32 coefficients
+// (pair_coef_otf_mixed: FP64 only for the distance, the delay split and the
+// phase reduction) with their sum from the Lagrange identities, and the FP32
 // difference-form convolution of the mixed table path.
 //
 // Compiled with -fmad=false (the delay arithmetic must match the near-pair
@@ -73,25 +74,23 @@ __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
       ds[k] = a_src ? da[k] : db[k];
       dob[k] = a_src ? db[k] : da[k];
     }
-    double2 c[Q + 1];
-    const int d = pair_coef_otf<Q>(ps, po, ds, dob, a.cp, c);
-    if(valid && d >= kTimeBlock) {
-      const int tau0 = t0 - d - Q;
-      int slot0 = tau0 % W;
-      if(slot0 < 0) slot0 += W;
-      if(MIXED) {
-        float2 cf[Q + 2];
-        double2 sum = make_double2(0.0, 0.0);
-#pragma unroll
-        for(int i = 0; i <= Q; ++i) {
-          cf[i] = make_float2((float)c[i].x, (float)c[i].y);
-          sum.x += c[i].x;
-          sum.y += c[i].y;
-        }
-        cf[Q + 1] = make_float2((float)sum.x, (float)sum.y);
+    if(MIXED) {
+      float2 cf[Q + 2];
+      const int d = pair_coef_otf_mixed<Q>(ps, po, ds, dob, a.cp, cf);
+      if(valid && d >= kTimeBlock) {
+        const int tau0 = t0 - d - Q;
+        int slot0 = tau0 % W;
+        if(slot0 < 0) slot0 += W;
         window_conv_mixed<Q, LAB, K>(a.ring32w + (long long)ib * a.stride, a.ring32d + (long long)ib * a.stride,
                                      slot0, tau0, cf, accf);
-      } else {
+      }
+    } else {
+      double2 c[Q + 1];
+      const int d = pair_coef_otf<Q>(ps, po, ds, dob, a.cp, c);
+      if(valid && d >= kTimeBlock) {
+        const int tau0 = t0 - d - Q;
+        int slot0 = tau0 % W;
+        if(slot0 < 0) slot0 += W;
         window_conv<Q, LAB, K>(a.ring + (long long)ib * a.stride, slot0, tau0, c, acc);
       }
     }
