@@ -24,7 +24,10 @@
 
 namespace qg {
 
-template <int Q, bool LAB, bool MIXED, int K = kTimeBlock>
+// PACKED: the mixed convolution with packed FP32 pairs (same bits).  Measured
+// at N = 65536 it is slower here (10.0 against 9.4 ms per step): the swaps it
+// needs compete for issue slots with the coefficient work.
+template <int Q, bool LAB, bool MIXED, int K = kTimeBlock, bool PACKED = false>
 __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
 {
   const int lane = threadIdx.x & 31;
@@ -81,8 +84,8 @@ __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
         const int tau0 = t0 - d - Q;
         int slot0 = tau0 % W;
         if(slot0 < 0) slot0 += W;
-        window_conv_mixed<Q, LAB, K>(a.ring32w + (long long)ib * a.stride, a.ring32d + (long long)ib * a.stride,
-                                     slot0, tau0, cf, accf);
+        window_conv_mixed<Q, LAB, K, PACKED>(a.ring32w + (long long)ib * a.stride,
+                                             a.ring32d + (long long)ib * a.stride, slot0, tau0, cf, accf);
       }
     } else {
       double2 c[Q + 1];
