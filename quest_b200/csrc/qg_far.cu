@@ -357,31 +357,22 @@ __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restric
         hi = mid - 1;
     }
     const FarArgs a = args[lo];  // a copy: the bodies read its fields in their inner loops
-    if(MIXED) {
+    if(MIXED)
       far_body_mixed<Q, LAB>(a, task - task_off[lo]);
-    } else {
-      extern __shared__ double2 far_smem[];
-      FarStage<Q, kFarStages> *st = reinterpret_cast<FarStage<Q, kFarStages> *>(far_smem);
-      far_body_async<Q, LAB, kFarStages, 0>(a, task - task_off[lo], st[threadIdx.x >> 5]);
-    }
+    else
+      far_body<Q, LAB, 0>(a, task - task_off[lo]);
   }
 }
 
-// FP64 members stage their table entries in shared memory (as far_kernel_async)
+// FP64 members take far_kernel's body (table prefetched in registers, the
+// fastest FP64 variant, 168 registers: 3 blocks per SM, the persistent
+// grid's shape); mixed members the scalar FP32 convolution (the packed form
+// measured 13 % slower in this kernel).  Every form gives the same bits, so
+// a member's result is the same alone and in a batch.
 template <int Q, bool LAB, bool MIXED>
 static void launch_far_batch_q(const FarArgs *args, const int *task_off, int n_ens, int grid, cudaStream_t s)
 {
-  const size_t smem = MIXED ? 0 : 4 * sizeof(FarStage<Q, kFarStages>);
-  if(smem > 48 * 1024) {
-    static bool attr_set[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if(dev >= 64 || !attr_set[dev]) {
-      cudaFuncSetAttribute(far_batch_kernel<Q, LAB, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if(dev < 64) attr_set[dev] = true;
-    }
-  }
-  far_batch_kernel<Q, LAB, MIXED><<<grid, 128, smem, s>>>(args, task_off, n_ens);
+  far_batch_kernel<Q, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens);
 }
 
 template <bool LAB, bool MIXED>
