@@ -841,40 +841,82 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
   const int B0 = a.pb_ptr[blk], NB = a.pb_ptr[blk + 1] - B0;  // blocks holding this block's partners
 
   // prologue: window, weights, the launch's far field and pulse, prev01, and
-  // the block's mid list and partner history when they fit
-  for(int sl = part; sl < kPcDepth; sl += kBlockWarps)
-    for(int c = 0; c < 4; ++c) m.win[sl][c][lane] = a.pcr[((long long)sl * 4 + c) * a.n_pad + idx];
+  // the block's mid list and partner history when they fit.  The copies are
+  // latency-bound (one L2 round trip each), so each thread issues several
+  // independent loads before it stores any.
+  constexpr int kPro = 4;  // loads in flight per thread in the copy loops
+  for(int sl = part; sl < kPcDepth; sl += kBlockWarps) {
+    double2 v[4];
+#pragma unroll
+    for(int c = 0; c < 4; ++c) v[c] = a.pcr[((long long)sl * 4 + c) * a.n_pad + idx];
+#pragma unroll
+    for(int c = 0; c < 4; ++c) m.win[sl][c][lane] = v[c];
+  }
   for(int i = threadIdx.x; i < 2 * nt; i += blockDim.x) {
     m.ps[i] = a.w.ps[i];
     m.cs[i] = a.w.cs[i];
   }
-  for(int kk = k0 + part; kk < k1; kk += kBlockWarps) {
-    m.far[kk * BS + lane] = live ? a.far_field[(long long)kk * a.n_pad + idx] : make_double2(0.0, 0.0);
-    m.pul[kk * BS + lane] = live ? pulse_rabi(a, idx, t0 + kk) : 0.0;
+  {
+    // the pulse from the dot's k.r and dipole, loaded once (pulse_rabi's
+    // operations)
+    const double kr = live ? pulse_kr(a, idx) : 0.0;
+    const double d0 = live ? a.dip[3 * idx] : 0.0, d1 = live ? a.dip[3 * idx + 1] : 0.0,
+                 d2 = live ? a.dip[3 * idx + 2] : 0.0;
+    for(int kk = k0 + part; kk < k1; kk += kBlockWarps) {
+      m.far[kk * BS + lane] = live ? a.far_field[(long long)kk * a.n_pad + idx] : make_double2(0.0, 0.0);
+      m.pul[kk * BS + lane] = live ? pulse_at(a, kr, d0, d1, d2, t0 + kk) : 0.0;
+    }
   }
   const int E0 = a.mid_ptr[blk * BS], E = a.mid_ptr[blk * BS + BS] - E0;
   const bool cached = E <= a.mid_cache;
   const int P0 = a.bp_ptr[blk], NP = a.bp_ptr[blk + 1] - P0;
   const bool hist = cached && a.hist_cap > 0 && NP <= a.hist_cap;
   if(cached) {
-    const int q1 = a.q + 1;
-    for(int i = threadIdx.x; i < E * q1; i += blockDim.x) {
-      const int e = i / q1, tap = i - e * q1;
-      m.mc_coef[tap * a.mid_cache + e] = a.mid_coef[(long long)E0 * q1 + i];
+    const int q1 = a.q + 1, total = E * q1;
+    for(int i0 = threadIdx.x; i0 < total; i0 += kPro * blockDim.x) {
+      double2 v[kPro];
+#pragma unroll
+      for(int u = 0; u < kPro; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if(i < total) v[u] = a.mid_coef[(long long)E0 * q1 + i];
+      }
+#pragma unroll
+      for(int u = 0; u < kPro; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if(i < total) {
+          const int e = i / q1, tap = i - e * q1;
+          m.mc_coef[tap * a.mid_cache + e] = v[u];
+        }
+      }
     }
     for(int i = threadIdx.x; i < E; i += blockDim.x) {
       m.mc_idx[i] = hist ? a.mid_pj[E0 + i] : a.mid_idx[E0 + i];
       m.mc_del[i] = a.mid_delay[E0 + i];
     }
   }
-  if(hist)
-    for(int i = threadIdx.x; i < NP; i += blockDim.x) m.bp[i] = a.bp_idx[P0 + i];
   if(hist) {
+    for(int i = threadIdx.x; i < NP; i += blockDim.x) m.bp[i] = a.bp_idx[P0 + i];
+    __syncthreads();  // uniform: hist depends on the block only
     // samples t0+k0-22 .. t0+k0-2; later ones are appended step by step
-    const int first = t0 + k0 - kHistSpan, count = kHistSpan - 1;
-    for(int i = threadIdx.x; i < NP * count; i += blockDim.x) {
-      const int j = i / count, s = first + i % count;
-      m.hist[j * kHistStride + hist_slot(s)] = __ldcg(a.ring + (long long)a.bp_idx[P0 + j] * a.stride + ring_slot(s, a.W));
+    const int first = t0 + k0 - kHistSpan, count = kHistSpan - 1, total = NP * count;
+    for(int i0 = threadIdx.x; i0 < total; i0 += kPro * blockDim.x) {
+      double2 v[kPro];
+#pragma unroll
+      for(int u = 0; u < kPro; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if(i < total) {
+          const int j = i / count, s = first + i % count;
+          v[u] = __ldcg(a.ring + (long long)m.bp[j] * a.stride + ring_slot(s, a.W));
+        }
+      }
+#pragma unroll
+      for(int u = 0; u < kPro; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if(i < total) {
+          const int j = i / count, s = first + i % count;
+          m.hist[j * kHistStride + hist_slot(s)] = v[u];
+        }
+      }
     }
   }
   if(part == 0) m.prev01[lane] = a.ring[(long long)idx * a.stride + ring_slot(t0 + k0 - 1, a.W)];
