@@ -255,7 +255,8 @@ __device__ __forceinline__ int pair_coef_otf(const double (&psrc)[3], const doub
 // difference-form convolution multiplies the sum by the window's first
 // sample and each tap by a step difference, so the sum must be accurate to
 // FP32 rounding while the taps (each ~1e-7 relative) only meet differences.
-// An integer delay (x = 0) gives NaN taps, as the reference's weights do.
+// An integer delay (x = 0) gives NaN taps 1..Q (and sum) and a finite tap 0,
+// as the reference's weights do, so a run turns non-finite at the same step.
 template <int Q>
 __device__ __forceinline__ int pair_coef_otf_mixed(const double (&psrc)[3], const double (&pobs)[3],
                                                    const double (&dsrc)[3], const double (&dobs)[3],
@@ -335,8 +336,11 @@ __device__ __forceinline__ int pair_coef_otf_mixed(const double (&psrc)[3], cons
     cf[Q + 1] = make_float2(A * G0, 0.f);
   }
   if(xd == 0.0) {
+    // the reference's weights at x = 0: node 0's are finite, every other
+    // node's w1 and w2 are 0 * inf = NaN (lagrange_set.cpp:25-33); the sum
+    // carries them
 #pragma unroll
-    for(int i = 0; i <= Q + 1; ++i) cf[i] = make_float2(__int_as_float(0x7fc00000), 0.f);
+    for(int i = 1; i <= Q + 1; ++i) cf[i] = make_float2(__int_as_float(0x7fc00000), 0.f);
   }
   return fd;
 }

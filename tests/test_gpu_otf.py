@@ -5,8 +5,10 @@ an algebraically equal form of the reference's table build.
 Checks: the interaction-level sum (HistoryInteraction::evaluate) against the
 oracle's reference-order table on random histories, whole runs against the
 oracle at the FP64 tolerance (1e-10), against the table path, in the lab
-frame and at other interpolation orders, mixed precision against FP64, and
-the N = 65536 workload (whose table would need 215 GB) for a few blocks."""
+frame and at other interpolation orders, mixed precision (FP32
+coefficients) against FP64, the reference's non-finite run at an integer
+delay, and the N = 65536 workload (whose table would need 215 GB) for a
+few blocks."""
 import numpy as np
 import pytest
 
@@ -113,6 +115,24 @@ def test_otf_mixed_matches_fp64(golden_weights):
     assert info["precision"] == capi.PREC_MIXED and info["coef_mode"] == capi.COEF_ON_THE_FLY
     assert rel_err(ref[..., 0], got[..., 0]) <= 1e-6
     assert rel_err(ref[..., 1], got[..., 1]) <= 1e-6
+
+
+def test_otf_integer_delay_raises_where_the_reference_does(golden_weights, oracle_weights):
+    """A pair at an exactly integer delay (distance 5, c dt = 0.125: 40
+    steps, a far pair) has NaN Lagrange weights in the reference; the
+    on-the-fly coefficients, FP64 and FP32, make the run non-finite at the
+    step the reference and the table path do."""
+    c = I.Constants(c0=1.0, dt=0.125, num_timesteps=40)
+    dots = np.array([[0.0, 0, 0, 200, 10, 10, 0, 0, 2e-3],
+                     [5.0, 0, 0, 200, 10, 10, 0, 0, 2e-3]])
+    _, bad = O.run_faithful(dots, I.make_pulse(delay=0.0), c, oracle_weights, 40)
+    assert bad is not None
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        with capi.Simulation(dots, I.make_pulse(delay=0.0), c, weights=golden_weights, precision=prec,
+                             coef_mode=capi.COEF_ON_THE_FLY) as sim:
+            with pytest.raises(capi.NonFiniteError) as e:
+                sim.run(40)
+        assert e.value.step == bad, (prec, e.value.step, bad)
 
 
 def test_otf_rejected_where_a_table_is_needed(golden_weights):
