@@ -370,10 +370,11 @@ def test_integer_delay_raises_where_the_reference_does(golden_weights, oracle_we
     dots = np.array([[0.0, 0, 0, 200, 10, 10, 0, 0, 2e-3],
                      [5.0, 0, 0, 200, 10, 10, 0, 0, 2e-3]])
     _, bad = O.run_faithful(dots, I.make_pulse(delay=0.0), c, oracle_weights, 40)
-    with capi.Simulation(dots, I.make_pulse(delay=0.0), c, weights=golden_weights) as sim:
-        with pytest.raises(capi.NonFiniteError) as e:
-            sim.run(40)
-    assert e.value.step == bad == 19
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        with capi.Simulation(dots, I.make_pulse(delay=0.0), c, weights=golden_weights, precision=prec) as sim:
+            with pytest.raises(capi.NonFiniteError) as e:
+                sim.run(40)
+        assert e.value.step == bad == 19, prec
 
 
 def test_steps_past_the_end_are_rejected(golden_weights):
