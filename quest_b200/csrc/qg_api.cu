@@ -368,6 +368,8 @@ static size_t table_bytes(int nT, int q, bool mixed)
 }
 
 // Even, so every ring row starts 32-byte aligned for paired-sample loads.
+static int far_group(bool mixed, int nT) { return mixed && nT < 256 ? 2 : kTileGroup; }
+
 static int ring_depth(int max_delay, int q)
 {
   const int w = max_delay + q + kTimeBlock + 2;
@@ -744,9 +746,11 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_TRY(order_for_near_groups(h, dots, morton_order(dots, n), order));
   h->n_pad = (int)order.size();
   h->nT = h->n_pad / kTile;
-  // source tiles per far-kernel warp: 2 for the mixed path (twice as many
-  // warps balance its shorter per-source work better), 4 in FP64
-  h->group = p->precision == QG_PREC_MIXED ? 2 : kTileGroup;
+  // source tiles per far-kernel warp: 4 in FP64; 2 for the mixed path up to
+  // 255 tiles (twice as many warps balance its shorter per-source work
+  // better), 4 from 256 tiles, where the partial sums (16 steps x groups x
+  // N, FP64) would otherwise add ~13 % to the FP32 table stream
+  h->group = far_group(p->precision == QG_PREC_MIXED, h->nT);
   h->nG = (h->nT + h->group - 1) / h->group;
   h->nblk = (long long)h->nT * (h->nT + 1) / 2;
   std::vector<double> pos((size_t)h->n_pad * 3, 0.0), dip((size_t)h->n_pad * 3, 0.0);
@@ -1679,7 +1683,7 @@ extern "C" qg_status qg_footprint(int n, const qg_params *p, double side, size_t
   if(!p || !bytes || n < 1) return qg_fail(QG_ERR_INVALID_ARG, "qg_footprint: bad argument");
   const int nT = (n + kTile - 1) / kTile, n_pad = nT * kTile;
   const bool otf = p->coef_mode == QG_COEF_ON_THE_FLY;
-  const int group = otf ? (nT + 15) / 16 : (p->precision == QG_PREC_MIXED ? 2 : kTileGroup);
+  const int group = otf ? (nT + 15) / 16 : far_group(p->precision == QG_PREC_MIXED, nT);
   const int nG = otf ? (nT + group - 1) / group : (nT <= 512 ? nT : (nT + group - 1) / group);
   const int q = p->interpolation_order;
   const int md = (int)std::floor(side * std::sqrt(3.0) / (p->c0 * p->dt));
