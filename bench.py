@@ -161,8 +161,9 @@ def fp64_peak_tflops(dtype="float64") -> float:
     return 2 * n ** 3 / (best / 1e3) / 1e12
 
 
-# far-pair kernel variants (qg_set_option "far_variant"; qg_create keeps the
-# fastest of 0, 3, 5 and 6): kernel name and the ncu summary of its traffic
+# far-pair kernel variants (qg_set_option "far_variant"; the first qg_run
+# keeps the fastest of 0, 3, 5 and 6): kernel name and the ncu summary of
+# its traffic
 FAR_VARIANTS = {0: ("far_kernel<5,false>", "far_kernel_fp64_N4096"), 1: ("far_kernel_r4<5,false>", None),
                 2: ("far_kernel_v2<5,false>", None), 3: ("far_kernel_async<5,false,0>", "far_kernel_async_fp64_N4096"),
                 4: ("far_kernel_async<5,false,1>", None), 5: ("far_kernel_async<5,false,2>", None),

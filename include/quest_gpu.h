@@ -257,8 +257,9 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * kernels: event nodes inside the block graphs, or around each launch when
  * "graph" is 0),
  * "far_variant" (0..6: resource shape of the far-pair kernel, same results;
- *   qg_create picks the fastest of 0, 3, 5 and 6 for FP64 table handles of
- *   512 dots or more by timing one launch of each),
+ *   the first qg_run of an FP64 table handle of 512 dots or more picks the
+ *   fastest of 0, 3, 5 and 6 by timing launches of each, unless a variant
+ *   was set; batch members are not timed, the batch kernel having its own),
  * "autotune" (1 = time the far-kernel variants again now; at a block
  *   boundary between runs),
  * "far_group" (source tiles each far-kernel warp sums before writing its

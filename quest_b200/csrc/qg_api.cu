@@ -121,6 +121,7 @@ struct qg_handle_s {
   bool use_graph = true;
   int far_variant = 3;  // cp.async-staged table (see qg_far.cu); the autotuner may change it
   float tuned_far_ms = 0;  // far-kernel time of the autotuner's choice
+  bool tune_pending = false;  // the far-kernel autotuner runs at the first qg_run
   bool profile = false;
   cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
   bool events_ready = false;
@@ -882,8 +883,9 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 
   QG_TRY(build_lists(h, ta));
   QG_TRY(reset_state(h));
-  QG_TRY(autotune_far(h));
-  QG_TRY(reset_state(h));
+  // the far-kernel autotuner runs at the first qg_run: a batch member never
+  // runs alone (the batch kernel has its own form), so it is never timed
+  h->tune_pending = true;
   return QG_OK;
 }
 
@@ -1168,6 +1170,12 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
                    h->next_step + n_steps, h->T);
   if(bad_step) *bad_step = -1;
   QG_CUDA(cudaSetDevice(h->device));
+  if(h->tune_pending) {
+    // at any step: it only clobbers the far field and partials, which the
+    // run recomputes (far_block is invalidated)
+    h->tune_pending = false;
+    QG_TRY(autotune_far(h));
+  }
   const int t_start = h->next_step;
   h->eval_cached = -0x7fffffff;
   const size_t row = (size_t)h->n * 2;  // double2 per step
@@ -1737,6 +1745,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
     } else if(!std::strcmp(key, "far_variant")) {
       if(value < 0 || value > 6) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..6");
       h->far_variant = value;
+      h->tune_pending = false;  // an explicit choice is kept
     } else {
       if(value && !h->block_step_ok)
         return qg_fail(QG_ERR_UNSUPPORTED, "qg_set_option: block_step needs the fused form with all %d "
@@ -1765,6 +1774,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
                      h->next_step);
     if(value) {
       for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
+      h->tune_pending = false;
       QG_TRY(autotune_far(h));
       for(auto &g : h->graph)
         if(g) {

@@ -4,7 +4,8 @@ Requests (one ensemble each: dots, pulse, constants) arrive over time.  The
 service admits them first-come first-served while their device footprint
 (coefficient table + history rings + integrator state, qg_footprint) fits
 the memory budget, builds each admitted ensemble (qg_create: upload and table
-build), and adds it to the running batch at the next 16-step block.  Every
+build) on a worker thread while the batch keeps running, and adds it to the
+running batch at the first 16-step block after its build is done.  Every
 block advances all running ensembles in one persistent far-pair launch and
 16 step launches (qg_batch_run); ensembles that reach their last step are
 retired, their final state read back and their memory returned, which lets
@@ -18,6 +19,7 @@ process (src/main.cpp).
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import dataclasses
 import math
 import time
@@ -75,6 +77,11 @@ class Server:
         self.blocks_per_round = blocks_per_round
         self.batch = capi.Batch(capacity)
         self.running: dict[int, tuple[Request, capi.Simulation, float, int]] = {}
+        # builds in flight, in admission order: (request, future, admitted, footprint)
+        self.building: collections.deque = collections.deque()
+        self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+        import torch
+        self._device = torch.cuda.current_device()  # the worker builds on the caller's GPU
         self.used = 0.0
         self.results: list[Result] = []
         self.pair_updates_done = 0.0
@@ -82,12 +89,27 @@ class Server:
     def footprint(self, req: Request) -> int:
         return capi.footprint(req.n, req.constants, req.side(), precision=self.precision)
 
+    def _build(self, req: Request) -> capi.Simulation:
+        # runs on the worker thread: the library's calls release the GIL, its
+        # error state is per thread, and the new handle has a stream of its own
+        import torch
+        torch.cuda.set_device(self._device)
+        return capi.Simulation(req.dots, req.pulse, req.constants, weights=self.weights, precision=self.precision)
+
     def _admit(self, req: Request, now: float) -> None:
         fp = self.footprint(req)
-        sim = capi.Simulation(req.dots, req.pulse, req.constants, weights=self.weights, precision=self.precision)
-        self.batch.add(sim)
-        self.running[req.rid] = (req, sim, now, fp)
+        self.building.append((req, self._pool.submit(self._build, req), now, fp))
         self.used += fp
+
+    def _join_built(self, wait: bool) -> None:
+        """Moves finished builds (in admission order) into the batch; with
+        `wait`, blocks for the oldest one first."""
+        while self.building and (wait or self.building[0][1].done()):
+            req, fut, admitted, fp = self.building.popleft()
+            sim = fut.result()
+            self.batch.add(sim)
+            self.running[req.rid] = (req, sim, admitted, fp)
+            wait = False
 
     def _retire(self, rid: int, now: float) -> None:
         req, sim, admitted, fp = self.running.pop(rid)
@@ -108,16 +130,17 @@ class Server:
         queue: collections.deque[Request] = collections.deque()
         t0 = clock()
         busy = 0.0
-        while pending or queue or self.running:
+        while pending or queue or self.running or self.building:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
             # admit first-come first-served while memory and slots allow
-            while queue and len(self.running) < self.capacity:
+            while queue and len(self.running) + len(self.building) < self.capacity:
                 fp = self.footprint(queue[0])
-                if self.running and self.used + fp > self.budget:
+                if (self.running or self.building) and self.used + fp > self.budget:
                     break
                 self._admit(queue.popleft(), clock() - t0)
+            self._join_built(wait=not self.running and bool(self.building))
             if not self.running:
                 if pending:  # idle until the next arrival
                     time.sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.01)))
@@ -142,6 +165,10 @@ class Server:
         }
 
     def close(self) -> None:
+        while self.building:
+            _, fut, _, _ = self.building.popleft()
+            fut.result().close()
+        self._pool.shutdown(wait=True)
         for rid in list(self.running):
             _, sim, _, _ = self.running.pop(rid)
             sim.close()
