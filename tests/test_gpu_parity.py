@@ -295,6 +295,22 @@ def test_far_kernel_variants_agree_bitwise(golden_weights):
         np.testing.assert_array_equal(outs[0], outs[i])
 
 
+def test_far_autotuner_runs_at_the_first_run_and_keeps_an_explicit_choice(golden_weights):
+    """FP64 table handles of 512 dots or more time the far variants at their
+    first qg_run and keep the fastest; a variant set before that run is kept.
+    Either way the results are the same bits."""
+    wl = I.plain_table(seed=4, n=600, steps=64, pulse_delay=0.05)
+    outs = []
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        outs.append(sim.run(48))
+        assert sim.get_option("far_variant") in (0, 3, 5, 6)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+        sim.set_option("far_variant", 4)
+        outs.append(sim.run(48))
+        assert sim.get_option("far_variant") == 4
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
 def line_of_dots(n, spacing, seed=5):
     """n dots on a line along x, `spacing` apart (c dt = 1e-3): neighbours at
     floor delay 1, none at delay 0, so the groups coupled at delay <= 1 are
