@@ -263,8 +263,8 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "autotune" (1 = time the far-kernel variants again now; at a block
  *   boundary between runs),
  * "far_group" (source tiles each far-kernel warp sums before writing its
- *   partial, table handles; default 4; changes the summation grouping, so
- *   results change in the last bits),
+ *   partial, table handles; default 4, mixed precision 2 below 256 tiles;
+ *   changes the summation grouping, so results change in the last bits),
  * "block_step" (1 = the K steps of a block in one cooperative launch, the
  *   default where every 32-dot block fits on the device at once; 0 = one
  *   launch per step; same results),
