@@ -368,9 +368,10 @@ static size_t table_bytes(int nT, int q, bool mixed)
   return (size_t)nT * nT * kTilePairs * per;
 }
 
-// Even, so every ring row starts 32-byte aligned for paired-sample loads.
+// Source tiles per far-kernel warp (see create_impl).
 static int far_group(bool mixed, int nT) { return mixed && nT < 256 ? 2 : kTileGroup; }
 
+// Even, so every ring row starts 32-byte aligned for paired-sample loads.
 static int ring_depth(int max_delay, int q)
 {
   const int w = max_delay + q + kTimeBlock + 2;
