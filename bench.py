@@ -349,6 +349,7 @@ def run_ours(args, world, rank, local):
     # ---- device-resident throughput (value) and the sweep kernel's roofline
     nonfinite = None
     prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    mixed_prec = args.precision == "mixed"
     otf = args.workload == "otf"
     cmode = capi.COEF_ON_THE_FLY if otf else capi.COEF_TABLE
     sim = capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec, coef_mode=cmode)
@@ -377,7 +378,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ms = e0.elapsed_time(e1)
     pair_ms, launches, step_ms, step_launches = sim.kernel_times()
-    variant = sim.get_option("far_variant")
+    variant = sim.get_option("far_variant") if not (mixed_prec or otf) else None  # FP64 table only
     sim.close()
     ms_max = max_over_ranks(ms, world)
     value = job_throughput(world, n, args.steps, ms_max)
@@ -416,7 +417,8 @@ def run_ours(args, world, rank, local):
     fp64_tf = flops / (avg_ms / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops("float32" if mixed else "float64")
     # ncu dram read + write per launch of the same kernel on the same workload
-    kname, prof = ("far_kernel_mixed<5,false>", "far_kernel_mixed_N4096") if mixed else FAR_VARIANTS[variant]
+    kname, prof = (("far_kernel_mixed<5,false>", "far_kernel_mixed_N4096") if mixed else
+                   FAR_VARIANTS[variant] if variant is not None else (None, None))
     traffic = profile_traffic(prof) if prof else None
     if otf:
         # compute-bound: every ordered pair's coefficients once per launch
