@@ -81,7 +81,8 @@ class Server:
         self.building: collections.deque = collections.deque()
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=1)
         import torch
-        self._device = torch.cuda.current_device()  # the worker builds on the caller's GPU
+        # the worker builds on the caller's GPU
+        self._device = torch.cuda.current_device() if torch.cuda.is_available() else None
         self.used = 0.0
         self.results: list[Result] = []
         self.pair_updates_done = 0.0
@@ -92,8 +93,9 @@ class Server:
     def _build(self, req: Request) -> capi.Simulation:
         # runs on the worker thread: the library's calls release the GIL, its
         # error state is per thread, and the new handle has a stream of its own
-        import torch
-        torch.cuda.set_device(self._device)
+        if self._device is not None:
+            import torch
+            torch.cuda.set_device(self._device)
         return capi.Simulation(req.dots, req.pulse, req.constants, weights=self.weights, precision=self.precision)
 
     def _admit(self, req: Request, now: float) -> None:
