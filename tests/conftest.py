@@ -20,6 +20,9 @@ def pytest_configure(config):
 def _ensure_built():
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libquest_ref.so")):
+        # the reference's own sources, where a checkout exists (skipped otherwise)
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False)
     if not (os.path.exists(os.path.join(ROOT, "quest_b200", "libquest_gpu.so")) and
             os.path.exists(os.path.join(ROOT, "quest_b200", "quest-gpu"))):
         subprocess.run(["make", "-s", "-j4", "-C", os.path.join(ROOT, "quest_b200", "csrc")], check=True)
