@@ -355,6 +355,18 @@ def cpu_baseline(args, n: int, steps: int):
                       f"on a synthetic history, {dt:.2f} s; table build not timed"}
 
 
+def workload(args, rank: int, total: int) -> I.Workload:
+    """This rank's ensemble (seed + rank: every rank its own) for a run of
+    `total` steps."""
+    if args.workload == "otf":
+        wl = I.mixed_large(seed=3 + rank, n=args.n, steps=max(5000, total), pulse_delay=args.pulse_delay)
+    else:
+        wl = I.plain_table(seed=2 + rank, n=args.n, steps=total, pulse_delay=args.pulse_delay)
+    if args.dipole_scale != 1.0:
+        wl.dots[:, 6:9] *= args.dipole_scale
+    return wl
+
+
 def main_window(args) -> tuple[int, int]:
     """The main line's aligned (warm-up, timed) steps; with no --steps the
     table workload times the rest of its 20000-step run."""
@@ -502,15 +514,9 @@ def run_ours(args, world, rank, local):
     otf = args.workload == "otf"
     mixed = args.precision == "mixed"
     n = args.n
-    side = 0.5 if otf else 0.2
     warm, timed = main_window(args)
     total = warm + timed
-    if otf:
-        wl = I.mixed_large(seed=3 + rank, n=n, steps=max(5000, total), side=side, pulse_delay=args.pulse_delay)
-    else:
-        wl = I.plain_table(seed=2 + rank, n=n, steps=total, pulse_delay=args.pulse_delay)
-    if args.dipole_scale != 1.0:
-        wl.dots[:, 6:9] *= args.dipole_scale
+    wl = workload(args, rank, total)
     weights = load_weights()
     prec = capi.PREC_MIXED if mixed else capi.PREC_FP64
     cmode = capi.COEF_ON_THE_FLY if otf else capi.COEF_TABLE

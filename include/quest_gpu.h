@@ -154,7 +154,11 @@ qg_status qg_history_evaluate(qg_handle *h, int step, const double *rho01_step,
  * `step` (the handle's device history, like qg_history_evaluate);
  * d_field_out receives N complex, user order.  Work is enqueued on `stream`
  * (a cudaStream_t; NULL = the handle's stream) and the call returns without
- * waiting; the result is ready when that stream reaches this point.
+ * waiting; the result is ready when that stream reaches this point.  The
+ * call reads and writes the handle's device history: a non-NULL stream must
+ * already be ordered after any work still pending on the handle's stream
+ * (qg_stream; qg_run, qg_history_evaluate and qg_set_history finish theirs
+ * before they return), and the handle's own calls must not overlap it.
  *
  * The call allocates nothing and copies nothing to or from the host: its
  * scratch is a fixed 2.2 MB array in the library's device memory, held on
@@ -188,7 +192,10 @@ qg_status qg_get_history(qg_handle *h, int t0, int n, double *rho01_out);
  * user order. */
 qg_status qg_get_state(qg_handle *h, double *rho_out);
 
-/* First step at which a non-finite value appeared, or -1. */
+/* First step at which a non-finite value appeared, or -1.  For a batch
+ * member it is the value the batch's last qg_batch_run read (one gathered
+ * copy for all members), so a caller can retire a failed member after every
+ * batch run without a device round trip per member. */
 qg_status qg_bad_step(qg_handle *h, int *bad_step);
 
 /* Checkpoint / resume (no reference counterpart; the reference keeps the
@@ -268,12 +275,20 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "block_step" (1 = the K steps of a block in one cooperative launch, the
  *   default where every 32-dot block fits on the device at once; 0 = one
  *   launch per step; same results),
+ * "wait_limit" (polls the step-block kernel makes on a partner block's step
+ *   count before it gives up; 0 = the default, about a second.  A wait that
+ *   runs out ends the launch: qg_run returns QG_ERR_CUDA "timed out" and the
+ *   handle needs "reset" or a checkpoint load before it runs again),
+ * "test_skip_post" (failure-detection tests only: the index of a 32-dot block
+ *   that never posts its finished steps, so that its partners' waits run
+ *   out; -1 = none, the default),
  * "reset" (restart the history at step 0, main.cpp:30-36). */
 qg_status qg_set_option(qg_handle *h, const char *key, int value);
 
 /* Reads an option back: "graph", "profile", "far_variant" (the variant in
  * use, which after qg_create is the autotuner's choice), "block_step",
- * "far_group".  No reference counterpart (the reference has no options). */
+ * "far_group", "wait_limit", "test_skip_post".  No reference counterpart (the
+ * reference has no options). */
 qg_status qg_get_option(const qg_handle *h, const char *key, int *value);
 
 #ifdef __cplusplus

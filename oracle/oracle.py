@@ -60,6 +60,9 @@ def lib():
                                         ctypes.POINTER(OrWeights), ctypes.c_int, ip, dp, dp,
                                         ctypes.c_int, ctypes.c_int]
         L.or_faithful_steps.restype = ctypes.c_int
+        L.or_history_evaluate_targets.argtypes = [dp, ctypes.c_int, ctypes.POINTER(OrParams), dp, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ip, ctypes.c_int, dp]
+        L.or_history_evaluate_targets.restype = ctypes.c_int
         L.or_coord2idx.argtypes = [ctypes.c_int, ctypes.c_int]
         L.or_coord2idx.restype = ctypes.c_longlong
         L.or_idx2coord.argtypes = [ctypes.c_longlong, ip, ip]
@@ -127,6 +130,23 @@ def history_evaluate(dots, c, delays, coefs, hist, step) -> np.ndarray:
     h = np.ascontiguousarray(hist).view(np.float64).reshape(-1)
     lib().or_history_evaluate(n, ctypes.byref(p), _ip(np.ascontiguousarray(delays, dtype=np.int32)),
                               _dp(cf), _dp(h), WINDOW, T, step, _dp(out))
+    return out.view(np.complex128)
+
+
+def history_evaluate_targets(dots, c, rho01: np.ndarray, t_lo: int, step: int, targets) -> np.ndarray:
+    """HistoryInteraction::evaluate(step) for the given target dots only,
+    coefficients on the fly (O(N) per target).  rho01: complex (N, nt) for
+    steps t_lo .. t_lo + nt - 1."""
+    n = dots.shape[0]
+    tg = np.ascontiguousarray(targets, dtype=np.int32)
+    r = np.ascontiguousarray(rho01, dtype=np.complex128)
+    out = np.zeros(2 * tg.size)
+    p = params(c)
+    rc = lib().or_history_evaluate_targets(_dp(np.ascontiguousarray(dots)), n, ctypes.byref(p),
+                                           _dp(r.view(np.float64).reshape(-1)), t_lo, r.shape[1], step, _ip(tg),
+                                           tg.size, _dp(out))
+    if rc != 0:
+        raise ValueError("the rho01 window does not cover every tap the targets read")
     return out.view(np.complex128)
 
 

@@ -256,6 +256,48 @@ void or_history_evaluate(int n, const or_params *p, const int *delays,
   }
 }
 
+/* history_interaction.cpp:47-70 for selected target dots only, each pair's
+ * coefficients computed on the fly in the table's orientation (src = the
+ * larger index, obs = the smaller, history_interaction.cpp:29-43), so the
+ * cost is O(N) per target.  rho01: [dot][t - t_lo] complex for steps
+ * t_lo .. t_lo + nt - 1, which must cover every tap read (returns -1 with
+ * out untouched for the offending target otherwise).  out: one complex per
+ * target. */
+int or_history_evaluate_targets(const or_dot *dots, int n, const or_params *p, const double *rho01, int t_lo,
+                                int nt, int step, const int *targets, int ntargets, double *out)
+{
+  const int q = p->interpolation_order;
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+  for(int k = 0; k < ntargets; ++k) {
+    const int a = targets[k];
+    cx acc = {0.0, 0.0};
+    double coef[2 * 16];
+    for(int b = 0; b < n && !bad; ++b) {
+      if(b == a) continue;
+      const int src = a > b ? a : b, obs = a > b ? b : a;
+      int d;
+      or_pair_coefficients(&dots[src], &dots[obs], p, &d, coef);
+      const int s = step - d;
+      for(int i = 0; i <= q; ++i) {
+        const int t = s - i;
+        if(t < -WINDOW) continue;
+        if(t < t_lo || t >= t_lo + nt) {
+          bad = 1;
+          break;
+        }
+        const double *z = rho01 + 2 * ((size_t)b * nt + (size_t)(t - t_lo));
+        const cx pr = p->frame == 0 ? (cx){z[0], z[1]} : (cx){2 * z[0], 0.0};
+        const cx c = {coef[2 * i], coef[2 * i + 1]};
+        acc = cadd(acc, cmul(pr, c));
+      }
+    }
+    out[2 * k] = acc.re;
+    out[2 * k + 1] = acc.im;
+  }
+  return bad ? -1 : 0;
+}
+
 /* ---- pulse_interaction.cpp:9-20, pulse.cpp:15-20, math_utils.cpp:27-30 */
 static inline double gaussian(double t) { return exp(-pow(t, 2) / 2); }
 

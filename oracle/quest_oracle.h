@@ -97,6 +97,11 @@ void or_history_evaluate(int n, const or_params *p, const int *delays,
 
 /* PulseInteraction::evaluate (src/interactions/pulse_interaction.cpp:9-20,
  * src/pulse.cpp:15-20, src/math_utils.cpp:27-30). out: 2*N doubles. */
+/* history_interaction.cpp:47-70 for a few target dots, coefficients on the
+ * fly (O(N) per target); rho01 [dot][t - t_lo] complex, nt steps. */
+int or_history_evaluate_targets(const or_dot *dots, int n, const or_params *p, const double *rho01, int t_lo,
+                                int nt, int step, const int *targets, int ntargets, double *out);
+
 void or_pulse_evaluate(const or_dot *dots, int n, const or_pulse *pulse,
                        const or_params *p, int step, double *out);
 

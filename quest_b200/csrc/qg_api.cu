@@ -123,6 +123,12 @@ struct qg_handle_s {
   float tuned_far_ms = 0;  // far-kernel time of the autotuner's choice
   bool tune_pending = false;  // the far-kernel autotuner runs at the first qg_run
   bool profile = false;
+  // first bad step as the last batch run read it (qg_bad_step answers from it
+  // without a device copy while valid; any other run invalidates it)
+  int batch_bad = kBadNone;
+  bool batch_bad_valid = false;
+  int spin_limit = 0;       // step-block kernel polls per wait (0: its default, about a second)
+  int skip_post = -1;       // failure-detection tests: a block that never posts its steps
   cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
   bool events_ready = false;
   double pair_ms = 0, step_ms = 0;
@@ -224,6 +230,8 @@ struct qg_handle_s {
     a.traj_t0 = d_ints + 3;
     a.d_next = d_ints + 0;
     a.d_bad = d_ints + 2;
+    a.spin_limit = spin_limit;
+    a.skip_post_block = skip_post;
     a.w = w;
     return a;
   }
@@ -588,6 +596,7 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
 
 static qg_status reset_state(qg_handle *h)
 {
+  h->batch_bad_valid = false;
   QG_CUDA(cudaMemsetAsync(h->d_ring, 0, sizeof(double2) * (size_t)h->n_pad * h->stride, h->stream));
   if(h->mixed) {
     QG_CUDA(cudaMemsetAsync(h->d_ring32w, 0, sizeof(float2) * (size_t)h->n_pad * h->stride, h->stream));
@@ -1170,6 +1179,7 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
     return qg_fail(QG_ERR_INVALID_ARG, "qg_run: steps [%d, %d) exceed num_timesteps %d", h->next_step,
                    h->next_step + n_steps, h->T);
   if(bad_step) *bad_step = -1;
+  h->batch_bad_valid = false;
   QG_CUDA(cudaSetDevice(h->device));
   if(h->tune_pending) {
     // at any step: it only clobbers the far field and partials, which the
@@ -1241,6 +1251,8 @@ struct qg_batch_s {
   int far_grid = 0;
   bool dirty = true;
   cudaGraphExec_t graph = nullptr;
+  int *d_bad_all = nullptr;  // members' first bad steps, gathered after each run
+  int *h_bad_all = nullptr;  // pinned copy
 };
 
 extern "C" qg_status qg_batch_create(int capacity, qg_batch **out)
@@ -1250,6 +1262,8 @@ extern "C" qg_status qg_batch_create(int capacity, qg_batch **out)
   qg_batch *b = new qg_batch();
   b->capacity = capacity;
   auto fail = [&](qg_status st) {
+    if(b->d_bad_all) cudaFree(b->d_bad_all);
+    if(b->h_bad_all) cudaFreeHost(b->h_bad_all);
     if(b->d_far) cudaFree(b->d_far);
     if(b->d_step) cudaFree(b->d_step);
     if(b->d_task_off) cudaFree(b->d_task_off);
@@ -1264,7 +1278,9 @@ extern "C" qg_status qg_batch_create(int capacity, qg_batch **out)
      (e = cudaMalloc(&b->d_far, sizeof(FarArgs) * capacity)) != cudaSuccess ||
      (e = cudaMalloc(&b->d_step, sizeof(StepArgs) * capacity)) != cudaSuccess ||
      (e = cudaMalloc(&b->d_task_off, sizeof(int) * (capacity + 1))) != cudaSuccess ||
-     (e = cudaMalloc(&b->d_block_off, sizeof(int) * (capacity + 1))) != cudaSuccess)
+     (e = cudaMalloc(&b->d_block_off, sizeof(int) * (capacity + 1))) != cudaSuccess ||
+     (e = cudaMalloc(&b->d_bad_all, sizeof(int) * capacity)) != cudaSuccess ||
+     (e = cudaMallocHost(&b->h_bad_all, sizeof(int) * capacity)) != cudaSuccess)
     return fail(qg_fail(e == cudaErrorMemoryAllocation ? QG_ERR_OOM : QG_ERR_CUDA, "qg_batch_create: %s",
                         cudaGetErrorString(e)));
   int sms = 0, per_sm = 0;
@@ -1284,6 +1300,8 @@ extern "C" qg_status qg_batch_destroy(qg_batch *b)
   cudaFree(b->d_step);
   cudaFree(b->d_task_off);
   cudaFree(b->d_block_off);
+  cudaFree(b->d_bad_all);
+  cudaFreeHost(b->h_bad_all);
   cudaStreamDestroy(b->stream);
   delete b;
   return QG_OK;
@@ -1380,13 +1398,21 @@ extern "C" qg_status qg_batch_run(qg_batch *b, int n_blocks)
   if(b->dirty) QG_TRY(batch_rebuild(b));
   if(b->members.empty()) return QG_OK;
   for(int i = 0; i < n_blocks; ++i) QG_CUDA(cudaGraphLaunch(b->graph, b->stream));
+  // every member's first bad step in one copy, so a caller can retire a
+  // member that went non-finite without a device round trip per member
+  const int nm = (int)b->members.size();
+  launch_gather_bad(b->d_step, nm, b->d_bad_all, b->stream);
+  QG_CUDA(cudaMemcpyAsync(b->h_bad_all, b->d_bad_all, sizeof(int) * nm, cudaMemcpyDeviceToHost, b->stream));
   QG_CUDA(cudaStreamSynchronize(b->stream));
   QG_CUDA(cudaGetLastError());
-  for(qg_handle *h : b->members) {
+  for(int e = 0; e < nm; ++e) {
+    qg_handle *h = b->members[e];
     const int start = h->next_step;
     h->next_step = std::min(h->T, start + n_blocks * kTimeBlock);
     h->far_block = start + (n_blocks - 1) * kTimeBlock;
     h->eval_cached = -0x7fffffff;
+    h->batch_bad = b->h_bad_all[e];
+    h->batch_bad_valid = true;
   }
   return QG_OK;
 }
@@ -1403,9 +1429,13 @@ extern "C" qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, 
 extern "C" qg_status qg_bad_step(qg_handle *h, int *bad_step)
 {
   if(!h || !bad_step) return qg_fail(QG_ERR_INVALID_ARG, "qg_bad_step: NULL argument");
-  QG_CUDA(cudaSetDevice(h->device));
   int bad = kBadNone;
-  QG_CUDA(cudaMemcpy(&bad, h->d_ints + 2, sizeof(int), cudaMemcpyDeviceToHost));
+  if(h->batch_bad_valid) {
+    bad = h->batch_bad;
+  } else {
+    QG_CUDA(cudaSetDevice(h->device));
+    QG_CUDA(cudaMemcpy(&bad, h->d_ints + 2, sizeof(int), cudaMemcpyDeviceToHost));
+  }
   *bad_step = bad == kBadNone ? -1 : bad;
   return QG_OK;
 }
@@ -1514,6 +1544,7 @@ extern "C" qg_status qg_checkpoint_load(qg_handle *h, const void *buf, size_t by
     return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: step %d outside [0, %d]", hd.next_step, hd.T);
   const size_t need = sizeof hd + hd.ring_bytes + 2 * hd.ring32_bytes + hd.pcr_bytes;
   if(bytes < need) return qg_fail(QG_ERR_INVALID_ARG, "qg_checkpoint_load: buffer of %zu bytes, need %zu", bytes, need);
+  h->batch_bad_valid = false;
   QG_CUDA(cudaSetDevice(h->device));
   for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
   const char *p = static_cast<const char *>(buf) + sizeof hd;
@@ -1649,6 +1680,9 @@ extern "C" qg_status qg_set_history(qg_handle *h, int t0, int n, const double *r
   }
   launch_ring32_rebuild(a, h->stream);
   QG_CUDA(cudaGetLastError());
+  // the history is complete when the call returns, so work the caller
+  // enqueues on another stream (qg_history_evaluate_noalloc) sees all of it
+  QG_CUDA(cudaStreamSynchronize(h->stream));
   h->eval_cached = -0x7fffffff;
   h->far_block = -0x7fffffff;
   return QG_OK;
@@ -1736,8 +1770,16 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
     if(value) QG_TRY(ensure_events(h));
     h->profile = value != 0;
   } else if(!std::strcmp(key, "far_variant") || !std::strcmp(key, "block_step") ||
-            !std::strcmp(key, "far_group")) {
-    if(!std::strcmp(key, "far_group")) {
+            !std::strcmp(key, "far_group") || !std::strcmp(key, "wait_limit") ||
+            !std::strcmp(key, "test_skip_post")) {
+    if(!std::strcmp(key, "wait_limit")) {
+      if(value < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: wait_limit >= 0 (0: the default)");
+      h->spin_limit = value;
+    } else if(!std::strcmp(key, "test_skip_post")) {
+      if(value < -1 || value >= std::max(h->step_blocks, 1))
+        return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: test_skip_post in -1 .. %d", h->step_blocks - 1);
+      h->skip_post = value;
+    } else if(!std::strcmp(key, "far_group")) {
       if(h->otf || value < 1 || (h->nT + value - 1) / value > h->max_groups)
         return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_group %d not available (table handles, "
                        "at least %d)", value, (h->nT + h->max_groups - 1) / std::max(h->max_groups, 1));
@@ -1808,6 +1850,10 @@ extern "C" qg_status qg_get_option(const qg_handle *h, const char *key, int *val
     *value = h->block_step ? 1 : 0;
   else if(!std::strcmp(key, "far_group"))
     *value = h->group;
+  else if(!std::strcmp(key, "wait_limit"))
+    *value = h->spin_limit;
+  else if(!std::strcmp(key, "test_skip_post"))
+    *value = h->skip_post;
   else
     return qg_fail(QG_ERR_INVALID_ARG, "qg_get_option: unknown key '%s'", key);
   return QG_OK;

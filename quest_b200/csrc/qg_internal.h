@@ -145,6 +145,11 @@ struct StepArgs {
   int *d_next;           // first step of the next far block (set by the last
                          // step kernel of a block, read by the far kernel)
   int *d_bad;
+  // step-block kernel: polls per wait on a partner block before it gives up
+  // (0: the default, about a second), and a block that never posts its steps
+  // (-1: none; set only by failure-detection tests, so that waits run out)
+  int spin_limit;
+  int skip_post_block;
   PCW w;
 };
 
@@ -167,6 +172,8 @@ void launch_far_step1(const FarArgs &a, void *stream);
 void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
                       int grid, void *stream);
 void launch_ring32_rebuild(const StepArgs &a, void *stream);
+// out[e] = *args[e].d_bad for the n members of a batch
+void launch_gather_bad(const StepArgs *args, int n, int *out, void *stream);
 // The step-block kernel's per-block step counts, one per 128-byte line (so
 // the polls on one block's count do not queue behind those on another's).
 constexpr int kFlagStride = 32;

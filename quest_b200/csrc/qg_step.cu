@@ -652,16 +652,18 @@ __device__ __forceinline__ void post_step(unsigned *p)
 }
 
 // Called by a whole warp: waits until flags[list[i] * kFlagStride] >= target
-// for every i < n (the lanes poll in parallel, each wait bounded).  False if
-// a wait ran out.
-__device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *list, int n, unsigned target)
+// for every i < n (the lanes poll in parallel, each wait bounded by `limit`
+// polls, kBarrierSpins when 0).  False if a wait ran out.
+__device__ __forceinline__ bool wait_blocks(const unsigned *flags, const int *list, int n, unsigned target,
+                                            int limit)
 {
   bool ok = true;
+  const int max_spins = limit > 0 ? limit : kBarrierSpins;
   for(int i = threadIdx.x & 31; i < n && ok; i += 32) {
     const unsigned *f = flags + (long long)__ldg(list + i) * kFlagStride;
     int spins = 0;
     while(ld_acquire(f) < target) {
-      if(++spins > kBarrierSpins) {
+      if(++spins > max_spins) {
         ok = false;
         break;
       }
@@ -942,7 +944,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
     const int buf = k & 1;
     if(part == 0) {
       bool ok = true;
-      if(!a.lag && k > k0) ok = wait_blocks(flags, a.pb_idx + B0, NB, k - k0);  // partners' step t-1
+      if(!a.lag && k > k0) ok = wait_blocks(flags, a.pb_idx + B0, NB, k - k0, a.spin_limit);  // partners' step t-1
       if(ok) {
         double2 P[2], H[2], r[2], dr[2], past = make_double2(0.0, 0.0);
         double pul = 0;
@@ -972,7 +974,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
         // rho01 first, then post the step, then the rest of the state
         if(live) finish_ring(a, idx, t, r);
         __syncwarp();
-        if(lane == 0) post_step(flags + (long long)blk * kFlagStride);
+        if(lane == 0 && blk != a.skip_post_block) post_step(flags + (long long)blk * kFlagStride);
         if(live) {
           finish_state(a, idx, t, r, dr);
           const int sl = pc_slot(t);
@@ -990,7 +992,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps, 2) step_block_kernel(StepArg
       }
     } else if(helper && k + 1 < k1 && t + 1 < a.T) {
       // step k+1's sums; M_old needs the partner blocks' step k-1
-      if(hw == 0 && k > k0 && !wait_blocks(flags, a.pb_idx + B0, NB, k - k0) && lane == 0) {
+      if(hw == 0 && k > k0 && !wait_blocks(flags, a.pb_idx + B0, NB, k - k0, a.spin_limit) && lane == 0) {
         s_abort = 1;
         atomicMin(a.d_bad, -2);
       }
@@ -1173,6 +1175,17 @@ __global__ void init_state_kernel(StepArgs a)
   base[a.n_pad] = make_double2(0.0, 0.0);
   base[2 * a.n_pad] = make_double2(0.0, 0.0);
   base[3 * a.n_pad] = make_double2(0.0, 0.0);
+}
+
+__global__ void gather_bad_kernel(const StepArgs *args, int n, int *out)
+{
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if(e < n) out[e] = *args[e].d_bad;
+}
+
+void launch_gather_bad(const StepArgs *args, int n, int *out, void *stream)
+{
+  if(n > 0) gather_bad_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(args, n, out);
 }
 
 void launch_init_state(const StepArgs &a, void *stream)

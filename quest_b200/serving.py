@@ -9,7 +9,10 @@ running batch at the first 16-step block after its build is done.  Every
 block advances all running ensembles in one persistent far-pair launch and
 16 step launches (qg_batch_run); ensembles that reach their last step are
 retired, their final state read back and their memory returned, which lets
-waiting requests in.  Results do not depend on what else is running: a
+waiting requests in.  An ensemble whose state goes non-finite is retired at
+the first batch run that sees it, with that first bad step as its error (the
+reference stops a run there with std::domain_error, integrator.cpp:200-207);
+the other ensembles go on unchanged.  Results do not depend on what else is running: a
 batch member is advanced by the same kernels, in the same order, as it
 would be alone.
 
@@ -61,6 +64,11 @@ class Result:
     finished: float
     state: np.ndarray             # (N, 2) complex: rho00, rho01 after the last step
     bad_step: int                 # first non-finite step, -1 if none
+    steps_done: int = 0           # steps computed (num_timesteps unless it failed earlier)
+
+    @property
+    def failed(self) -> bool:
+        return self.bad_step >= 0
 
     @property
     def latency(self) -> float:
@@ -117,12 +125,13 @@ class Server:
         req, sim, admitted, fp = self.running.pop(rid)
         state = sim.state()
         bad = sim.bad_step()
+        done = sim.next_step
         self.batch.remove(sim)
         sim.close()
         self.used -= fp
-        self.pair_updates_done += req.pair_updates
+        self.pair_updates_done += float(req.n) ** 2 * done
         self.results.append(Result(req.rid, req.n, req.constants.num_timesteps, req.arrival, admitted, now,
-                                   state, bad))
+                                   state, bad, done))
 
     def serve(self, requests: list[Request], clock=time.perf_counter) -> dict:
         """Runs until every request is finished.  Arrival times are seconds
@@ -151,13 +160,16 @@ class Server:
             self.batch.run(self.blocks_per_round)
             busy += clock() - b0
             now = clock() - t0
+            # finished, or non-finite (the batch run gathered every member's
+            # first bad step, so bad_step() costs no device round trip)
             for rid in [r for r, (req, sim, _, _) in self.running.items()
-                        if sim.next_step >= req.constants.num_timesteps]:
+                        if sim.next_step >= req.constants.num_timesteps or sim.bad_step() >= 0]:
                 self._retire(rid, now)
         wall = clock() - t0
         lat = np.array([r.latency for r in self.results])
         return {
             "requests": len(self.results),
+            "failed": sum(1 for r in self.results if r.failed),
             "wall_s": wall,
             "busy_s": busy,
             "pair_updates": self.pair_updates_done,

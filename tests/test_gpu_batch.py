@@ -73,3 +73,36 @@ def test_batch_rejects_mismatched_members(golden_weights):
     with pytest.raises(capi.QuestError):
         batch.add(sc)  # not on a 16-step boundary
     batch.close()
+
+
+def test_member_going_nonfinite_is_reported_and_the_others_are_unchanged(golden_weights):
+    """The N = 200 workload with the pulse at delay 0.5 and dipoles 2e-3
+    overflows (the reference's domain_error) near step 800; in a batch its
+    first bad step is the one it has alone, read after every batch run, and
+    the stable members beside it are bitwise their solo runs."""
+    bad_wl = I.plain_small(n=200, steps=880, pulse_delay=0.5)
+    with capi.Simulation(bad_wl.dots, bad_wl.pulse, bad_wl.constants, weights=golden_weights) as sim:
+        with pytest.raises(capi.NonFiniteError) as e:
+            sim.run(880, record=False)
+    solo_bad = e.value.step
+    assert 700 < solo_bad < 880
+    good = [ensemble(21, 150, 0.1, 880, 10.0), ensemble(22, 300, 0.15, 880, 25.0)]
+    batch = capi.Batch(4)
+    sims = [capi.Simulation(bad_wl.dots, bad_wl.pulse, bad_wl.constants, weights=golden_weights)]
+    sims += [capi.Simulation(d, p, c, weights=golden_weights) for d, p, c in good]
+    for s in sims:
+        batch.add(s)
+    seen = None
+    for blk in range(880 // 16):
+        batch.run(1)
+        if seen is None and sims[0].bad_step() >= 0:
+            seen = (blk, sims[0].bad_step())
+    assert seen is not None and seen[1] == solo_bad
+    assert seen[0] == solo_bad // 16  # visible after the block that holds it
+    for (d, p, c), sim in zip(good, sims[1:]):
+        ref, bad = solo(d, p, c, golden_weights, 880)
+        np.testing.assert_array_equal(sim.state(), ref)
+        assert sim.bad_step() == bad == -1
+    for s in sims:
+        batch.remove(s)
+        s.close()

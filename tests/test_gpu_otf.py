@@ -167,3 +167,31 @@ def test_otf_n65536_blocks(golden_weights):
             sim.run(32, record=False)
             st = sim.state()
             assert np.all(np.isfinite(st))
+
+
+def test_otf_n65536_evaluate_sampled_targets_against_oracle(golden_weights):
+    """cfg 3 at full size (N = 65536 in the 0.5 cube, delays up to ~866
+    steps): HistoryInteraction::evaluate (history_interaction.cpp:47-70)
+    through qg_history_evaluate with on-the-fly FP64 coefficients, on a
+    random rho01 history covering every tap read, against the oracle's
+    per-target sum (coefficients on the fly in the reference's pair
+    orientation, O(N) per target) for 64 sampled targets."""
+    wl = I.mixed_large(n=65536, steps=5000)
+    n = wl.n
+    rng = np.random.default_rng(65536)
+    with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights, precision=capi.PREC_FP64,
+                         coef_mode=capi.COEF_ON_THE_FLY) as sim:
+        info = sim.info()
+        W = info["ring_depth"]
+        step = 1000
+        t_lo = step - W + 1
+        assert t_lo <= step - info["max_delay"] - 5
+        # (steps, N) for qg_set_history, complex64 draws widened to keep the host copy small
+        hist = (rng.standard_normal((W, n), dtype=np.float32) +
+                1j * rng.standard_normal((W, n), dtype=np.float32)).astype(np.complex128)
+        sim.set_history(t_lo, hist)
+        got = sim.history_evaluate(step)
+    targets = np.sort(rng.choice(n, size=64, replace=False))
+    ref = O.history_evaluate_targets(wl.dots, wl.constants, np.ascontiguousarray(hist.T), t_lo, step, targets)
+    assert np.all(np.abs(ref) > 0)
+    assert rel_err(ref, got[targets]) <= 1e-12

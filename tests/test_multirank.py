@@ -17,17 +17,17 @@ import json, os, sys
 sys.path.insert(0, os.environ["QG_ROOT"])
 import argparse
 import bench
-args = argparse.Namespace(workload="table", n=64, steps=10, warmup=3, pulse_delay=5.0, dipole_scale=1.0,
-                          precision="fp64")
+args = bench.parse_args(["--n", "64", "--steps", "10", "--warmup", "3"])
 world, rank, local = bench.dist_setup(args, backend="gloo")
-wl = bench.workload(args, rank)
+warm, timed = bench.main_window(args)
+wl = bench.workload(args, rank, warm + timed)
 ms = 10.0 + 5.0 * rank            # this rank's (pretend) device time
 ms_max = bench.max_over_ranks(ms, world)
 bench.barrier(world)
-value = bench.job_throughput(world, wl.n, args.steps, ms_max)
+value = bench.job_throughput(world, wl.n, timed, ms_max)
 out = {"rank": rank, "world": world, "ms_max": ms_max, "value": value,
        "first_dot": [float(x) for x in wl.dots[0, :3]],
-       "parallelism": bench.config_dict(args)["parallelism"]}
+       "timed": timed, "parallelism": bench.config_dict(args, warm, timed)["parallelism"]}
 import torch.distributed as dist
 dist.destroy_process_group()
 print(json.dumps(out))
@@ -58,6 +58,7 @@ def test_two_gloo_ranks():
     a, b = sorted(outs, key=lambda d: d["rank"])
     assert a["world"] == b["world"] == 2
     assert a["ms_max"] == b["ms_max"] == 15.0          # the slower rank
-    assert a["value"] == b["value"] == pytest.approx(2 * 64 * 64 * 10 / 0.015)
+    assert a["timed"] == b["timed"] == 16                # whole 16-step blocks
+    assert a["value"] == b["value"] == pytest.approx(2 * 64 * 64 * 16 / 0.015)
     assert a["first_dot"] != b["first_dot"]            # each rank its own ensemble
     assert a["parallelism"] == "independent ensemble per GPU"

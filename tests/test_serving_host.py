@@ -21,13 +21,15 @@ class FakeSim:
         self.next_step = 0
         self.closed = False
         self.thread = threading.current_thread().name
+        # a dot with T1 = 0 makes the state non-finite at step 0, as on the GPU
+        self.fails_at = 0 if np.any(dots[:, 4] == 0) else None
         time.sleep(0.01)  # a build takes a while
 
     def state(self):
         return np.zeros((self.n, 2), dtype=np.complex128)
 
     def bad_step(self):
-        return -1
+        return self.fails_at if (self.fails_at is not None and self.next_step > self.fails_at) else -1
 
     def close(self):
         self.closed = True
@@ -113,3 +115,14 @@ def test_a_request_larger_than_the_budget_runs_alone(monkeypatch):
     stats, batch, _ = run_server(monkeypatch, reqs, budget=5, footprint=lambda n: 10)
     assert stats["requests"] == 3
     assert batch.max_members == 1
+
+
+def test_a_member_that_goes_nonfinite_is_retired_at_once(monkeypatch):
+    reqs = make_requests([40, 50, 60], [320, 320, 320], gap=0.0)
+    reqs[1].dots[3, 4] = 0.0  # T1 = 0
+    stats, batch, results = run_server(monkeypatch, reqs, budget=1e12, footprint=lambda n: n)
+    by = {r.rid: r for r in results}
+    assert stats["requests"] == 3 and stats["failed"] == 1
+    assert by[1].failed and by[1].bad_step == 0 and by[1].steps_done == 16  # retired after its first block
+    assert not by[0].failed and by[0].steps_done == 320 and by[2].steps_done == 320
+    assert stats["pair_updates"] == 40 ** 2 * 320 + 50 ** 2 * 16 + 60 ** 2 * 320
