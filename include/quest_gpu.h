@@ -227,6 +227,41 @@ qg_status qg_batch_remove(qg_batch *b, qg_handle *h);
 /* Advances every member by n_blocks x 16 steps (capped at its num_timesteps). */
 qg_status qg_batch_run(qg_batch *b, int n_blocks);
 qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks);
+/* Batch options: "profile" (1 = each block's kernels launched one by one
+ * instead of as the graph, with CUDA events around the far-pair launch and
+ * around the step launches; same results), "far_packed" (mixed-precision
+ * members: 1 = the FP32 convolution with packed pairs, 0 = scalar; same
+ * results). */
+qg_status qg_batch_set_option(qg_batch *b, const char *key, int value);
+/* Device time in milliseconds of the batch's far-pair launches and step
+ * launches (each nullable), accumulated while "profile" is on. */
+qg_status qg_batch_kernel_time(qg_batch *b, int reset, double *far_ms, int *far_launches, double *step_ms,
+                               int *step_launches);
+
+/* Target sharding of one ensemble over several GPUs (one process per GPU):
+ * the reference sums every pair in one loop (history_interaction.cpp:47-70);
+ * here shard `rank` of `world` computes the targets in its range of 32-dot
+ * blocks of the internal order (every group of dots coupled at delay 0 lies
+ * inside one block, so the current-step coupling never crosses shards) and
+ * holds every dot's rho01 history, which its far and mid terms read.  Shards
+ * compute their coefficients on the fly (coef_mode TABLE is refused).  Each
+ * step: qg_shard_step computes this shard's dots and writes their new rho01
+ * (count complex, internal order) to the device buffer d_slice; the caller
+ * gathers all shards' slices in rank order into one internal-order vector of
+ * n_pad complex (NCCL all-gather, peer copies) and passes it to
+ * qg_shard_import, which writes the other shards' dots into this shard's
+ * history as their own steps wrote theirs, and moves on one step.  Each
+ * target's sums are the unsharded handle's, term for term: a sharded run
+ * gives the unsharded run's results bit for bit.  qg_get_state, qg_bad_step
+ * and qg_checkpoint_* report this shard's dots only; qg_run is not used. */
+qg_status qg_shard_create(const qg_dot *dots, int n, const qg_pulse *pulse, const qg_params *params,
+                          const qg_weights *weights, int rank, int world, qg_handle **out);
+/* This shard's internal dots [*first, *first + *count), the internal slot
+ * count, and (user nullable, n_pad ints) the internal -> user index map, -1
+ * for padding. */
+qg_status qg_shard_layout(const qg_handle *h, int *first, int *count, int *n_pad, int *user);
+qg_status qg_shard_step(qg_handle *h, double *d_slice);
+qg_status qg_shard_import(qg_handle *h, const double *d_full);
 
 /* Diagnostics of the built state. */
 typedef struct {

@@ -63,6 +63,10 @@ def lib():
         L.or_history_evaluate_targets.argtypes = [dp, ctypes.c_int, ctypes.POINTER(OrParams), dp, ctypes.c_int,
                                                   ctypes.c_int, ctypes.c_int, ip, ctypes.c_int, dp]
         L.or_history_evaluate_targets.restype = ctypes.c_int
+        L.or_faithful_step_range.argtypes = [dp, ctypes.c_int, dp, ctypes.POINTER(OrParams),
+                                             ctypes.POINTER(OrWeights), ctypes.c_int, ip, dp, dp, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int]
+        L.or_faithful_step_range.restype = ctypes.c_int
         L.or_coord2idx.argtypes = [ctypes.c_int, ctypes.c_int]
         L.or_coord2idx.restype = ctypes.c_longlong
         L.or_idx2coord.argtypes = [ctypes.c_longlong, ip, ip]
@@ -205,6 +209,29 @@ def faithful_steps(dots, pulse, c, w: Weights, T, delays, coefs, hist, t0, nstep
                                    ctypes.byref(p), ctypes.byref(w.s), T,
                                    _ip(np.ascontiguousarray(delays, dtype=np.int32)), _dp(cf),
                                    _dp(hist.view(np.float64).reshape(-1)), t0, nsteps)
+
+
+def init_history(n: int, T: int) -> np.ndarray:
+    """The reference's initial History (main.cpp:30-36): rho = (1, 0) for
+    t <= 0, zeros elsewhere; complex128 (N, 22 + T, 2, 2)."""
+    hist = np.zeros((n, T + WINDOW, 2, 2), dtype=np.complex128)
+    hist[:, : WINDOW + 1, 0, 0] = 1.0
+    return hist
+
+
+def faithful_step_range(dots, pulse, c, w: Weights, T, delays, coefs, hist, step, lo, hi) -> None:
+    """One faithful step for dots [lo, hi) of `hist` in place (the others'
+    history read as it stands)."""
+    n = dots.shape[0]
+    p = params(c)
+    cf = np.ascontiguousarray(coefs).view(np.float64).reshape(-1)
+    assert hist.flags.c_contiguous and hist.dtype == np.complex128
+    rc = lib().or_faithful_step_range(_dp(np.ascontiguousarray(dots)), n, _dp(np.ascontiguousarray(pulse)),
+                                      ctypes.byref(p), ctypes.byref(w.s), T,
+                                      _ip(np.ascontiguousarray(delays, dtype=np.int32)), _dp(cf),
+                                      _dp(hist.view(np.float64).reshape(-1)), step, lo, hi)
+    if rc != 0:
+        raise ValueError("a delay-0 pair crosses the range [lo, hi)")
 
 
 def rho_trajectory(hist: np.ndarray) -> np.ndarray:

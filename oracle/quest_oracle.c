@@ -447,6 +447,58 @@ static void faithful_step(const or_dot *dots, int n, const or_pulse *pulse,
   }
 }
 
+/* One faithful step (integrator.cpp:128-140) for dots [lo, hi) only, the
+ * others' history read as it stands: each owned target's pair sum runs over
+ * its partners in the pair order of history_interaction.cpp:47-70, so the
+ * result is that of faithful_step bit for bit.  The current step's delay-0
+ * terms read partners' iterates of this step, which exist here only for
+ * owned partners: returns -1 (nothing done) when a delay-0 pair crosses the
+ * range.  Test infrastructure for the target-sharded driver. */
+int or_faithful_step_range(const or_dot *dots, int n, const or_pulse *pulse, const or_params *p,
+                           const or_weights *w, int T, const int *delays, const double *coefs, double *hist,
+                           int step, int lo, int hi)
+{
+  const int q = p->interpolation_order;
+  const int nc = 2 * (q + 1);
+  for(int a = lo; a < hi; ++a)
+    for(int b = 0; b < n; ++b)
+      if(b != a && (b < lo || b >= hi) && delays[or_coord2idx(a, b)] == 0) return -1;
+  double *pf = (double *)malloc(sizeof(double) * 2 * (n > 0 ? n : 1));
+  double *hf = (double *)calloc(2 * (size_t)(n > 0 ? n : 1), sizeof(double));
+  for(int a = lo; a < hi; ++a) predictor_one(hist, WINDOW, T, a, step, w, p->dt);
+  for(int it = 0; it <= NUM_CORRECTOR_STEPS; ++it) {
+    if(it > 0)
+      for(int a = lo; a < hi; ++a) corrector_one(hist, WINDOW, T, a, step, w, p->dt);
+    or_pulse_evaluate(dots, n, pulse, p, step, pf);
+    for(int a = lo; a < hi; ++a) {
+      double re = 0, im = 0;
+      for(int b = 0; b < n; ++b) {
+        if(b == a) continue;
+        const long long idx = or_coord2idx(a, b);
+        const int s = step - delays[idx];
+        for(int i = 0; i <= q; ++i) {
+          if(s - i < -WINDOW) continue;
+          const cx c = {coefs[idx * nc + 2 * i], coefs[idx * nc + 2 * i + 1]};
+          const cx v = cmul(prefactor(hist_at(hist, WINDOW, T, b, s - i, 0), p->frame), c);
+          re += v.re;
+          im += v.im;
+        }
+      }
+      hf[2 * a] = re;
+      hf[2 * a + 1] = im;
+    }
+    for(int a = lo; a < hi; ++a) {
+      double rabi[2] = {(0.0 + pf[2 * a]) + hf[2 * a], (0.0 + pf[2 * a + 1]) + hf[2 * a + 1]};
+      double out[4];
+      or_liouville_rhs(&dots[a], hist_at(hist, WINDOW, T, a, step, 0), rabi, p->laser_frequency, out);
+      memcpy(hist_atw(hist, WINDOW, T, a, step, 1), out, sizeof out);
+    }
+  }
+  free(pf);
+  free(hf);
+  return 0;
+}
+
 /* ---- integrator.cpp:120-140, 187-207 ---------------------------------- */
 int or_run_faithful(const or_dot *dots, int n, const or_pulse *pulse,
                     const or_params *p, const or_weights *w, int T,

@@ -139,6 +139,12 @@ int or_faithful_steps(const or_dot *dots, int n, const or_pulse *pulse,
                       const int *delays, const double *coefs, double *hist,
                       int t0, int nsteps);
 
+/* One faithful step for dots [lo, hi) only (the target-sharded driver's
+ * test backend); -1 when a delay-0 pair crosses the range. */
+int or_faithful_step_range(const or_dot *dots, int n, const or_pulse *pulse, const or_params *p,
+                           const or_weights *w, int T, const int *delays, const double *coefs, double *hist,
+                           int step, int lo, int hi);
+
 int or_window(void); /* 22: the history's negative-time extent (main.cpp:30) */
 
 #ifdef __cplusplus

@@ -74,7 +74,8 @@ EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_dest
            "qg_get_history", "qg_get_info", "qg_footprint", "qg_stream", "qg_kernel_time",
            "qg_set_option", "qg_get_option", "qg_history_evaluate_noalloc", "qg_get_state", "qg_bad_step",
            "qg_batch_create", "qg_batch_destroy", "qg_batch_add", "qg_batch_remove", "qg_batch_run",
-           "qg_batch_size", "qg_checkpoint_size", "qg_checkpoint_save", "qg_checkpoint_load"]
+           "qg_batch_size", "qg_batch_set_option", "qg_batch_kernel_time", "qg_checkpoint_size",
+           "qg_checkpoint_save", "qg_checkpoint_load"]
 
 _lib = None
 
@@ -121,6 +122,8 @@ def lib():
         L.qg_batch_remove.argtypes = [vp, vp]
         L.qg_batch_run.argtypes = [vp, ctypes.c_int]
         L.qg_batch_size.argtypes = [vp, ip, ip, ip]
+        L.qg_batch_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.qg_batch_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip, dp, ip]
         _lib = L
     return _lib
 
@@ -328,6 +331,16 @@ class Batch:
 
     def run(self, n_blocks: int) -> None:
         _check(lib().qg_batch_run(self.b, n_blocks))
+
+    def set_option(self, key: str, value: int) -> None:
+        _check(lib().qg_batch_set_option(self.b, key.encode(), int(value)))
+
+    def kernel_times(self, reset: bool = False) -> tuple[float, int, float, int]:
+        """(far ms, far launches, step ms, step launches) while "profile" is on."""
+        ms, n, sms, sn = ctypes.c_double(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().qg_batch_kernel_time(self.b, int(reset), ctypes.byref(ms), ctypes.byref(n),
+                                          ctypes.byref(sms), ctypes.byref(sn)))
+        return ms.value, n.value, sms.value, sn.value
 
     def size(self) -> tuple[int, int, int]:
         m, t, bl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

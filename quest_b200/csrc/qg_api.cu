@@ -127,6 +127,11 @@ struct qg_handle_s {
   // without a device copy while valid; any other run invalidates it)
   int batch_bad = kBadNone;
   bool batch_bad_valid = false;
+  // target sharding: this handle computes the 32-dot blocks [blk_lo, blk_hi)
+  // of the internal order (all of them unless it is a shard)
+  int shard_rank = 0, shard_world = 1;
+  int blk_lo = 0, blk_hi = 0;
+  double2 *d_shard_io = nullptr;  // n_pad complex: a shard's exchange staging
   int spin_limit = 0;       // step-block kernel polls per wait (0: its default, about a second)
   int skip_post = -1;       // failure-detection tests: a block that never posts its steps
   cudaEvent_t ev_a[256], ev_b[256], ev_c[256], ev_d[256];
@@ -170,6 +175,8 @@ struct qg_handle_s {
     s.cp.omega = params.laser_frequency;
     s.cp.q = q;
     s.cp.frame = params.frame;
+    s.tile_lo = shard_world > 1 ? blk_lo : 0;  // 32-dot blocks are the 32-dot target tiles
+    s.tile_n = shard_world > 1 ? blk_hi - blk_lo : 0;
     return s;
   }
 
@@ -232,6 +239,7 @@ struct qg_handle_s {
     a.d_bad = d_ints + 2;
     a.spin_limit = spin_limit;
     a.skip_post_block = skip_post;
+    a.blk_lo = shard_world > 1 ? blk_lo : 0;
     a.w = w;
     return a;
   }
@@ -1017,7 +1025,7 @@ static void enqueue_dot_step(qg_handle *h, int k, bool traj)
   StepArgs a = h->step_args(!h->fused);
   if(traj) a.traj = h->d_traj;
   if(h->fused) {
-    launch_step_fused(a, k, h->step_blocks, h->stream);
+    launch_step_fused(a, k, h->shard_world > 1 ? h->blk_hi - h->blk_lo : h->step_blocks, h->stream);
   } else {
     for(int ph = 0; ph <= kCorrectorSteps + 1; ++ph) launch_step_general(a, k, ph, h->stream);
   }
@@ -1171,6 +1179,113 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
   return QG_OK;
 }
 
+// ---- target sharding of one ensemble ------------------------------------------
+// A shard computes the targets in its range of 32-dot blocks of the internal
+// order (Morton order with every delay-0 group inside one block, so the
+// current-step coupling never crosses shards) and keeps every dot's rho01
+// history, which the far and mid terms read.  Coefficients are computed on the
+// fly (sharding is for ensembles whose table would not fit one GPU).  A step:
+// qg_shard_step computes the shard's dots and exports their new rho01; the
+// caller gathers all shards' slices (NCCL all-gather, peer copies, ...) into
+// the internal-order vector and hands it to qg_shard_import, which writes the
+// other shards' dots into the rings exactly as their own step kernels wrote
+// theirs.  Each target's sums are those of the unsharded handle, term for
+// term, so a sharded run gives the unsharded run's bits.
+extern "C" qg_status qg_shard_create(const qg_dot *dots, int n, const qg_pulse *pulse, const qg_params *params,
+                                     const qg_weights *weights, int rank, int world, qg_handle **out)
+{
+  if(!out) return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_create: out is NULL");
+  *out = nullptr;
+  if(world < 1 || rank < 0 || rank >= world)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_create: rank %d outside [0, %d)", rank, world);
+  QG_TRY(validate(dots, n, pulse, params));
+  if(params->coef_mode == QG_COEF_TABLE)
+    return qg_fail(QG_ERR_UNSUPPORTED, "qg_shard_create: shards compute their coefficients on the fly");
+  qg_params p = *params;
+  p.coef_mode = QG_COEF_ON_THE_FLY;
+  qg_handle *h = new qg_handle();
+  qg_status st = create_impl(dots, n, pulse, &p, weights, h);
+  if(st == QG_OK && !h->fused)
+    st = qg_fail(QG_ERR_UNSUPPORTED,
+                 "qg_shard_create: a group of dots coupled at delay 0 exceeds 32; it cannot be sharded");
+  if(st == QG_OK && h->step_blocks < world)
+    st = qg_fail(QG_ERR_INVALID_ARG, "qg_shard_create: %d blocks of 32 dots for %d shards", h->step_blocks,
+                 world);
+  if(st == QG_OK) {
+    h->shard_rank = rank;
+    h->shard_world = world;
+    h->blk_lo = (int)((long long)h->step_blocks * rank / world);
+    h->blk_hi = (int)((long long)h->step_blocks * (rank + 1) / world);
+    h->block_step = false;  // partners' steps come from other devices between steps
+    h->use_graph = false;
+    h->tune_pending = false;
+    st = dalloc(h, &h->d_shard_io, (size_t)h->n_pad);
+  }
+  if(st != QG_OK) {
+    destroy_handle(h);
+    return st;
+  }
+  *out = h;
+  return QG_OK;
+}
+
+// This shard's internal dots [*first, *first + *count) and the internal ->
+// user map of all n_pad internal slots (nullable; -1 marks padding).
+extern "C" qg_status qg_shard_layout(const qg_handle *h, int *first, int *count, int *n_pad, int *user)
+{
+  if(!h) return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_layout: NULL handle");
+  const int lo = h->shard_world > 1 ? h->blk_lo * kTile : 0;
+  const int hi = h->shard_world > 1 ? h->blk_hi * kTile : h->n_pad;
+  if(first) *first = lo;
+  if(count) *count = hi - lo;
+  if(n_pad) *n_pad = h->n_pad;
+  if(user) {
+    QG_CUDA(cudaSetDevice(h->device));
+    QG_CUDA(cudaMemcpy(user, h->d_user, sizeof(int) * (size_t)h->n_pad, cudaMemcpyDeviceToHost));
+  }
+  return QG_OK;
+}
+
+// One step of this shard's dots (the far field at block starts, then the
+// step kernel), and their new rho01 (count complex, internal order) into the
+// device buffer d_slice.  Returns when d_slice is written.
+extern "C" qg_status qg_shard_step(qg_handle *h, double *d_slice)
+{
+  if(!h || !d_slice) return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_step: NULL argument");
+  if(h->shard_world < 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_step: not a shard (qg_shard_create)");
+  if(h->next_step >= h->T)
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_step: step %d is past num_timesteps %d", h->next_step, h->T);
+  QG_CUDA(cudaSetDevice(h->device));
+  h->batch_bad_valid = false;
+  const int t = h->next_step, t0 = t - t % kTimeBlock;
+  if(h->far_block != t0) {
+    enqueue_far(h, t0, false, nullptr, nullptr);
+    h->far_block = t0;
+  }
+  enqueue_dot_step(h, t - t0, false);
+  launch_shard_export(h->step_args(false), t, h->blk_lo * kTile, h->blk_hi * kTile, (double2 *)d_slice,
+                      h->stream);
+  QG_CUDA(cudaGetLastError());
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  return QG_OK;
+}
+
+// The step just computed by every shard: d_full holds all n_pad dots' rho01
+// at that step (internal order, device memory); the other shards' dots go
+// into this shard's rings, and the shard moves to the next step.
+extern "C" qg_status qg_shard_import(qg_handle *h, const double *d_full)
+{
+  if(!h || !d_full) return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_import: NULL argument");
+  if(h->shard_world < 2) return qg_fail(QG_ERR_INVALID_ARG, "qg_shard_import: not a shard (qg_shard_create)");
+  QG_CUDA(cudaSetDevice(h->device));
+  launch_shard_import(h->step_args(false), h->next_step, h->blk_lo * kTile, h->blk_hi * kTile,
+                      (const double2 *)d_full, h->stream);
+  QG_CUDA(cudaGetLastError());
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  h->next_step += 1;
+  return QG_OK;
+}
+
 extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad_step)
 {
   if(!h) return qg_fail(QG_ERR_INVALID_ARG, "qg_run: NULL handle");
@@ -1253,6 +1368,13 @@ struct qg_batch_s {
   cudaGraphExec_t graph = nullptr;
   int *d_bad_all = nullptr;  // members' first bad steps, gathered after each run
   int *h_bad_all = nullptr;  // pinned copy
+  // "profile": blocks launched without the graph, CUDA events around the far
+  // launch and around the block's step launches
+  bool profile = false;
+  bool far_packed = false;  // mixed members: the packed FP32 convolution (same bits)
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double far_ms = 0, step_ms = 0;
+  int far_launches = 0, step_launches = 0;
 };
 
 extern "C" qg_status qg_batch_create(int capacity, qg_batch **out)
@@ -1302,6 +1424,8 @@ extern "C" qg_status qg_batch_destroy(qg_batch *b)
   cudaFree(b->d_block_off);
   cudaFree(b->d_bad_all);
   cudaFreeHost(b->h_bad_all);
+  for(auto e : b->ev)
+    if(e) cudaEventDestroy(e);
   cudaStreamDestroy(b->stream);
   delete b;
   return QG_OK;
@@ -1380,7 +1504,8 @@ static qg_status batch_rebuild(qg_batch *b)
   if(n > 0) {
     cudaGraph_t g;
     QG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->mixed, b->far_grid, b->stream);
+    launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->mixed ? (b->far_packed ? 2 : 1) : 0,
+                     b->far_grid, b->stream);
     for(int k = 0; k < kTimeBlock; ++k)
       launch_step_batch(b->d_step, b->d_block_off, n, b->total_blocks, b->n_time, k, b->stream);
     QG_CUDA(cudaStreamEndCapture(b->stream, &g));
@@ -1397,7 +1522,29 @@ extern "C" qg_status qg_batch_run(qg_batch *b, int n_blocks)
   QG_CUDA(cudaSetDevice(b->device));
   if(b->dirty) QG_TRY(batch_rebuild(b));
   if(b->members.empty()) return QG_OK;
-  for(int i = 0; i < n_blocks; ++i) QG_CUDA(cudaGraphLaunch(b->graph, b->stream));
+  const int nm0 = (int)b->members.size();
+  for(int i = 0; i < n_blocks; ++i) {
+    if(!b->profile) {
+      QG_CUDA(cudaGraphLaunch(b->graph, b->stream));
+      continue;
+    }
+    // the graph's kernels one by one, timed
+    QG_CUDA(cudaEventRecord(b->ev[0], b->stream));
+    launch_far_batch(b->d_far, b->d_task_off, nm0, b->q, b->frame, b->mixed ? (b->far_packed ? 2 : 1) : 0,
+                     b->far_grid, b->stream);
+    QG_CUDA(cudaEventRecord(b->ev[1], b->stream));
+    for(int k = 0; k < kTimeBlock; ++k)
+      launch_step_batch(b->d_step, b->d_block_off, nm0, b->total_blocks, b->n_time, k, b->stream);
+    QG_CUDA(cudaEventRecord(b->ev[2], b->stream));
+    QG_CUDA(cudaEventSynchronize(b->ev[2]));
+    float f = 0, g = 0;
+    QG_CUDA(cudaEventElapsedTime(&f, b->ev[0], b->ev[1]));
+    QG_CUDA(cudaEventElapsedTime(&g, b->ev[1], b->ev[2]));
+    b->far_ms += f;
+    b->step_ms += g;
+    b->far_launches += 1;
+    b->step_launches += kTimeBlock;
+  }
   // every member's first bad step in one copy, so a caller can retire a
   // member that went non-finite without a device round trip per member
   const int nm = (int)b->members.size();
@@ -1413,6 +1560,39 @@ extern "C" qg_status qg_batch_run(qg_batch *b, int n_blocks)
     h->eval_cached = -0x7fffffff;
     h->batch_bad = b->h_bad_all[e];
     h->batch_bad_valid = true;
+  }
+  return QG_OK;
+}
+
+extern "C" qg_status qg_batch_set_option(qg_batch *b, const char *key, int value)
+{
+  if(!b || !key) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_set_option: NULL argument");
+  if(!std::strcmp(key, "profile")) {
+    QG_CUDA(cudaSetDevice(b->device));
+    for(auto &e : b->ev)
+      if(!e) QG_CUDA(cudaEventCreate(&e));
+    b->profile = value != 0;
+    return QG_OK;
+  }
+  if(!std::strcmp(key, "far_packed")) {
+    b->far_packed = value != 0;
+    b->dirty = true;  // the block graph holds the kernel
+    return QG_OK;
+  }
+  return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_set_option: unknown key '%s'", key);
+}
+
+extern "C" qg_status qg_batch_kernel_time(qg_batch *b, int reset, double *far_ms, int *far_launches,
+                                          double *step_ms, int *step_launches)
+{
+  if(!b) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_kernel_time: NULL batch");
+  if(far_ms) *far_ms = b->far_ms;
+  if(far_launches) *far_launches = b->far_launches;
+  if(step_ms) *step_ms = b->step_ms;
+  if(step_launches) *step_launches = b->step_launches;
+  if(reset) {
+    b->far_ms = b->step_ms = 0;
+    b->far_launches = b->step_launches = 0;
   }
   return QG_OK;
 }

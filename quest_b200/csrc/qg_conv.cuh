@@ -115,10 +115,7 @@ __device__ __forceinline__ float2 pref32(float2 r)
 }
 
 // Packed FP32 pairs (Blackwell fma.rn.f32x2 / add.rn.f32x2): one instruction
-// does the two lanes of a complex component pair.  A complex multiply-add
-// acc += c r is two packed FMAs, (acc.x, acc.y) += (c.x, c.x) (r.x, r.y), then
-// += (-c.y, c.y) (r.y, r.x): per component exactly cfmaf's two fmaf in the
-// same order, so the results are bit-identical to the scalar form.
+// does two independent FP32 operations, each rounded as the scalar one is.
 __device__ __forceinline__ unsigned long long pk2(float2 v)
 {
   unsigned long long r;
@@ -143,44 +140,109 @@ __device__ __forceinline__ unsigned long long fadd2(unsigned long long a, unsign
   asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
-// acc += c r with c given as its packed pair (cxx = (c.x, c.x), cyy = (-c.y, c.y))
-__device__ __forceinline__ void cfma2(unsigned long long &acc, unsigned long long cxx, unsigned long long cyy,
-                                      unsigned long long r, unsigned long long rsw)
+// Accumulators of the mixed-precision convolution (difference form, see
+// qg_far.cu).  A complex multiply-add acc += c u is kept as two real pairs,
+// a += (c.x, c.x) (u.x, u.y) and b += (c.y, c.y) (u.x, u.y), so a packed
+// FP32 pair instruction (fma.rn.f32x2) does each without first swapping u's
+// halves; the product's real part is a.x - b.y and its imaginary part
+// a.y + b.x, formed in FP64 when the partial is written.  `base` collects the
+// tap-sum term (sum_i c_i) w_0, which is the same for all K outputs of a
+// pair, once per pair.  The packed form (PACKED) and the scalar form do the
+// same operations on the same values in the same order: the same bits.
+template <int K, bool PACKED>
+struct MixedAcc;
+
+template <int K>
+struct MixedAcc<K, false> {
+  float2 a[K], b[K];
+  float2 base;
+  __device__ __forceinline__ void zero()
+  {
+#pragma unroll
+    for(int k = 0; k < K; ++k) a[k] = b[k] = make_float2(0.f, 0.f);
+    base = make_float2(0.f, 0.f);
+  }
+  // a[k] += (cx, cx) u, b[k] += (cy, cy) u
+  __device__ __forceinline__ void mac(int k, float2 c, float2 u)
+  {
+    a[k].x = fmaf(c.x, u.x, a[k].x);
+    a[k].y = fmaf(c.x, u.y, a[k].y);
+    b[k].x = fmaf(c.y, u.x, b[k].x);
+    b[k].y = fmaf(c.y, u.y, b[k].y);
+  }
+  __device__ __forceinline__ float2 av(int k) const { return a[k]; }
+  __device__ __forceinline__ float2 bv(int k) const { return b[k]; }
+};
+
+template <int K>
+struct MixedAcc<K, true> {
+  unsigned long long a[K], b[K];
+  float2 base;
+  __device__ __forceinline__ void zero()
+  {
+#pragma unroll
+    for(int k = 0; k < K; ++k) a[k] = b[k] = pk2(make_float2(0.f, 0.f));
+    base = make_float2(0.f, 0.f);
+  }
+  __device__ __forceinline__ float2 av(int k) const { return upk2(a[k]); }
+  __device__ __forceinline__ float2 bv(int k) const { return upk2(b[k]); }
+};
+
+// The convolution's output k of one warp's sum, in FP64.
+template <int K, bool PACKED>
+__device__ __forceinline__ double2 mixed_out(const MixedAcc<K, PACKED> &m, int k)
 {
-  acc = ffma2(cxx, r, acc);
-  acc = ffma2(cyy, rsw, acc);
+  const float2 a = m.av(k), b = m.bv(k);
+  return make_double2(((double)a.x - (double)b.y) + (double)m.base.x,
+                      ((double)a.y + (double)b.x) + (double)m.base.y);
 }
 
-// The mixed-precision window convolution (difference form, see qg_far.cu):
-// acc[k] += sum_i c_i w_{k+Q-i}, w_m = w_0 + sum_{j<=m} d_j.  PACKED selects
-// the packed-pair form (bit-identical; faster where registers allow).
-template <int Q, bool LAB, int K>
-__device__ __forceinline__ void window_conv_mixed_packed(const float2 *rw, const float2 *rd, int slot0, int tau0,
-                                                         const float2 (&c)[Q + 2], float2 (&accf)[K]);
-
-template <int Q, bool LAB, int K, bool PACKED = false>
+// acc[k] += sum_i c_i w_{k+Q-i} over the window w_m, m = 0 .. K+Q-1, whose
+// first sample w_0 (step tau0) is rw[slot0] and whose later samples are
+// w_0 + u_m, u_m the running sum of the FP32 step-to-step differences
+// rd[slot0 + 1 .. slot0 + m].  c[Q+1] is the pair's tap sum.  When every
+// sample is live (tau0 >= -22) this is (sum_i c_i) w_0 + sum_i c_i u_{k+Q-i}:
+// the first term goes to `base` once and the differences meet only the taps.
+// Samples before step -22 are skipped (their taps are skipped by the
+// reference); there the absolute samples w_0 + u_m meet the live taps.
+template <int Q, bool LAB, int K, bool PACKED>
 __device__ __forceinline__ void window_conv_mixed(const float2 *rw, const float2 *rd, int slot0, int tau0,
-                                                  const float2 (&c)[Q + 2], float2 (&acc)[K])
+                                                  const float2 (&c)[Q + 2], MixedAcc<K, PACKED> &acc)
 {
-  if(PACKED) {
-    window_conv_mixed_packed<Q, LAB, K>(rw, rd, slot0, tau0, c, acc);
-    return;
-  }
   const float2 w0 = pref32<LAB>(__ldg(rw + slot0));
-  float2 u = make_float2(0.f, 0.f);
   if(tau0 >= -kWindow) {
+    cfmaf(acc.base, c[Q + 1], w0);
+    if constexpr(PACKED) {
+      unsigned long long cx[Q + 1], cy[Q + 1];
 #pragma unroll
-    for(int k = 0; k < K; ++k) cfmaf(acc[k], c[Q + 1], w0);
+      for(int i = 0; i <= Q; ++i) {
+        cx[i] = pk2(make_float2(c[i].x, c[i].x));
+        cy[i] = pk2(make_float2(c[i].y, c[i].y));
+      }
+      unsigned long long u = pk2(make_float2(0.f, 0.f));
 #pragma unroll
-    for(int m = 1; m < K + Q; ++m) {
-      const float2 d = pref32<LAB>(__ldg(rd + slot0 + m));
-      u.x += d.x;
-      u.y += d.y;
+      for(int m = 1; m < K + Q; ++m) {
+        u = fadd2(u, pk2(pref32<LAB>(__ldg(rd + slot0 + m))));
 #pragma unroll
-      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfmaf(acc[k], c[k + Q - m], u);
+        for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) {
+          acc.a[k] = ffma2(cx[k + Q - m], u, acc.a[k]);
+          acc.b[k] = ffma2(cy[k + Q - m], u, acc.b[k]);
+        }
+      }
+    } else {
+      float2 u = make_float2(0.f, 0.f);
+#pragma unroll
+      for(int m = 1; m < K + Q; ++m) {
+        const float2 d = pref32<LAB>(__ldg(rd + slot0 + m));
+        u.x += d.x;
+        u.y += d.y;
+#pragma unroll
+        for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) acc.mac(k, c[k + Q - m], u);
+      }
     }
   } else {
     // early steps: absolute samples, taps before step -22 skipped
+    float2 u = make_float2(0.f, 0.f);
 #pragma unroll
     for(int m = 0; m < K + Q; ++m) {
       if(m > 0) {
@@ -191,55 +253,16 @@ __device__ __forceinline__ void window_conv_mixed(const float2 *rw, const float2
       if(tau0 + m < -kWindow) continue;
       const float2 w = make_float2(w0.x + u.x, w0.y + u.y);
 #pragma unroll
-      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfmaf(acc[k], c[k + Q - m], w);
+      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) {
+        if constexpr(PACKED) {
+          acc.a[k] = ffma2(pk2(make_float2(c[k + Q - m].x, c[k + Q - m].x)), pk2(w), acc.a[k]);
+          acc.b[k] = ffma2(pk2(make_float2(c[k + Q - m].y, c[k + Q - m].y)), pk2(w), acc.b[k]);
+        } else {
+          acc.mac(k, c[k + Q - m], w);
+        }
+      }
     }
   }
-}
-
-// The same convolution with the accumulators and coefficients as packed
-// FP32 pairs: half the FMA instructions, more registers.
-template <int Q, bool LAB, int K>
-__device__ __forceinline__ void window_conv_mixed_packed(const float2 *rw, const float2 *rd, int slot0, int tau0,
-                                                  const float2 (&c)[Q + 2], float2 (&accf)[K])
-{
-  unsigned long long cxx[Q + 2], cyy[Q + 2], acc[K];
-#pragma unroll
-  for(int i = 0; i <= Q + 1; ++i) {
-    cxx[i] = pk2(make_float2(c[i].x, c[i].x));
-    cyy[i] = pk2(make_float2(-c[i].y, c[i].y));
-  }
-#pragma unroll
-  for(int k = 0; k < K; ++k) acc[k] = pk2(accf[k]);
-  const float2 w0f = pref32<LAB>(__ldg(rw + slot0));
-  const unsigned long long w0 = pk2(w0f), w0s = pk2(make_float2(w0f.y, w0f.x));
-  unsigned long long u = pk2(make_float2(0.f, 0.f));
-  if(tau0 >= -kWindow) {
-#pragma unroll
-    for(int k = 0; k < K; ++k) cfma2(acc[k], cxx[Q + 1], cyy[Q + 1], w0, w0s);
-#pragma unroll
-    for(int m = 1; m < K + Q; ++m) {
-      u = fadd2(u, pk2(pref32<LAB>(__ldg(rd + slot0 + m))));
-      const float2 uf = upk2(u);
-      const unsigned long long us = pk2(make_float2(uf.y, uf.x));
-#pragma unroll
-      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k)
-        cfma2(acc[k], cxx[k + Q - m], cyy[k + Q - m], u, us);
-    }
-  } else {
-    // early steps: absolute samples, taps before step -22 skipped
-#pragma unroll
-    for(int m = 0; m < K + Q; ++m) {
-      if(m > 0) u = fadd2(u, pk2(pref32<LAB>(__ldg(rd + slot0 + m))));
-      if(tau0 + m < -kWindow) continue;
-      const float2 wf = make_float2(w0f.x + upk2(u).x, w0f.y + upk2(u).y);
-      const unsigned long long w = pk2(wf), ws = pk2(make_float2(wf.y, wf.x));
-#pragma unroll
-      for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k)
-        cfma2(acc[k], cxx[k + Q - m], cyy[k + Q - m], w, ws);
-    }
-  }
-#pragma unroll
-  for(int k = 0; k < K; ++k) accf[k] = upk2(acc[k]);
 }
 
 // Writes a warp's K accumulators as the partial of source group g for target

@@ -277,7 +277,8 @@ __global__ void __launch_bounds__(128, VEC == 3 ? 4 : 1) far_kernel_async(FarArg
 // step-to-step differences (themselves computed in FP64).  The large
 // interpolation weights (w1 ~ 1/dt, w2 ~ 1/dt^2) multiply only differences,
 // and sum_i c_i carries no such factor, so FP32 storage loses no more than a
-// few units in the last place of the pair's contribution.
+// few units in the last place of the pair's contribution.  The first term is
+// the same for all K outputs and is accumulated once per pair (MixedAcc).
 template <int Q, bool LAB, int K = kTimeBlock, bool PACKED = false>
 __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
 {
@@ -290,9 +291,8 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
   if(task == 0 && lane == 0) *a.far_t0_out = t0;
   const int W = a.W;
 
-  float2 acc[K];
-#pragma unroll
-  for(int k = 0; k < K; ++k) acc[k] = make_float2(0.f, 0.f);
+  MixedAcc<K, PACKED> acc;
+  acc.zero();
 
   const long long tile0 = (long long)I * a.nT + J0;
   const int iters = nJ * kTile;
@@ -325,7 +325,7 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
   // the per-dot sums across groups are carried in FP64
   double2 acc64[K];
 #pragma unroll
-  for(int k = 0; k < K; ++k) acc64[k] = make_double2((double)acc[k].x, (double)acc[k].y);
+  for(int k = 0; k < K; ++k) acc64[k] = mixed_out(acc, k);
   group_partials_reduce<K>(a, I, g, acc64);
 }
 
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(128, 4) far_kernel_v2(FarArgs a) { far_body<Q,
 // ensemble e (prefix sums, task_off[n_ens] = total).  Warps stride over the
 // list; every task writes its own partial slot, so the assignment of tasks to
 // warps does not change any result.
-template <int Q, bool LAB, bool MIXED>
+template <int Q, bool LAB, bool MIXED, bool PACKED = false>
 __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restrict__ args,
                                                         const int *__restrict__ task_off, int n_ens)
 {
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restric
     }
     const FarArgs a = args[lo];  // a copy: the bodies read its fields in their inner loops
     if(MIXED)
-      far_body_mixed<Q, LAB>(a, task - task_off[lo]);
+      far_body_mixed<Q, LAB, kTimeBlock, PACKED>(a, task - task_off[lo]);
     else
       far_body<Q, LAB, 0>(a, task - task_off[lo]);
   }
@@ -366,27 +366,31 @@ __global__ void __launch_bounds__(128) far_batch_kernel(const FarArgs *__restric
 
 // FP64 members take far_kernel's body (table prefetched in registers, the
 // fastest FP64 variant, 168 registers: 3 blocks per SM, the persistent
-// grid's shape); mixed members the scalar FP32 convolution (the packed form
-// measured 13 % slower in this kernel).  Every form gives the same bits, so
-// a member's result is the same alone and in a batch.
+// grid's shape); mixed members the FP32 convolution, scalar (mixed == 1) or
+// with packed pairs (mixed == 2).  Every form gives the same bits, so a
+// member's result is the same alone and in a batch.
 template <int Q, bool LAB, bool MIXED>
-static void launch_far_batch_q(const FarArgs *args, const int *task_off, int n_ens, int grid, cudaStream_t s)
+static void launch_far_batch_q(const FarArgs *args, const int *task_off, int n_ens, int grid, bool packed,
+                               cudaStream_t s)
 {
-  far_batch_kernel<Q, LAB, MIXED><<<grid, 128, 0, s>>>(args, task_off, n_ens);
+  if(MIXED && packed)
+    far_batch_kernel<Q, LAB, MIXED, true><<<grid, 128, 0, s>>>(args, task_off, n_ens);
+  else
+    far_batch_kernel<Q, LAB, MIXED, false><<<grid, 128, 0, s>>>(args, task_off, n_ens);
 }
 
 template <bool LAB, bool MIXED>
 static void launch_far_batch_frame(const FarArgs *args, const int *task_off, int n_ens, int q, int grid,
-                                   cudaStream_t s)
+                                   bool packed, cudaStream_t s)
 {
   switch(q) {
-    case 1: launch_far_batch_q<1, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
-    case 2: launch_far_batch_q<2, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
-    case 3: launch_far_batch_q<3, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
-    case 4: launch_far_batch_q<4, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
-    case 5: launch_far_batch_q<5, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
-    case 6: launch_far_batch_q<6, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
-    case 7: launch_far_batch_q<7, LAB, MIXED>(args, task_off, n_ens, grid, s); break;
+    case 1: launch_far_batch_q<1, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
+    case 2: launch_far_batch_q<2, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
+    case 3: launch_far_batch_q<3, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
+    case 4: launch_far_batch_q<4, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
+    case 5: launch_far_batch_q<5, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
+    case 6: launch_far_batch_q<6, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
+    case 7: launch_far_batch_q<7, LAB, MIXED>(args, task_off, n_ens, grid, packed, s); break;
     default: break;
   }
 }
@@ -396,12 +400,13 @@ void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q
 {
   if(n_ens <= 0) return;
   cudaStream_t s = (cudaStream_t)stream;
+  const bool packed = mixed == 2;
   if(frame == 0)
-    mixed ? launch_far_batch_frame<false, true>(args, task_off, n_ens, q, grid, s)
-          : launch_far_batch_frame<false, false>(args, task_off, n_ens, q, grid, s);
+    mixed ? launch_far_batch_frame<false, true>(args, task_off, n_ens, q, grid, packed, s)
+          : launch_far_batch_frame<false, false>(args, task_off, n_ens, q, grid, packed, s);
   else
-    mixed ? launch_far_batch_frame<true, true>(args, task_off, n_ens, q, grid, s)
-          : launch_far_batch_frame<true, false>(args, task_off, n_ens, q, grid, s);
+    mixed ? launch_far_batch_frame<true, true>(args, task_off, n_ens, q, grid, packed, s)
+          : launch_far_batch_frame<true, false>(args, task_off, n_ens, q, grid, packed, s);
 }
 
 template <int Q, bool LAB>

@@ -89,6 +89,9 @@ struct FarArgs {
   const double *dip;    // [n_pad][3]
   const int *user;      // internal -> user index, -1 for padding
   CoefParams cp;
+  // target tiles [tile_lo, tile_lo + tile_n) only (a shard of a sharded
+  // handle; on-the-fly kernel); tile_n == 0: all nT
+  int tile_lo, tile_n;
 };
 
 // Arguments of the per-dot step kernels.
@@ -150,6 +153,7 @@ struct StepArgs {
   // (-1: none; set only by failure-detection tests, so that waits run out)
   int spin_limit;
   int skip_post_block;
+  int blk_lo;  // first 32-dot block of the per-step launch (a shard's range)
   PCW w;
 };
 
@@ -169,9 +173,16 @@ struct NoAllocScratch {
 };
 qg_status noalloc_scratch(NoAllocScratch *out);
 void launch_far_step1(const FarArgs &a, void *stream);
+// mixed: 0 FP64 members, 1 mixed (scalar FP32 convolution), 2 mixed (packed
+// FP32 pairs; the same bits as 1)
 void launch_far_batch(const FarArgs *args, const int *task_off, int n_ens, int q, int frame, int mixed,
                       int grid, void *stream);
 void launch_ring32_rebuild(const StepArgs &a, void *stream);
+// Sharded handles: a shard's rho01 at step t for internal dots [lo, hi)
+// into out[0 .. hi-lo), and the other dots' rho01 at step t from the full
+// internal-order vector into the rings (as the step kernel writes its own)
+void launch_shard_export(const StepArgs &a, int t, int lo, int hi, double2 *out, void *stream);
+void launch_shard_import(const StepArgs &a, int t, int lo, int hi, const double2 *full, void *stream);
 // out[e] = *args[e].d_bad for the n members of a batch
 void launch_gather_bad(const StepArgs *args, int n, int *out, void *stream);
 // The step-block kernel's per-block step counts, one per 128-byte line (so

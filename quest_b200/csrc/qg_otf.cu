@@ -24,15 +24,14 @@
 
 namespace qg {
 
-// PACKED: the mixed convolution with packed FP32 pairs (same bits).  Measured
-// at N = 65536 it is slower here (10.0 against 9.4 ms per step): the swaps it
-// needs compete for issue slots with the coefficient work.
+// PACKED: the mixed convolution with packed FP32 pairs (same bits).
 template <int Q, bool LAB, bool MIXED, int K = kTimeBlock, bool PACKED = false>
 __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
 {
   const int lane = threadIdx.x & 31;
-  if(task >= a.nT * a.nG) return;  // uniform per warp
-  const int I = task / a.nG, g = task % a.nG;
+  const int n_tiles = a.tile_n > 0 ? a.tile_n : a.nT;  // target tiles of this launch
+  if(task >= n_tiles * a.nG) return;                   // uniform per warp
+  const int I = a.tile_lo + task / a.nG, g = task % a.nG;
   const int J0 = g * a.group;
   const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
@@ -48,12 +47,10 @@ __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
   }
 
   double2 acc[K];
-  float2 accf[K];
+  MixedAcc<K, PACKED> accf;
 #pragma unroll
-  for(int k = 0; k < K; ++k) {
-    acc[k] = make_double2(0.0, 0.0);
-    accf[k] = make_float2(0.f, 0.f);
-  }
+  for(int k = 0; k < K; ++k) acc[k] = make_double2(0.0, 0.0);
+  if(MIXED) accf.zero();
 
   const int iters = nJ * kTile;
   for(int it = 0; it < iters; ++it) {
@@ -100,7 +97,7 @@ __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
   }
   if(MIXED) {
 #pragma unroll
-    for(int k = 0; k < K; ++k) acc[k] = make_double2((double)accf[k].x, (double)accf[k].y);
+    for(int k = 0; k < K; ++k) acc[k] = mixed_out(accf, k);
   }
   group_partials_reduce<K>(a, I, g, acc);
 }
@@ -114,7 +111,7 @@ __global__ void __launch_bounds__(128) far_otf_kernel(FarArgs a)
 template <bool LAB, bool MIXED>
 static void launch_otf_q(const FarArgs &a, cudaStream_t s)
 {
-  const unsigned blocks = (unsigned)(((long long)a.nT * a.nG + 3) / 4);
+  const unsigned blocks = (unsigned)(((long long)(a.tile_n > 0 ? a.tile_n : a.nT) * a.nG + 3) / 4);
   switch(a.q) {
     case 1: far_otf_kernel<1, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
     case 2: far_otf_kernel<2, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;

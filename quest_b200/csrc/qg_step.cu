@@ -563,7 +563,7 @@ __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int 
 template <int NT>
 __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int k)
 {
-  step_fused_body<NT>(a, blockIdx.x, k);
+  step_fused_body<NT>(a, a.blk_lo + blockIdx.x, k);
 }
 
 // Many ensembles, one launch: block_off[e] = first 32-dot block of ensemble e.
@@ -1175,6 +1175,36 @@ __global__ void init_state_kernel(StepArgs a)
   base[a.n_pad] = make_double2(0.0, 0.0);
   base[2 * a.n_pad] = make_double2(0.0, 0.0);
   base[3 * a.n_pad] = make_double2(0.0, 0.0);
+}
+
+__global__ void shard_export_kernel(StepArgs a, int t, int lo, int hi, double2 *out)
+{
+  const int idx = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= hi) return;
+  out[idx - lo] = a.user[idx] >= 0 ? a.ring[(long long)idx * a.stride + ring_slot(t, a.W)] : make_double2(0.0, 0.0);
+}
+
+void launch_shard_export(const StepArgs &a, int t, int lo, int hi, double2 *out, void *stream)
+{
+  if(hi > lo) shard_export_kernel<<<(hi - lo + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, lo, hi, out);
+}
+
+// The other shards' dots: their rho01 at step t written exactly as their own
+// step kernel writes it (finish_ring: FP64 ring, and in mixed precision the
+// FP32 value and the FP64-formed step difference).
+__global__ void shard_import_kernel(StepArgs a, int t, int lo, int hi, const double2 *full)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if(idx >= a.n_pad || (idx >= lo && idx < hi) || a.user[idx] < 0) return;
+  double2 r[2];
+  r[0] = make_double2(0.0, 0.0);
+  r[1] = full[idx];
+  finish_ring(a, idx, t, r);
+}
+
+void launch_shard_import(const StepArgs &a, int t, int lo, int hi, const double2 *full, void *stream)
+{
+  shard_import_kernel<<<(a.n_pad + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, t, lo, hi, full);
 }
 
 __global__ void gather_bad_kernel(const StepArgs *args, int n, int *out)
