@@ -75,7 +75,8 @@ EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_dest
            "qg_set_option", "qg_get_option", "qg_history_evaluate_noalloc", "qg_get_state", "qg_bad_step",
            "qg_batch_create", "qg_batch_destroy", "qg_batch_add", "qg_batch_remove", "qg_batch_run",
            "qg_batch_size", "qg_batch_set_option", "qg_batch_kernel_time", "qg_checkpoint_size",
-           "qg_checkpoint_save", "qg_checkpoint_load"]
+           "qg_checkpoint_save", "qg_checkpoint_load", "qg_shard_create", "qg_shard_layout", "qg_shard_step",
+           "qg_shard_import"]
 
 _lib = None
 
@@ -123,6 +124,12 @@ def lib():
         L.qg_batch_run.argtypes = [vp, ctypes.c_int]
         L.qg_batch_size.argtypes = [vp, ip, ip, ip]
         L.qg_batch_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.qg_shard_create.argtypes = [ctypes.POINTER(QgDot), ctypes.c_int, ctypes.POINTER(QgPulse),
+                                      ctypes.POINTER(QgParams), ctypes.POINTER(QgWeights), ctypes.c_int,
+                                      ctypes.c_int, ctypes.POINTER(vp)]
+        L.qg_shard_layout.argtypes = [vp, ip, ip, ip, ip]
+        L.qg_shard_step.argtypes = [vp, dp]
+        L.qg_shard_import.argtypes = [vp, dp]
         L.qg_batch_kernel_time.argtypes = [vp, ctypes.c_int, dp, ip, dp, ip]
         _lib = L
     return _lib

@@ -22,7 +22,7 @@ GPUs and in the CPU tests:
 from __future__ import annotations
 
 import ctypes
-from typing import Optional, Sequence
+from typing import Sequence
 
 import numpy as np
 
@@ -42,9 +42,11 @@ class DistExchange:
 
     def all_gather(self, x):
         import torch
-        out = torch.empty((self.world,) + tuple(x.shape), dtype=x.dtype, device=x.device)
+        # the ranks' tensors concatenated along the first dimension, then
+        # viewed as (world, *x.shape)
+        out = torch.empty((self.world * x.shape[0],) + tuple(x.shape[1:]), dtype=x.dtype, device=x.device)
         self.dist.all_gather_into_tensor(out, x.contiguous(), group=self.group)
-        return out
+        return out.view((self.world,) + tuple(x.shape))
 
 
 class ShardDriver:
@@ -144,20 +146,6 @@ class GpuShard:
             self.close()
         except Exception:
             pass
-
-
-class LocalExchange:
-    """The ranks of one process (a test on one GPU, or shards whose drivers
-    are stepped in turn): all_gather collects each rank's tensor once every
-    rank has handed it in.  Used with LocalGroup.step, never across
-    processes."""
-
-    def __init__(self, world: int):
-        self.world = world
-        self.pending: list = []
-
-    def all_gather(self, x):
-        raise RuntimeError("LocalExchange gathers through LocalGroup.step")
 
 
 class LocalGroup:
