@@ -69,7 +69,13 @@ typedef struct {
 
 typedef enum { QG_FRAME_ROTATING = 0, QG_FRAME_LAB = 1 } qg_frame;
 typedef enum { QG_PREC_FP64 = 0, QG_PREC_MIXED = 1 } qg_precision;
-typedef enum { QG_COEF_AUTO = 0, QG_COEF_TABLE = 1, QG_COEF_ON_THE_FLY = 2 } qg_coef_mode;
+/* QG_COEF_AUTO: the per-pair table when it takes at most half of the free
+ * device memory, else on the fly.  QG_COEF_TUNED: where the table fits, the
+ * first qg_run times the table kernel (its fastest variant) against the
+ * on-the-fly kernel and keeps the faster, freeing the table if it loses; the
+ * two coefficient forms are algebraically equal, so results differ only in
+ * the last bits (qg_get_option "coef_mode" reports the choice). */
+typedef enum { QG_COEF_AUTO = 0, QG_COEF_TABLE = 1, QG_COEF_ON_THE_FLY = 2, QG_COEF_TUNED = 3 } qg_coef_mode;
 
 /* Everything the reference reads from its global `config`
  * (src/configuration.h:12-19) plus this library's options. */
@@ -321,9 +327,11 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
 qg_status qg_set_option(qg_handle *h, const char *key, int value);
 
 /* Reads an option back: "graph", "profile", "far_variant" (the variant in
- * use, which after qg_create is the autotuner's choice), "block_step",
- * "far_group", "wait_limit", "test_skip_post".  No reference counterpart (the
- * reference has no options). */
+ * use, which after the first qg_run is the autotuner's choice), "block_step",
+ * "far_group", "wait_limit", "test_skip_post", "coef_mode" (QG_COEF_TABLE or
+ * QG_COEF_ON_THE_FLY: the form in use), "tuned_far_us" (the far kernel's
+ * launch time the autotuner measured for its choice, microseconds; 0 if it
+ * did not run).  No reference counterpart (the reference has no options). */
 qg_status qg_get_option(const qg_handle *h, const char *key, int *value);
 
 #ifdef __cplusplus

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libquest_gpu.so")
 QG_OK, QG_ERR_INVALID_ARG, QG_ERR_CUDA, QG_ERR_OOM, QG_ERR_NONFINITE, QG_ERR_UNSUPPORTED = range(6)
 FRAME_ROTATING, FRAME_LAB = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
-COEF_AUTO, COEF_TABLE, COEF_ON_THE_FLY = 0, 1, 2
+COEF_AUTO, COEF_TABLE, COEF_ON_THE_FLY, COEF_TUNED = 0, 1, 2, 3
 
 
 class QuestError(RuntimeError):

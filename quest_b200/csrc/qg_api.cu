@@ -121,6 +121,7 @@ struct qg_handle_s {
   bool use_graph = true;
   int far_variant = 3;  // cp.async-staged table (see qg_far.cu); the autotuner may change it
   float tuned_far_ms = 0;  // far-kernel time of the autotuner's choice
+  bool tune_coef = false;  // QG_COEF_TUNED: also time the on-the-fly kernel against the table
   bool tune_pending = false;  // the far-kernel autotuner runs at the first qg_run
   bool profile = false;
   // first bad step as the last batch run read it (qg_bad_step answers from it
@@ -371,7 +372,8 @@ static qg_status validate(const qg_dot *dots, int n, const qg_pulse *pulse, cons
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown frame %d", p->frame);
   if(p->precision != QG_PREC_FP64 && p->precision != QG_PREC_MIXED)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown precision %d", p->precision);
-  if(p->coef_mode != QG_COEF_AUTO && p->coef_mode != QG_COEF_TABLE && p->coef_mode != QG_COEF_ON_THE_FLY)
+  if(p->coef_mode != QG_COEF_AUTO && p->coef_mode != QG_COEF_TABLE && p->coef_mode != QG_COEF_ON_THE_FLY &&
+     p->coef_mode != QG_COEF_TUNED)
     return qg_fail(QG_ERR_INVALID_ARG, "qg_create: unknown coef_mode %d", p->coef_mode);
   return QG_OK;
 }
@@ -810,7 +812,9 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   const size_t tb = table_bytes(h->nT, h->q, h->mixed);
   size_t free_b = 0, total_b = 0;
   QG_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  h->otf = p->coef_mode == QG_COEF_ON_THE_FLY || (p->coef_mode == QG_COEF_AUTO && tb > free_b / 2);
+  const bool rule = p->coef_mode == QG_COEF_AUTO || p->coef_mode == QG_COEF_TUNED;
+  h->otf = p->coef_mode == QG_COEF_ON_THE_FLY || (rule && tb > free_b / 2);
+  h->tune_coef = p->coef_mode == QG_COEF_TUNED && !h->otf;
   if(!h->otf && tb > free_b * 0.9)
     return qg_fail(QG_ERR_OOM, "qg_create: coefficient table needs %zu bytes, %zu free", tb, free_b);
   if(h->otf) {
@@ -916,9 +920,77 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 // fastest is kept.  The history
 // is whatever the handle holds (its values do not change the work), and the
 // far field and partials are recomputed by the next run.
+static qg_status time_far(qg_handle *h, int rounds_untimed, int rounds_timed, float *best_ms)
+{
+  cudaEvent_t e0, e1;
+  QG_CUDA(cudaEventCreate(&e0));
+  QG_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for(int round = 0; round < rounds_untimed + rounds_timed; ++round) {
+    const FarArgs fa = h->far_args(h->d_ints + 7, h->d_ints + 6);
+    if(round < rounds_untimed) {
+      launch_far(fa, h->stream);
+      continue;
+    }
+    QG_CUDA(cudaEventRecord(e0, h->stream));
+    launch_far(fa, h->stream);
+    QG_CUDA(cudaEventRecord(e1, h->stream));
+    QG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *best_ms = best;
+  return QG_OK;
+}
+
+// QG_COEF_TUNED: the on-the-fly kernel (its own source grouping) against the
+// table kernel's time; when it wins, the handle switches to it and frees the
+// table.
+static qg_status autotune_coef(qg_handle *h)
+{
+  const int group_t = h->group, nG_t = h->nG;
+  h->otf = true;
+  h->group = (h->nT + 15) / 16;
+  h->nG = (h->nT + h->group - 1) / h->group;
+  float otf_ms = 0;
+  const qg_status st = time_far(h, 2, 3, &otf_ms);
+  if(st != QG_OK || otf_ms >= h->tuned_far_ms) {
+    h->otf = false;
+    h->group = group_t;
+    h->nG = nG_t;
+    return st;
+  }
+  // the on-the-fly kernel is faster: keep it, return the table's memory
+  QG_CUDA(cudaStreamSynchronize(h->stream));
+  for(void *p : {(void *)h->d_delay, (void *)h->d_coef, (void *)h->d_coef32}) {
+    if(!p) continue;
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+    if(it != h->allocs.end()) h->allocs.erase(it);
+    QG_CUDA(cudaFree(p));
+  }
+  h->bytes -= table_bytes(h->nT, h->q, h->mixed);
+  h->d_delay = nullptr;
+  h->d_coef = nullptr;
+  h->d_coef32 = nullptr;
+  h->tuned_far_ms = otf_ms;
+  return QG_OK;
+}
+
 static qg_status autotune_far(qg_handle *h)
 {
-  if(h->otf || h->mixed || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
+  if(h->otf || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
+  if(h->mixed) {
+    // one table kernel: its time is the one the coefficient choice compares
+    launch_set_int(h->d_ints + 7, h->max_delay + h->q + 2 * kTimeBlock, h->stream);
+    QG_TRY(time_far(h, 2, 3, &h->tuned_far_ms));
+    if(h->tune_coef) QG_TRY(autotune_coef(h));
+    h->far_block = -0x7fffffff;
+    h->eval_cached = -0x7fffffff;
+    return QG_OK;
+  }
   static const int candidates[] = {0, 3, 5, 6};
   const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
   cudaEvent_t e0, e1;
@@ -955,6 +1027,7 @@ static qg_status autotune_far(qg_handle *h)
   QG_CUDA(cudaGetLastError());
   h->far_variant = best_v;
   h->tuned_far_ms = best;
+  if(h->tune_coef) QG_TRY(autotune_coef(h));
   h->far_block = -0x7fffffff;
   h->eval_cached = -0x7fffffff;
   return QG_OK;
@@ -2032,6 +2105,10 @@ extern "C" qg_status qg_get_option(const qg_handle *h, const char *key, int *val
     *value = h->group;
   else if(!std::strcmp(key, "wait_limit"))
     *value = h->spin_limit;
+  else if(!std::strcmp(key, "coef_mode"))
+    *value = h->otf ? QG_COEF_ON_THE_FLY : QG_COEF_TABLE;
+  else if(!std::strcmp(key, "tuned_far_us"))
+    *value = (int)(h->tuned_far_ms * 1000.0f + 0.5f);
   else if(!std::strcmp(key, "test_skip_post"))
     *value = h->skip_post;
   else

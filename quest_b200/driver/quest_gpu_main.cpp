@@ -8,7 +8,7 @@
 // output.dat (history.cpp:17-34).  Options of this build only:
 //   --output PATH        output file (default output.dat)
 //   --precision fp64|mixed
-//   --coefficients auto|table|on-the-fly
+//   --coefficients auto|table|on-the-fly|tuned
 // A non-finite state ends the run with the reference's std::domain_error
 // message on stderr and exit status 1, before any output is written (the
 // reference's uncaught exception also leaves no output.dat).
@@ -43,7 +43,7 @@ void usage(std::ostream &os)
         "  -c [ --config ] arg (=input.cfg) path to configuration file\n"
         "  --output arg (=output.dat)       path of the trajectory output\n"
         "  --precision arg (=fp64)          fp64 or mixed\n"
-        "  --coefficients arg (=auto)       auto, table or on-the-fly\n"
+        "  --coefficients arg (=auto)       auto, table, on-the-fly or tuned (timed)\n"
         "\n"
         "Configuration files:\n"
         "  --files.qd_path arg (=dots.cfg)     path to dot configuration file\n"
@@ -96,6 +96,8 @@ bool parse_args(int argc, char **argv, Options &o)
         o.coef_mode = QG_COEF_TABLE;
       else if(v == "on-the-fly")
         o.coef_mode = QG_COEF_ON_THE_FLY;
+      else if(v == "tuned")
+        o.coef_mode = QG_COEF_TUNED;
       else
         throw std::runtime_error("the argument ('" + v + "') for option '--coefficients' is invalid");
     } else {
