@@ -230,6 +230,9 @@ def fp_peak_tflops(dtype="float64") -> float:
 FAR_VARIANTS = {0: "far_kernel<5,false>", 1: "far_kernel_r4<5,false>", 2: "far_kernel_v2<5,false>",
                 3: "far_kernel_async<5,false,0>", 4: "far_kernel_async<5,false,1>",
                 5: "far_kernel_async<5,false,2>", 6: "far_kernel_async<5,false,3>"}
+# 7 and 8: kernels of 0 and 3 with the source-group-major task order
+FAR_VARIANTS[7] = FAR_VARIANTS[0]
+FAR_VARIANTS[8] = FAR_VARIANTS[3]
 TRAFFIC_NOTE = ("DRAM bytes need a profiler capture; they are not measured inside this run (null). "
                 "The committed ncu summaries of the same kernel give them.")
 

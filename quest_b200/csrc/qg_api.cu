@@ -164,6 +164,7 @@ struct qg_handle_s {
     s.d_t0 = d_t0;
     s.far_t0_out = far_t0_out;
     s.variant = far_variant;
+    s.gmajor = 0;
     s.otf = otf ? 1 : 0;
     s.group = group;
     s.pos = d_pos;
@@ -983,15 +984,22 @@ static qg_status autotune_far(qg_handle *h)
 {
   if(h->otf || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
   if(h->mixed) {
-    // one table kernel: its time is the one the coefficient choice compares
+    // one table kernel, in its two task orders (0 and 7, the same sums); the
+    // faster one's time is the one the coefficient choice compares
     launch_set_int(h->d_ints + 7, h->max_delay + h->q + 2 * kTimeBlock, h->stream);
-    QG_TRY(time_far(h, 2, 3, &h->tuned_far_ms));
+    float t0 = 0, t7 = 0;
+    h->far_variant = 0;
+    QG_TRY(time_far(h, 2, 3, &t0));
+    h->far_variant = 7;
+    QG_TRY(time_far(h, 2, 3, &t7));
+    h->far_variant = t7 < t0 ? 7 : 0;
+    h->tuned_far_ms = std::min(t0, t7);
     if(h->tune_coef) QG_TRY(autotune_coef(h));
     h->far_block = -0x7fffffff;
     h->eval_cached = -0x7fffffff;
     return QG_OK;
   }
-  static const int candidates[] = {0, 3, 5, 6};
+  static const int candidates[] = {0, 3, 5, 6, 7, 8};
   const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
   cudaEvent_t e0, e1;
   QG_CUDA(cudaEventCreate(&e0));
@@ -2039,7 +2047,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
       h->group = value;
       h->nG = (h->nT + value - 1) / value;
     } else if(!std::strcmp(key, "far_variant")) {
-      if(value < 0 || value > 6) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..6");
+      if(value < 0 || value > 8) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..8");
       h->far_variant = value;
       h->tune_pending = false;  // an explicit choice is kept
     } else {

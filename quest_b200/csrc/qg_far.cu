@@ -84,7 +84,7 @@ __device__ __forceinline__ void far_body(const FarArgs &a, int task)
   const int lane = threadIdx.x & 31;
   static_assert(VEC == 0 || VEC == 1, "VEC");
   if(task >= a.nT * a.nG) return;  // uniform per warp
-  const int I = task / a.nG, g = task % a.nG;
+  const int I = a.gmajor ? task % a.nT : task / a.nG, g = a.gmajor ? task / a.nT : task % a.nG;
   const int J0 = g * a.group;
   const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
@@ -169,7 +169,7 @@ __device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarSt
 {
   const int lane = threadIdx.x & 31;
   if(task >= a.nT * a.nG) return;  // uniform per warp
-  const int I = task / a.nG, g = task % a.nG;
+  const int I = a.gmajor ? task % a.nT : task / a.nG, g = a.gmajor ? task / a.nT : task % a.nG;
   const int J0 = g * a.group;
   const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
@@ -284,7 +284,7 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
 {
   const int lane = threadIdx.x & 31;
   if(task >= a.nT * a.nG) return;  // uniform per warp
-  const int I = task / a.nG, g = task % a.nG;
+  const int I = a.gmajor ? task % a.nT : task / a.nG, g = a.gmajor ? task / a.nT : task % a.nG;
   const int J0 = g * a.group;
   const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
@@ -416,8 +416,14 @@ __global__ void __launch_bounds__(128) far_kernel_mixed(FarArgs a)
 }
 
 template <int Q, bool LAB>
-static void launch_far_q(const FarArgs &a, cudaStream_t s)
+static void launch_far_q(const FarArgs &a0, cudaStream_t s)
 {
+  // variants 7 and 8 are 0 and 3 with the source-group-major task order
+  FarArgs a = a0;
+  if(a.variant == 7 || a.variant == 8) {
+    a.gmajor = 1;
+    a.variant = a.variant == 7 ? 0 : 3;
+  }
   const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
   if(a.mixed)
     far_kernel_mixed<Q, LAB><<<blocks, 128, 0, s>>>(a);

@@ -81,6 +81,11 @@ struct FarArgs {
   const int *d_t0;      // first step of the block
   int *far_t0_out;      // receives *d_t0 (read by the dot-step kernels)
   int variant;          // kernel variant (same results), see qg_far.cu
+  // task order: 0 target-tile major (a block's warps take consecutive source
+  // groups of one target tile), 1 source-group major (they take one source
+  // group of consecutive target tiles, so they read the same history rows);
+  // the same sums either way
+  int gmajor;
   // on-the-fly coefficients (no table): dot data, constants, and the source
   // tiles per warp (nG = ceil(nT / group) groups)
   int otf;
