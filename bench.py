@@ -429,11 +429,13 @@ def timed_run(sim, warm: int, timed: int, world: int) -> dict:
 
     from quest_b200 import capi
     nonfinite = None
+    # profiling on from the start: its graph instances (with event nodes) are
+    # built during the warm-up, not inside the timed window
+    sim.set_option("profile", 1)
     try:
         sim.run(warm, record=False)
     except capi.NonFiniteError as e:
         nonfinite = e.step
-    sim.set_option("profile", 1)
     sim.kernel_time(reset=True)
     stream = torch.cuda.ExternalStream(capi.lib().qg_stream(sim.h))
     e0 = torch.cuda.Event(enable_timing=True)

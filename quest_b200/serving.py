@@ -167,6 +167,7 @@ class Server:
                 self._retire(rid, now)
         wall = clock() - t0
         lat = np.array([r.latency for r in self.results])
+        ok = np.array([r.latency for r in self.results if not r.failed])
         return {
             "requests": len(self.results),
             "failed": sum(1 for r in self.results if r.failed),
@@ -174,6 +175,8 @@ class Server:
             "busy_s": busy,
             "pair_updates": self.pair_updates_done,
             "pair_updates_per_s": self.pair_updates_done / wall if wall > 0 else 0.0,
+            "p50_s_completed": float(np.percentile(ok, 50)) if ok.size else None,
+            "p99_s_completed": float(np.percentile(ok, 99)) if ok.size else None,
             "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
             "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
         }

@@ -23,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 def test_wait_that_runs_out_returns_an_error_and_the_handle_recovers(golden_weights, oracle_weights):
     wl = I.plain_small(n=200, steps=400, pulse_delay=0.12)
+    wl.dots[:, 6:9] *= 0.1  # a stable case: parity with the oracle over the whole run
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         info = sim.info()
         assert info["fused_step"] == 2  # the step-block form with several blocks
