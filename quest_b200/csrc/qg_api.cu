@@ -1453,6 +1453,7 @@ struct qg_batch_s {
   // launch and around the block's step launches
   bool profile = false;
   bool far_packed = false;  // mixed members: the packed FP32 convolution (same bits)
+  bool far_gmajor = false;  // members' tasks in source-group-major order (same bits)
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double far_ms = 0, step_ms = 0;
   int far_launches = 0, step_launches = 0;
@@ -1565,6 +1566,7 @@ static qg_status batch_rebuild(qg_batch *b)
   for(int e = 0; e < n; ++e) {
     qg_handle *h = b->members[e];
     fa[e] = h->far_args(h->d_ints + 0, h->d_ints + 6);
+    fa[e].gmajor = b->far_gmajor ? 1 : 0;
     sa[e] = h->step_args(false);
     toff[e + 1] = toff[e] + h->nT * h->nG;
     boff[e + 1] = boff[e] + h->step_blocks;
@@ -1658,6 +1660,11 @@ extern "C" qg_status qg_batch_set_option(qg_batch *b, const char *key, int value
   if(!std::strcmp(key, "far_packed")) {
     b->far_packed = value != 0;
     b->dirty = true;  // the block graph holds the kernel
+    return QG_OK;
+  }
+  if(!std::strcmp(key, "far_gmajor")) {
+    b->far_gmajor = value != 0;
+    b->dirty = true;
     return QG_OK;
   }
   return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_set_option: unknown key '%s'", key);
