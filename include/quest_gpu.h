@@ -239,7 +239,9 @@ qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks
  * members: 1 = the FP32 convolution with packed pairs, 0 = scalar; same
  * results), "far_gmajor" (1 = each member's far tasks in source-group-major
  * order, so a thread block's warps read the same history rows; same
- * results). */
+ * results), "mid_pipe" (1 = the step launches fetch several mid-range pair
+ * entries per thread before summing them, which helps members with long
+ * mid lists; same results). */
 qg_status qg_batch_set_option(qg_batch *b, const char *key, int value);
 /* Device time in milliseconds of the batch's far-pair launches and step
  * launches (each nullable), accumulated while "profile" is on. */

@@ -1454,6 +1454,7 @@ struct qg_batch_s {
   bool profile = false;
   bool far_packed = false;  // mixed members: the packed FP32 convolution (same bits)
   bool far_gmajor = false;  // members' tasks in source-group-major order (same bits)
+  bool mid_pipe = false;    // step launches stage mid entries several at a time (same bits)
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double far_ms = 0, step_ms = 0;
   int far_launches = 0, step_launches = 0;
@@ -1590,7 +1591,7 @@ static qg_status batch_rebuild(qg_batch *b)
     launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->mixed ? (b->far_packed ? 2 : 1) : 0,
                      b->far_grid, b->stream);
     for(int k = 0; k < kTimeBlock; ++k)
-      launch_step_batch(b->d_step, b->d_block_off, n, b->total_blocks, b->n_time, k, b->stream);
+      launch_step_batch(b->d_step, b->d_block_off, n, b->total_blocks, b->n_time, k, b->mid_pipe, b->stream);
     QG_CUDA(cudaStreamEndCapture(b->stream, &g));
     QG_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
     cudaGraphDestroy(g);
@@ -1617,7 +1618,7 @@ extern "C" qg_status qg_batch_run(qg_batch *b, int n_blocks)
                      b->far_grid, b->stream);
     QG_CUDA(cudaEventRecord(b->ev[1], b->stream));
     for(int k = 0; k < kTimeBlock; ++k)
-      launch_step_batch(b->d_step, b->d_block_off, nm0, b->total_blocks, b->n_time, k, b->stream);
+      launch_step_batch(b->d_step, b->d_block_off, nm0, b->total_blocks, b->n_time, k, b->mid_pipe, b->stream);
     QG_CUDA(cudaEventRecord(b->ev[2], b->stream));
     QG_CUDA(cudaEventSynchronize(b->ev[2]));
     float f = 0, g = 0;
@@ -1664,6 +1665,11 @@ extern "C" qg_status qg_batch_set_option(qg_batch *b, const char *key, int value
   }
   if(!std::strcmp(key, "far_gmajor")) {
     b->far_gmajor = value != 0;
+    b->dirty = true;
+    return QG_OK;
+  }
+  if(!std::strcmp(key, "mid_pipe")) {
+    b->mid_pipe = value != 0;
     b->dirty = true;
     return QG_OK;
   }

@@ -195,8 +195,9 @@ void launch_gather_bad(const StepArgs *args, int n, int *out, void *stream);
 constexpr int kFlagStride = 32;
 void launch_step_block(const StepArgs &a, int k0, int k1, int nblocks, unsigned *flags, void *stream);
 int step_block_max_blocks(int q, int mid_cache, int hist_cap);
+// pipe: the mid list staged with several entries' loads in flight (same sums)
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
-                       int k, void *stream);
+                       int k, bool pipe, void *stream);
 
 // Launchers (defined in the .cu files).
 void launch_table_build(const TableArgs &a, int q, void *stream);

@@ -405,6 +405,34 @@ __device__ __forceinline__ double2 mid_old(const StepArgs &a, int e, int t, int 
   return mid_old_sum(a, d, t, a.mid_coef + (long long)e * (a.q + 1), 1, v);
 }
 
+// mid_old of entries [c0, c1) (at most kMidChunk) into out[e - c0], each
+// thread taking entries threadIdx.x + j * blockDim.x.  A thread's partners
+// and delays are fetched first, then its entries' history samples two
+// entries ahead of the sums, so their memory latencies overlap; every
+// entry's sum is mid_old's, the same operations in the same order.
+__device__ __forceinline__ void mid_old_stage(const StepArgs &a, int c0, int c1, int t, int tslot, double2 *out)
+{
+  constexpr int U = kMidChunk / (32 * kParts);
+  static_assert(U * 32 * kParts == kMidChunk, "chunk = U entries per thread");
+  int b[U], d[U];
+#pragma unroll
+  for(int j = 0; j < U; ++j) {
+    const int e = c0 + threadIdx.x + j * 32 * kParts;
+    b[j] = e < c1 ? a.mid_idx[e] : 0;
+    d[j] = e < c1 ? a.mid_delay[e] : kTimeBlock;
+  }
+  double2 v0[kMaxOrder + 1], v1[kMaxOrder + 1];
+  mid_old_fetch<true>(a, b[0], d[0], t, tslot, v0);
+#pragma unroll
+  for(int j = 0; j < U; ++j) {
+    double2(&cur)[kMaxOrder + 1] = (j & 1) ? v1 : v0;
+    double2(&nxt)[kMaxOrder + 1] = (j & 1) ? v0 : v1;
+    if(j + 1 < U) mid_old_fetch<true>(a, b[j + 1], d[j + 1], t, tslot, nxt);
+    const int e = c0 + threadIdx.x + j * 32 * kParts;
+    if(e < c1) out[e - c0] = mid_old_sum(a, d[j], t, a.mid_coef + (long long)e * (a.q + 1), 1, cur);
+  }
+}
+
 // M_new of dot idx; prev(b) = rho01 of partner b at step t-1.
 template <class Prev>
 __device__ __forceinline__ double2 mid_new(const StepArgs &a, int j0, int j1, const Prev &prev)
@@ -487,7 +515,10 @@ __device__ __forceinline__ void pc_combine(const double2 (&S)[4], const double2 
   H[1] = make_double2(S[3].x + T[3].x, S[3].y + T[3].y);
 }
 
-template <int NT>
+// PIPE: the mid list staged by mid_old_stage (several entries' loads in
+// flight per thread, 160 registers: 3 blocks per SM) instead of one entry at a
+// time (128 registers: 4 blocks per SM); the same sums either way.
+template <int NT, bool PIPE = false>
 __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int k)
 {
   constexpr int BS = 32;
@@ -531,7 +562,10 @@ __device__ __forceinline__ void step_fused_body(const StepArgs &a, int blk, int 
   const int tslot = ring_slot(t, a.W);
   for(int c0 = E0; c0 < E1; c0 += kMidChunk) {
     const int c1 = min(E1, c0 + kMidChunk);
-    for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_old(a, e, t, tslot);
+    if(PIPE)
+      mid_old_stage(a, c0, c1, t, tslot, midv);
+    else
+      for(int e = c0 + threadIdx.x; e < c1; e += 32 * kParts) midv[e - c0] = mid_old(a, e, t, tslot);
     __syncthreads();
     if(part == 0) {
       const double2 cs = entry_sum(midv, max(my0, c0) - c0, min(my1, c1) - c0);
@@ -567,7 +601,7 @@ __global__ void __launch_bounds__(32 * kParts) step_fused_kernel(StepArgs a, int
 }
 
 // Many ensembles, one launch: block_off[e] = first 32-dot block of ensemble e.
-template <int NT>
+template <int NT, bool PIPE>
 __global__ void __launch_bounds__(32 * kParts) step_batch_kernel(const StepArgs *__restrict__ args,
                                                                  const int *__restrict__ block_off,
                                                                  int n_ens, int k)
@@ -581,18 +615,20 @@ __global__ void __launch_bounds__(32 * kParts) step_batch_kernel(const StepArgs 
     else
       hi = mid - 1;
   }
-  step_fused_body<NT>(args[lo], b - block_off[lo], k);
+  step_fused_body<NT, PIPE>(args[lo], b - block_off[lo], k);
 }
 
 void launch_step_batch(const StepArgs *args, const int *block_off, int n_ens, int total_blocks, int n_time,
-                       int k, void *stream)
+                       int k, bool pipe, void *stream)
 {
   if(n_ens <= 0 || total_blocks <= 0) return;
   cudaStream_t s = (cudaStream_t)stream;
   if(n_time == 22)
-    step_batch_kernel<22><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
+    pipe ? step_batch_kernel<22, true><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k)
+         : step_batch_kernel<22, false><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
   else
-    step_batch_kernel<0><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
+    pipe ? step_batch_kernel<0, true><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k)
+         : step_batch_kernel<0, false><<<total_blocks, 32 * kParts, 0, s>>>(args, block_off, n_ens, k);
 }
 
 // ---- one launch for a whole 16-step block ------------------------------------

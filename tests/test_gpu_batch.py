@@ -106,3 +106,28 @@ def test_member_going_nonfinite_is_reported_and_the_others_are_unchanged(golden_
     for s in sims:
         batch.remove(s)
         s.close()
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_batch_kernel_options_keep_the_bits(golden_weights, precision):
+    """far_packed (packed FP32 pairs), far_gmajor (source-group-major task
+    order) and mid_pipe (mid entries fetched several at a time) change how the
+    batch's kernels run, not what they sum."""
+    specs = [(31, 70, 0.05, 96, 5.0), (32, 400, 0.04, 96, 20.0), (33, 900, 0.2, 96, 15.0)]
+    states = []
+    for opts in ({}, {"far_packed": 1}, {"far_gmajor": 1}, {"far_packed": 1, "far_gmajor": 1, "mid_pipe": 1}):
+        batch = capi.Batch(4)
+        sims = [capi.Simulation(*ensemble(*s), weights=golden_weights, precision=precision) for s in specs]
+        for s in sims:
+            batch.add(s)
+        for k, v in opts.items():
+            batch.set_option(k, v)
+        batch.run(6)
+        states.append([s.state() for s in sims])
+        for s in sims:
+            batch.remove(s)
+            s.close()
+        batch.close()
+    for other in states[1:]:
+        for a, b in zip(states[0], other):
+            np.testing.assert_array_equal(a, b)
