@@ -715,10 +715,12 @@ def batched_record(args, world, rank, capi_precision, weights) -> dict:
         t0 = time.perf_counter()
         live = list(zip(reqs, sims))
         blocks = 0
+        nonfinite = 0
         while live:
             batch.run(args.blocks_per_round)
             blocks += args.blocks_per_round
             for r, s in [(r, s) for r, s in live if s.next_step >= r.constants.num_timesteps]:
+                nonfinite += s.bad_step() >= 0
                 batch.remove(s)
             live = [(r, s) for r, s in live if s.next_step < r.constants.num_timesteps]
         torch.cuda.synchronize()
@@ -732,6 +734,9 @@ def batched_record(args, world, rank, capi_precision, weights) -> dict:
             "unit": "pair-updates/s", "precision": capi_precision, "wall_s": wall, "blocks": blocks,
             "ensembles": args.ensembles, "N_min": int(ns.min()), "N_max": int(ns.max()), "sum_N2T": total,
             "timing": "wall clock of the whole batch (graph replays, membership changes, retirement)",
+            "nonfinite_members": int(nonfinite),
+            "nonfinite_note": "members whose state overflowed (the reference's domain_error) still run every step: "
+                              "the work per step does not depend on the values",
             "clocks": clocks.summary()}
 
 
