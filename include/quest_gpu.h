@@ -236,12 +236,12 @@ qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks
 /* Batch options: "profile" (1 = each block's kernels launched one by one
  * instead of as the graph, with CUDA events around the far-pair launch and
  * around the step launches; same results), "far_packed" (mixed-precision
- * members: 1 = the FP32 convolution with packed pairs, 0 = scalar; same
- * results), "far_gmajor" (1 = each member's far tasks in source-group-major
- * order, so a thread block's warps read the same history rows; same
- * results), "mid_pipe" (1 = the step launches fetch several mid-range pair
- * entries per thread before summing them, which helps members with long
- * mid lists; same results). */
+ * members: 1 = the FP32 convolution with packed pairs, the default, 0 =
+ * scalar; same results), "far_gmajor" (1 = each member's far tasks in
+ * source-group-major order, so a thread block's warps read the same history
+ * rows, the default; same results), "mid_pipe" (1 = the step launches fetch
+ * several mid-range pair entries per thread before summing them, which helps
+ * members with long mid lists; same results). */
 qg_status qg_batch_set_option(qg_batch *b, const char *key, int value);
 /* Device time in milliseconds of the batch's far-pair launches and step
  * launches (each nullable), accumulated while "profile" is on. */

@@ -1452,8 +1452,11 @@ struct qg_batch_s {
   // "profile": blocks launched without the graph, CUDA events around the far
   // launch and around the block's step launches
   bool profile = false;
-  bool far_packed = false;  // mixed members: the packed FP32 convolution (same bits)
-  bool far_gmajor = false;  // members' tasks in source-group-major order (same bits)
+  // defaults measured on B200 with the 256-ensemble workload: packed FP32
+  // pairs 17.1 against 19.7 ms per far launch, and the source-group-major
+  // order 16.3 (mixed) and 22.5 against 23.9 ms (FP64)
+  bool far_packed = true;   // mixed members: the packed FP32 convolution (same bits)
+  bool far_gmajor = true;   // members' tasks in source-group-major order (same bits)
   bool mid_pipe = false;    // step launches stage mid entries several at a time (same bits)
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double far_ms = 0, step_ms = 0;
