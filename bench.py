@@ -233,6 +233,7 @@ FAR_VARIANTS = {0: "far_kernel<5,false>", 1: "far_kernel_r4<5,false>", 2: "far_k
 # 7 and 8: kernels of 0 and 3 with the source-group-major task order
 FAR_VARIANTS[7] = FAR_VARIANTS[0]
 FAR_VARIANTS[8] = FAR_VARIANTS[3]
+FAR_VARIANTS[9] = "far_kernel_bulk<5,false>"
 TRAFFIC_NOTE = ("DRAM bytes need a profiler capture; they are not measured inside this run (null). "
                 "The committed ncu summaries of the same kernel give them.")
 

@@ -308,13 +308,17 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "profile" (1 = CUDA events around the far-pair kernel and the step
  * kernels: event nodes inside the block graphs, or around each launch when
  * "graph" is 0),
- * "far_variant" (0..8: resource shape and task order of the far-pair
+ * "far_variant" (0..9: resource shape and task order of the far-pair
  *   kernel, same results; 7 and 8 are 0 and 3 with each block's warps on one
  *   source group of consecutive target tiles; the first qg_run of an FP64
  *   table handle of 512 dots or more picks the fastest of 0, 3, 5, 6, 7 and
- *   8 by timing launches of each, unless a variant was set; mixed-precision
- *   table handles choose between the task orders 0 and 7 the same way; batch
- *   members are not timed, the batch kernel having its own),
+ *   8 and 9 (9: the table staged by bulk-copy-engine copies on an mbarrier)
+ *   by timing launches of each, unless a variant was set; mixed-precision
+ *   table handles choose between the task orders 0 and 7 the same way; the
+ *   choice is remembered for the process, and later handles of the same kind
+ *   (device, size, order, frame, precision, coefficient mode) take it
+ *   without timing; batch members are not timed, the batch kernel having its
+ *   own),
  * "autotune" (1 = time the far-kernel variants again now; at a block
  *   boundary between runs),
  * "far_group" (source tiles each far-kernel warp sums before writing its

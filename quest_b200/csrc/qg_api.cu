@@ -14,6 +14,9 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "qg_internal.h"
@@ -165,6 +168,7 @@ struct qg_handle_s {
     s.far_t0_out = far_t0_out;
     s.variant = far_variant;
     s.gmajor = 0;
+    s.d_bad = d_ints + 2;
     s.otf = otf ? 1 : 0;
     s.group = group;
     s.pos = d_pos;
@@ -921,6 +925,8 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
 // fastest is kept.  The history
 // is whatever the handle holds (its values do not change the work), and the
 // far field and partials are recomputed by the next run.
+static qg_status switch_to_otf(qg_handle *h);
+
 static qg_status time_far(qg_handle *h, int rounds_untimed, int rounds_timed, float *best_ms)
 {
   cudaEvent_t e0, e1;
@@ -965,6 +971,18 @@ static qg_status autotune_coef(qg_handle *h)
     return st;
   }
   // the on-the-fly kernel is faster: keep it, return the table's memory
+  QG_TRY(switch_to_otf(h));
+  h->tuned_far_ms = otf_ms;
+  return QG_OK;
+}
+
+// A table handle moves to on-the-fly coefficients (the QG_COEF_TUNED choice)
+// and frees its table.
+static qg_status switch_to_otf(qg_handle *h)
+{
+  h->otf = true;
+  h->group = (h->nT + 15) / 16;
+  h->nG = (h->nT + h->group - 1) / h->group;
   QG_CUDA(cudaStreamSynchronize(h->stream));
   for(void *p : {(void *)h->d_delay, (void *)h->d_coef, (void *)h->d_coef32}) {
     if(!p) continue;
@@ -976,7 +994,6 @@ static qg_status autotune_coef(qg_handle *h)
   h->d_delay = nullptr;
   h->d_coef = nullptr;
   h->d_coef32 = nullptr;
-  h->tuned_far_ms = otf_ms;
   return QG_OK;
 }
 
@@ -999,7 +1016,7 @@ static qg_status autotune_far(qg_handle *h)
     h->eval_cached = -0x7fffffff;
     return QG_OK;
   }
-  static const int candidates[] = {0, 3, 5, 6, 7, 8};
+  static const int candidates[] = {0, 3, 5, 6, 7, 8, 9};
   const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
   cudaEvent_t e0, e1;
   QG_CUDA(cudaEventCreate(&e0));
@@ -1038,6 +1055,49 @@ static qg_status autotune_far(qg_handle *h)
   if(h->tune_coef) QG_TRY(autotune_coef(h));
   h->far_block = -0x7fffffff;
   h->eval_cached = -0x7fffffff;
+  return QG_OK;
+}
+
+// The autotuner's choices, remembered for the process: handles of the same
+// kind (device, tiles, order, frame, precision, coefficient mode) take the
+// first one's choice without timing again.
+struct TuneKey {
+  int device, nT, q, frame, mixed, tune_coef;
+  bool operator<(const TuneKey &o) const
+  {
+    return std::tie(device, nT, q, frame, mixed, tune_coef) < std::tie(o.device, o.nT, o.q, o.frame, o.mixed,
+                                                                         o.tune_coef);
+  }
+};
+struct TuneChoice {
+  int variant;
+  float far_ms;
+  bool otf;
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneChoice> g_tune;
+
+static qg_status switch_to_otf(qg_handle *h);
+
+static qg_status autotune_cached(qg_handle *h, bool force)
+{
+  if(h->otf || h->nT < 16) return QG_OK;
+  const TuneKey key{h->device, h->nT, h->q, h->params.frame, h->mixed ? 1 : 0, h->tune_coef ? 1 : 0};
+  if(!force) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if(it != g_tune.end()) {
+      h->far_variant = it->second.variant;
+      h->tuned_far_ms = it->second.far_ms;
+      if(it->second.otf) QG_TRY(switch_to_otf(h));
+      h->far_block = -0x7fffffff;
+      h->eval_cached = -0x7fffffff;
+      return QG_OK;
+    }
+  }
+  QG_TRY(autotune_far(h));
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[key] = TuneChoice{h->far_variant, h->tuned_far_ms, h->otf};
   return QG_OK;
 }
 
@@ -1381,7 +1441,7 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
     // at any step: it only clobbers the far field and partials, which the
     // run recomputes (far_block is invalidated)
     h->tune_pending = false;
-    QG_TRY(autotune_far(h));
+    QG_TRY(autotune_cached(h, false));
   }
   const int t_start = h->next_step;
   h->eval_cached = -0x7fffffff;
@@ -1424,6 +1484,8 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   h->next_step = t_start + n_steps;
   if(bad == -2)
     return qg_fail(QG_ERR_CUDA, "qg_run: a wait in the step-block kernel timed out");
+  if(bad == -3)
+    return qg_fail(QG_ERR_CUDA, "qg_run: a wait for the far kernel's bulk table copies timed out");
   if(bad < 0)
     return qg_fail(QG_ERR_CUDA, "qg_run: internal scheduling error (far block or trajectory row)");
   if(bad != kBadNone) {
@@ -2070,7 +2132,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
       h->group = value;
       h->nG = (h->nT + value - 1) / value;
     } else if(!std::strcmp(key, "far_variant")) {
-      if(value < 0 || value > 8) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..8");
+      if(value < 0 || value > 9) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..9");
       h->far_variant = value;
       h->tune_pending = false;  // an explicit choice is kept
     } else {
@@ -2102,7 +2164,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
     if(value) {
       for(int i = 0; i < qg_handle_s::kProfRing; ++i) QG_TRY(collect_prof(h, i));
       h->tune_pending = false;
-      QG_TRY(autotune_far(h));
+      QG_TRY(autotune_cached(h, true));
       for(auto &g : h->graph)
         if(g) {
           cudaGraphExecDestroy(g);

@@ -249,6 +249,146 @@ __device__ __forceinline__ void far_body_async(const FarArgs &a, int task, FarSt
 constexpr int kFarStages = 3;
 static_assert(4 * sizeof(FarStage<kMaxOrder, kFarStages>) <= 227 * 1024, "far stage buffers");
 
+// ---- table staged by the bulk-copy (TMA) engine ---------------------------------
+// Variant 9: for each source, lane 0 asks the copy engine for the source's
+// q+1 coefficient rows (32 lanes x 16 B = 512 B each) and its delay row
+// (128 B) with cp.async.bulk, completing on a per-stage mbarrier, P - 1
+// sources ahead; the lanes wait on the barrier's phase and read their entries
+// from shared memory.  The copies are plain global -> own shared memory (no
+// cluster multicast); sizes and addresses are multiples of 16 B (rows start
+// on 512-B and 128-B boundaries of 256-B aligned allocations).  Every wait is
+// bounded: one that runs out sets *a.d_bad = -3, waits (bounded again) for the
+// copies still in flight into this warp's buffers, and ends the warp.
+constexpr int kBulkSpins = 1 << 20;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// true once the barrier's phase with the given parity has completed, false
+// when kBulkSpins polls ran out
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+  for(int spin = 0; spin < kBulkSpins; ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if(done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar,
+                                         unsigned long long pol)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+
+template <int Q, bool LAB, int P, int K = kTimeBlock>
+__device__ __forceinline__ void far_body_bulk(const FarArgs &a, int task, FarStage<Q, P> &st,
+                                              unsigned long long *bar)
+{
+  const int lane = threadIdx.x & 31;
+  if(task >= a.nT * a.nG) return;  // uniform per warp; the barriers are this warp's alone
+  const int I = a.gmajor ? task % a.nT : task / a.nG, g = a.gmajor ? task / a.nT : task % a.nG;
+  const int J0 = g * a.group;
+  const int nJ = min(a.group, a.nT - J0);
+  const int t0 = *a.d_t0;
+  if(task == 0 && lane == 0) *a.far_t0_out = t0;
+  const int W = a.W;
+  unsigned long long pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  constexpr unsigned kStageBytes = (Q + 1) * kTile * sizeof(double2) + kTile * sizeof(int);
+
+  if(lane == 0) {
+#pragma unroll
+    for(int p = 0; p < P; ++p) mbar_init(&bar[p], 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+
+  double2 acc[K];
+#pragma unroll
+  for(int k = 0; k < K; ++k) acc[k] = make_double2(0.0, 0.0);
+
+  const long long tile0 = (long long)I * a.nT + J0;
+  const int iters = nJ * kTile;
+  // source `it` goes to stage it % P; its barrier completes phase it / P
+  auto issue = [&](int it) {  // lane 0
+    const int slot = it % P;
+    const long long tile = tile0 + it / kTile;
+    const int j = it % kTile;
+    mbar_arrive_expect_tx(&bar[slot], kStageBytes);
+#pragma unroll
+    for(int i = 0; i <= Q; ++i)
+      bulk_g2s(&st.coef[slot][i][0], a.coef + (tile * (Q + 1) + i) * kTilePairs + j * kTile,
+               kTile * sizeof(double2), &bar[slot], pol);
+    bulk_g2s(&st.delay[slot][0], a.delay + tile * kTilePairs + j * kTile, kTile * sizeof(int), &bar[slot], pol);
+  };
+  if(lane == 0) {
+#pragma unroll
+    for(int p = 0; p < P - 1; ++p)
+      if(p < iters) issue(p);
+  }
+  int it = 0;
+  bool ok = true;
+  for(; it < iters; ++it) {
+    // the stage of source it - 1 was read by every lane (syncwarp below)
+    if(lane == 0 && it + P - 1 < iters) issue(it + P - 1);
+    const int slot = it % P;
+    ok = __all_sync(0xffffffffu, mbar_wait(&bar[slot], (unsigned)((it / P) & 1)));
+    if(!ok) break;
+    const int d = st.delay[slot][lane];
+    double2 c[Q + 1];
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) c[i] = st.coef[slot][i][lane];
+    __syncwarp();
+    if(d >= kTimeBlock) {
+      const int ib = (J0 + it / kTile) * kTile + (it % kTile);
+      const int tau0 = t0 - d - Q;
+      int slot0 = tau0 % W;
+      if(slot0 < 0) slot0 += W;
+      window_conv<Q, LAB, K>(a.ring + (long long)ib * a.stride, slot0, tau0, c, acc);
+    }
+  }
+  if(!ok) {
+    // record the failure, let the copies already issued into this warp's
+    // stages (sources it .. it + P - 1) land, then stop
+    if(lane == 0) atomicMin(a.d_bad, -3);
+    for(int r = it; r < min(iters, it + P); ++r) mbar_wait(&bar[r % P], (unsigned)((r / P) & 1));
+    return;
+  }
+  group_partials_reduce<K>(a, I, g, acc);
+}
+
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128) far_kernel_bulk(FarArgs a)
+{
+  extern __shared__ double2 far_smem[];
+  __shared__ unsigned long long bars[4][kFarStages];
+  FarStage<Q, kFarStages> *st = reinterpret_cast<FarStage<Q, kFarStages> *>(far_smem);
+  far_body_bulk<Q, LAB, kFarStages>(a, warp_task(), st[threadIdx.x >> 5], bars[threadIdx.x >> 5]);
+}
+
 // Variant 6 is held to 128 registers (4 blocks, 16 warps per SM); uncapped
 // it takes 132 and fits 3 blocks.
 template <int Q, bool LAB, int VEC>
@@ -431,7 +571,7 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
-  else if(a.variant >= 3 && a.variant <= 6) {
+  else if((a.variant >= 3 && a.variant <= 6) || a.variant == 9) {
     // 38 KB at q = 5, 51 KB at q = 7 (above the 48 KB default: opt in);
     // variant 5 keeps one more stage
     const size_t smem = 4 * sizeof(FarStage<Q, kFarStages>), smem5 = 4 * sizeof(FarStage<Q, kFarStages + 1>);
@@ -443,6 +583,7 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem5);
       cudaFuncSetAttribute(far_kernel_async<Q, LAB, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(far_kernel_bulk<Q, LAB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if(dev < 64) attr_set[dev] = true;
     }
     if(a.variant == 3)
@@ -451,6 +592,8 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
       far_kernel_async<Q, LAB, 1><<<blocks, 128, smem, s>>>(a);
     else if(a.variant == 6)
       far_kernel_async<Q, LAB, 3><<<blocks, 128, smem, s>>>(a);
+    else if(a.variant == 9)
+      far_kernel_bulk<Q, LAB><<<blocks, 128, smem, s>>>(a);
     else
       far_kernel_async<Q, LAB, 2><<<blocks, 128, smem5, s>>>(a);
   }

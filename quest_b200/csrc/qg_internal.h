@@ -86,6 +86,7 @@ struct FarArgs {
   // group of consecutive target tiles, so they read the same history rows);
   // the same sums either way
   int gmajor;
+  int *d_bad;           // a far-kernel wait that ran out sets it to -3
   // on-the-fly coefficients (no table): dot data, constants, and the source
   // tiles per warp (nG = ceil(nT / group) groups)
   int otf;

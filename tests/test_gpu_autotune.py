@@ -43,14 +43,14 @@ def test_tuned_choice_is_reported_and_agrees_with_both_forms(golden_weights, pre
 def test_far_variants_are_timed_and_identical(golden_weights):
     wl = I.plain_table(seed=2, n=1024, steps=64, pulse_delay=0.3)
     res = []
-    for v in (None, 0, 3, 5, 6, 7, 8):
+    for v in (None, 0, 3, 5, 6, 7, 8, 9):
         with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights,
                              coef_mode=capi.COEF_TABLE) as sim:
             if v is not None:
                 sim.set_option("far_variant", v)
             res.append(sim.run(64))
             if v is None:
-                assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8)
+                assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8, 9)
                 assert sim.get_option("tuned_far_us") > 0
     for r in res[1:]:
         np.testing.assert_array_equal(r, res[0])

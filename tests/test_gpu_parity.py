@@ -286,7 +286,7 @@ def test_far_kernel_variants_agree_bitwise(golden_weights):
     task order; their arithmetic, and so their results, are identical."""
     wl = stable_small(300, 160, 0.06)
     outs = []
-    variants = (0, 1, 2, 3, 4, 5, 6, 7, 8)
+    variants = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9)
     for v in variants:
         with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
             sim.set_option("far_variant", v)
@@ -303,7 +303,7 @@ def test_far_autotuner_runs_at_the_first_run_and_keeps_an_explicit_choice(golden
     outs = []
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         outs.append(sim.run(48))
-        assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8)
+        assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8, 9)
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         sim.set_option("far_variant", 4)
         outs.append(sim.run(48))
