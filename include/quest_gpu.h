@@ -311,10 +311,11 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "far_variant" (0..9: resource shape and task order of the far-pair
  *   kernel, same results; 7 and 8 are 0 and 3 with each block's warps on one
  *   source group of consecutive target tiles; the first qg_run of an FP64
- *   table handle of 512 dots or more picks the fastest of 0, 3, 5, 6, 7 and
- *   8 and 9 (9: the table staged by bulk-copy-engine copies on an mbarrier)
+ *   table handle of 512 dots or more picks the fastest of 0, 3, 5, 6, 7, 8
+ *   and 9 (9: the table staged by bulk-copy-engine copies on an mbarrier)
  *   by timing launches of each, unless a variant was set; mixed-precision
- *   table handles choose between the task orders 0 and 7 the same way; the
+ *   table handles choose the same way among 0, 7 (its kernel at 150
+ *   registers, target-tile and source-group major) and 1, 8 (at 128); the
  *   choice is remembered for the process, and later handles of the same kind
  *   (device, size, order, frame, precision, coefficient mode) take it
  *   without timing; batch members are not timed, the batch kernel having its

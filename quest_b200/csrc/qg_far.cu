@@ -555,19 +555,35 @@ __global__ void __launch_bounds__(128) far_kernel_mixed(FarArgs a)
   far_body_mixed<Q, LAB, kTimeBlock, true>(a, warp_task());
 }
 
+// The same held to 128 registers (4 blocks, 16 warps per SM, against 3):
+// more warps to cover the window gathers' latency; same results.
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128, 4) far_kernel_mixed_r4(FarArgs a)
+{
+  far_body_mixed<Q, LAB, kTimeBlock, true>(a, warp_task());
+}
+
 template <int Q, bool LAB>
 static void launch_far_q(const FarArgs &a0, cudaStream_t s)
 {
-  // variants 7 and 8 are 0 and 3 with the source-group-major task order
   FarArgs a = a0;
+  const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
+  if(a.mixed) {
+    // mixed precision: 0 and 7 at 150 registers, 1 and 8 held to 128; 7 and
+    // 8 in the source-group-major task order
+    a.gmajor = a0.variant == 7 || a0.variant == 8;
+    if(a0.variant == 1 || a0.variant == 8)
+      far_kernel_mixed_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
+    else
+      far_kernel_mixed<Q, LAB><<<blocks, 128, 0, s>>>(a);
+    return;
+  }
+  // variants 7 and 8 are 0 and 3 with the source-group-major task order
   if(a.variant == 7 || a.variant == 8) {
     a.gmajor = 1;
     a.variant = a.variant == 7 ? 0 : 3;
   }
-  const unsigned blocks = (unsigned)((a.nT * a.nG + 3) / 4);
-  if(a.mixed)
-    far_kernel_mixed<Q, LAB><<<blocks, 128, 0, s>>>(a);
-  else if(a.variant == 1)
+  if(a.variant == 1)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
