@@ -315,7 +315,8 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  *   and 9 (9: the table staged by bulk-copy-engine copies on an mbarrier)
  *   by timing launches of each, unless a variant was set; mixed-precision
  *   table handles choose the same way among 0, 7 (its kernel at 150
- *   registers, target-tile and source-group major) and 1, 8 (at 128); the
+ *   registers, target-tile and source-group major) and 1, 8 (at 128);
+ *   on-the-fly handles take 7 for the source-group-major order; the
  *   choice is remembered for the process, and later handles of the same kind
  *   (device, size, order, frame, precision, coefficient mode) take it
  *   without timing; batch members are not timed, the batch kernel having its

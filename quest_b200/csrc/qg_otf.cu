@@ -31,7 +31,8 @@ __device__ __forceinline__ void far_body_otf(const FarArgs &a, int task)
   const int lane = threadIdx.x & 31;
   const int n_tiles = a.tile_n > 0 ? a.tile_n : a.nT;  // target tiles of this launch
   if(task >= n_tiles * a.nG) return;                   // uniform per warp
-  const int I = a.tile_lo + task / a.nG, g = task % a.nG;
+  const int I = a.tile_lo + (a.gmajor ? task % n_tiles : task / a.nG);
+  const int g = a.gmajor ? task / n_tiles : task % a.nG;
   const int J0 = g * a.group;
   const int nJ = min(a.group, a.nT - J0);
   const int t0 = *a.d_t0;
@@ -124,9 +125,11 @@ static void launch_otf_q(const FarArgs &a, cudaStream_t s)
   }
 }
 
-void launch_far_otf(const FarArgs &a, void *stream)
+void launch_far_otf(const FarArgs &a0, void *stream)
 {
-  if(a.nT <= 0) return;
+  if(a0.nT <= 0) return;
+  FarArgs a = a0;
+  a.gmajor = a0.variant == 7;  // source-group-major task order (same sums)
   cudaStream_t s = (cudaStream_t)stream;
   if(a.frame == 0) {
     if(a.mixed)
