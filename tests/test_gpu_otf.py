@@ -195,3 +195,18 @@ def test_otf_n65536_evaluate_sampled_targets_against_oracle(golden_weights):
     ref = O.history_evaluate_targets(wl.dots, wl.constants, np.ascontiguousarray(hist.T), t_lo, step, targets)
     assert np.all(np.abs(ref) > 0)
     assert rel_err(ref, got[targets]) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_otf_task_orders_agree_bitwise(golden_weights, precision):
+    """far_variant 7 runs the on-the-fly kernel's tasks source-group major;
+    each target's sums are unchanged."""
+    wl = stable(1000, 96, 0.1)
+    outs = []
+    for v in (None, 7):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights, precision=precision,
+                             coef_mode=capi.COEF_ON_THE_FLY) as sim:
+            if v is not None:
+                sim.set_option("far_variant", v)
+            outs.append(sim.run(96))
+    np.testing.assert_array_equal(outs[0], outs[1])
