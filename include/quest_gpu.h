@@ -243,6 +243,14 @@ qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks
  * several mid-range pair entries per thread before summing them, which helps
  * members with long mid lists; same results). */
 qg_status qg_batch_set_option(qg_batch *b, const char *key, int value);
+/* Reads a batch option back: "far_packed", "far_gmajor", "mid_pipe",
+ * "profile", "tuned_far_us" (the far launch's time the batch's autotuner
+ * measured for its choice, microseconds; 0 if it did not run).  The
+ * autotuner times the far launch's forms that sum the same terms (far_packed
+ * for mixed members x far_gmajor) at the batch's first qg_batch_run and keeps
+ * the fastest, unless one was set; "autotune" (1) asks for it again at the
+ * next run. */
+qg_status qg_batch_get_option(const qg_batch *b, const char *key, int *value);
 /* Device time in milliseconds of the batch's far-pair launches and step
  * launches (each nullable), accumulated while "profile" is on. */
 qg_status qg_batch_kernel_time(qg_batch *b, int reset, double *far_ms, int *far_launches, double *step_ms,

@@ -76,7 +76,7 @@ EXPORTS = ["qg_last_error", "qg_version", "qg_pc_weights", "qg_create", "qg_dest
            "qg_batch_create", "qg_batch_destroy", "qg_batch_add", "qg_batch_remove", "qg_batch_run",
            "qg_batch_size", "qg_batch_set_option", "qg_batch_kernel_time", "qg_checkpoint_size",
            "qg_checkpoint_save", "qg_checkpoint_load", "qg_shard_create", "qg_shard_layout", "qg_shard_step",
-           "qg_shard_import"]
+           "qg_shard_import", "qg_batch_get_option"]
 
 _lib = None
 
@@ -124,6 +124,7 @@ def lib():
         L.qg_batch_run.argtypes = [vp, ctypes.c_int]
         L.qg_batch_size.argtypes = [vp, ip, ip, ip]
         L.qg_batch_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.qg_batch_get_option.argtypes = [vp, ctypes.c_char_p, ip]
         L.qg_shard_create.argtypes = [ctypes.POINTER(QgDot), ctypes.c_int, ctypes.POINTER(QgPulse),
                                       ctypes.POINTER(QgParams), ctypes.POINTER(QgWeights), ctypes.c_int,
                                       ctypes.c_int, ctypes.POINTER(vp)]
@@ -341,6 +342,11 @@ class Batch:
 
     def set_option(self, key: str, value: int) -> None:
         _check(lib().qg_batch_set_option(self.b, key.encode(), int(value)))
+
+    def get_option(self, key: str) -> int:
+        v = ctypes.c_int()
+        _check(lib().qg_batch_get_option(self.b, key.encode(), ctypes.byref(v)))
+        return v.value
 
     def kernel_times(self, reset: bool = False) -> tuple[float, int, float, int]:
         """(far ms, far launches, step ms, step launches) while "profile" is on."""

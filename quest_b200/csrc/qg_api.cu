@@ -1527,6 +1527,10 @@ struct qg_batch_s {
   bool far_packed = true;   // mixed members: the packed FP32 convolution (same bits)
   bool far_gmajor = true;   // members' tasks in source-group-major order (same bits)
   bool mid_pipe = false;    // step launches stage mid entries several at a time (same bits)
+  // the far launch's forms (far_packed x far_gmajor) are timed at the first
+  // run, unless set explicitly; tuned_far_us reads the winner's time back
+  bool tune_pending = true;
+  float tuned_far_ms = 0;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double far_ms = 0, step_ms = 0;
   int far_launches = 0, step_launches = 0;
@@ -1679,12 +1683,58 @@ static qg_status batch_rebuild(qg_batch *b)
   return QG_OK;
 }
 
+// The batch's autotuner: its far launch in each of the forms that sum the
+// same terms (mixed: scalar or packed FP32 pairs; both: target-tile or
+// source-group-major task order), one untimed and two timed launches each,
+// the fastest kept.  The launch recomputes the far field of every member's
+// next block from history the run has not touched yet, so timing it changes
+// nothing the run then computes.
+static qg_status batch_autotune(qg_batch *b)
+{
+  b->tune_pending = false;
+  const int n = (int)b->members.size();
+  cudaEvent_t e0, e1;
+  QG_CUDA(cudaEventCreate(&e0));
+  QG_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  bool best_p = b->far_packed, best_g = b->far_gmajor;
+  for(int packed = 0; packed < (b->mixed ? 2 : 1); ++packed)
+    for(int gmajor = 0; gmajor < 2; ++gmajor) {
+      b->far_packed = packed != 0;
+      b->far_gmajor = gmajor != 0;
+      QG_TRY(batch_rebuild(b));  // the members' FarArgs carry the task order
+      float t = 1e30f;
+      for(int r = 0; r < 3; ++r) {
+        QG_CUDA(cudaEventRecord(e0, b->stream));
+        launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->mixed ? (b->far_packed ? 2 : 1) : 0,
+                         b->far_grid, b->stream);
+        QG_CUDA(cudaEventRecord(e1, b->stream));
+        QG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if(r > 0) t = std::min(t, ms);
+      }
+      if(t < best) {
+        best = t;
+        best_p = b->far_packed;
+        best_g = b->far_gmajor;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->far_packed = best_p;
+  b->far_gmajor = best_g;
+  b->tuned_far_ms = best;
+  return batch_rebuild(b);
+}
+
 extern "C" qg_status qg_batch_run(qg_batch *b, int n_blocks)
 {
   if(!b || n_blocks < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_run: bad argument");
   QG_CUDA(cudaSetDevice(b->device));
   if(b->dirty) QG_TRY(batch_rebuild(b));
   if(b->members.empty()) return QG_OK;
+  if(b->tune_pending && n_blocks > 0) QG_TRY(batch_autotune(b));
   const int nm0 = (int)b->members.size();
   for(int i = 0; i < n_blocks; ++i) {
     if(!b->profile) {
@@ -1740,11 +1790,17 @@ extern "C" qg_status qg_batch_set_option(qg_batch *b, const char *key, int value
   if(!std::strcmp(key, "far_packed")) {
     b->far_packed = value != 0;
     b->dirty = true;  // the block graph holds the kernel
+    b->tune_pending = false;  // an explicit choice is kept
     return QG_OK;
   }
   if(!std::strcmp(key, "far_gmajor")) {
     b->far_gmajor = value != 0;
     b->dirty = true;
+    b->tune_pending = false;
+    return QG_OK;
+  }
+  if(!std::strcmp(key, "autotune")) {
+    b->tune_pending = value != 0;
     return QG_OK;
   }
   if(!std::strcmp(key, "mid_pipe")) {
@@ -1753,6 +1809,24 @@ extern "C" qg_status qg_batch_set_option(qg_batch *b, const char *key, int value
     return QG_OK;
   }
   return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_set_option: unknown key '%s'", key);
+}
+
+extern "C" qg_status qg_batch_get_option(const qg_batch *b, const char *key, int *value)
+{
+  if(!b || !key || !value) return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_get_option: NULL argument");
+  if(!std::strcmp(key, "far_packed"))
+    *value = b->far_packed ? 1 : 0;
+  else if(!std::strcmp(key, "far_gmajor"))
+    *value = b->far_gmajor ? 1 : 0;
+  else if(!std::strcmp(key, "mid_pipe"))
+    *value = b->mid_pipe ? 1 : 0;
+  else if(!std::strcmp(key, "profile"))
+    *value = b->profile ? 1 : 0;
+  else if(!std::strcmp(key, "tuned_far_us"))
+    *value = (int)(b->tuned_far_ms * 1000.0f + 0.5f);
+  else
+    return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_get_option: unknown key '%s'", key);
+  return QG_OK;
 }
 
 extern "C" qg_status qg_batch_kernel_time(qg_batch *b, int reset, double *far_ms, int *far_launches,

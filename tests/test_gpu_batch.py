@@ -131,3 +131,25 @@ def test_batch_kernel_options_keep_the_bits(golden_weights, precision):
     for other in states[1:]:
         for a, b in zip(states[0], other):
             np.testing.assert_array_equal(a, b)
+
+
+def test_batch_autotuner_times_the_far_forms_and_keeps_the_bits(golden_weights):
+    """The batch's first run times its far launch's forms (packed x task
+    order); the tuned batch's members are still bitwise their solo runs."""
+    specs = [(41, 300, 0.1, 64, 5.0), (42, 800, 0.15, 64, 20.0)]
+    ens = [ensemble(*s) for s in specs]
+    batch = capi.Batch(4)
+    sims = [capi.Simulation(d, p, c, weights=golden_weights, precision=capi.PREC_MIXED) for d, p, c in ens]
+    for s in sims:
+        batch.add(s)
+    batch.run(4)
+    assert batch.get_option("tuned_far_us") > 0
+    assert batch.get_option("far_packed") in (0, 1) and batch.get_option("far_gmajor") in (0, 1)
+    for (d, p, c), sim in zip(ens, sims):
+        with capi.Simulation(d, p, c, weights=golden_weights, precision=capi.PREC_MIXED) as solo_sim:
+            solo_sim.run(64, record=False)
+            np.testing.assert_array_equal(sim.state(), solo_sim.state())
+    for s in sims:
+        batch.remove(s)
+        s.close()
+    batch.close()
