@@ -334,6 +334,11 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "far_group" (source tiles each far-kernel warp sums before writing its
  *   partial, table handles; default 4, mixed precision 2 below 256 tiles;
  *   changes the summation grouping, so results change in the last bits),
+ * "tune_group" (1 = the next qg_run times the far variants and then
+ *   far_group 1, 2, 4 and 8 against the default and keeps the fastest;
+ *   table handles; off by default because the group changes the last bits,
+ *   so a tuned handle's results depend on which group won; the choice is
+ *   remembered for the process like the variant's),
  * "block_step" (1 = the K steps of a block in one cooperative launch, the
  *   default where every 32-dot block fits on the device at once; 0 = one
  *   launch per step; same results),
@@ -349,7 +354,7 @@ qg_status qg_set_option(qg_handle *h, const char *key, int value);
 
 /* Reads an option back: "graph", "profile", "far_variant" (the variant in
  * use, which after the first qg_run is the autotuner's choice), "block_step",
- * "far_group", "wait_limit", "test_skip_post", "coef_mode" (QG_COEF_TABLE or
+ * "far_group", "tune_group", "wait_limit", "test_skip_post", "coef_mode" (QG_COEF_TABLE or
  * QG_COEF_ON_THE_FLY: the form in use), "tuned_far_us" (the far kernel's
  * launch time the autotuner measured for its choice, microseconds; 0 if it
  * did not run).  No reference counterpart (the reference has no options). */

@@ -125,6 +125,7 @@ struct qg_handle_s {
   int far_variant = 3;  // cp.async-staged table (see qg_far.cu); the autotuner may change it
   float tuned_far_ms = 0;  // far-kernel time of the autotuner's choice
   bool tune_coef = false;  // QG_COEF_TUNED: also time the on-the-fly kernel against the table
+  bool tune_group = false;  // "tune_group": also time source tiles per warp 1, 2, 4, 8
   bool tune_pending = false;  // the far-kernel autotuner runs at the first qg_run
   bool profile = false;
   // first bad step as the last batch run read it (qg_bad_step answers from it
@@ -997,6 +998,35 @@ static qg_status switch_to_otf(qg_handle *h)
   return QG_OK;
 }
 
+// Source tiles per far-kernel warp (the "far_group" option): each group
+// writes one partial per target and step, and the partials are then summed
+// over groups, so the group size changes the association of the far sums
+// (results move within rounding, not bit for bit).  The search therefore
+// runs only when asked for ("tune_group"), after the variant is chosen, and
+// keeps the faster of the default and each of 1, 2, 4 and 8 that the
+// handle's partial buffer holds.
+static qg_status autotune_group(qg_handle *h)
+{
+  const int g0 = h->group;
+  int best_g = g0;
+  float best = h->tuned_far_ms;
+  for(int g : {1, 2, 4, 8}) {
+    if(g == g0 || (h->nT + g - 1) / g > h->max_groups) continue;
+    h->group = g;
+    h->nG = (h->nT + g - 1) / g;
+    float t = 0;
+    QG_TRY(time_far(h, 2, 3, &t));
+    if(t < best) {
+      best = t;
+      best_g = g;
+    }
+  }
+  h->group = best_g;
+  h->nG = (h->nT + best_g - 1) / best_g;
+  h->tuned_far_ms = best;
+  return QG_OK;
+}
+
 static qg_status autotune_far(qg_handle *h)
 {
   if(h->otf || h->nT < 16) return QG_OK;  // one kernel, or too small to matter
@@ -1018,6 +1048,7 @@ static qg_status autotune_far(qg_handle *h)
     }
     h->far_variant = best_v;
     h->tuned_far_ms = best;
+    if(h->tune_group) QG_TRY(autotune_group(h));
     if(h->tune_coef) QG_TRY(autotune_coef(h));
     h->far_block = -0x7fffffff;
     h->eval_cached = -0x7fffffff;
@@ -1059,6 +1090,7 @@ static qg_status autotune_far(qg_handle *h)
   QG_CUDA(cudaGetLastError());
   h->far_variant = best_v;
   h->tuned_far_ms = best;
+  if(h->tune_group) QG_TRY(autotune_group(h));
   if(h->tune_coef) QG_TRY(autotune_coef(h));
   h->far_block = -0x7fffffff;
   h->eval_cached = -0x7fffffff;
@@ -1069,15 +1101,15 @@ static qg_status autotune_far(qg_handle *h)
 // kind (device, tiles, order, frame, precision, coefficient mode) take the
 // first one's choice without timing again.
 struct TuneKey {
-  int device, nT, q, frame, mixed, tune_coef;
+  int device, nT, q, frame, mixed, tune_coef, group;
   bool operator<(const TuneKey &o) const
   {
-    return std::tie(device, nT, q, frame, mixed, tune_coef) < std::tie(o.device, o.nT, o.q, o.frame, o.mixed,
-                                                                         o.tune_coef);
+    return std::tie(device, nT, q, frame, mixed, tune_coef, group) <
+           std::tie(o.device, o.nT, o.q, o.frame, o.mixed, o.tune_coef, o.group);
   }
 };
 struct TuneChoice {
-  int variant;
+  int variant, group;
   float far_ms;
   bool otf;
 };
@@ -1089,13 +1121,17 @@ static qg_status switch_to_otf(qg_handle *h);
 static qg_status autotune_cached(qg_handle *h, bool force)
 {
   if(h->otf || h->nT < 16) return QG_OK;
-  const TuneKey key{h->device, h->nT, h->q, h->params.frame, h->mixed ? 1 : 0, h->tune_coef ? 1 : 0};
+  // the group part of the key: 0 when the group is searched, else the one set
+  const TuneKey key{h->device, h->nT,  h->q, h->params.frame, h->mixed ? 1 : 0, h->tune_coef ? 1 : 0,
+                    h->tune_group ? 0 : h->group};
   if(!force) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune.find(key);
     if(it != g_tune.end()) {
       h->far_variant = it->second.variant;
       h->tuned_far_ms = it->second.far_ms;
+      h->group = it->second.group;
+      h->nG = (h->nT + h->group - 1) / h->group;
       if(it->second.otf) QG_TRY(switch_to_otf(h));
       h->far_block = -0x7fffffff;
       h->eval_cached = -0x7fffffff;
@@ -1104,7 +1140,7 @@ static qg_status autotune_cached(qg_handle *h, bool force)
   }
   QG_TRY(autotune_far(h));
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  g_tune[key] = TuneChoice{h->far_variant, h->tuned_far_ms, h->otf};
+  g_tune[key] = TuneChoice{h->far_variant, h->group, h->tuned_far_ms, h->otf};
   return QG_OK;
 }
 
@@ -2198,8 +2234,12 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
     h->profile = value != 0;
   } else if(!std::strcmp(key, "far_variant") || !std::strcmp(key, "block_step") ||
             !std::strcmp(key, "far_group") || !std::strcmp(key, "wait_limit") ||
-            !std::strcmp(key, "test_skip_post")) {
-    if(!std::strcmp(key, "wait_limit")) {
+            !std::strcmp(key, "test_skip_post") || !std::strcmp(key, "tune_group")) {
+    if(!std::strcmp(key, "tune_group")) {
+      if(h->otf) return qg_fail(QG_ERR_UNSUPPORTED, "qg_set_option: tune_group is for table handles");
+      h->tune_group = value != 0;
+      if(h->tune_group) h->tune_pending = true;  // the next run times the groups
+    } else if(!std::strcmp(key, "wait_limit")) {
       if(value < 0) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: wait_limit >= 0 (0: the default)");
       h->spin_limit = value;
     } else if(!std::strcmp(key, "test_skip_post")) {
@@ -2285,6 +2325,8 @@ extern "C" qg_status qg_get_option(const qg_handle *h, const char *key, int *val
     *value = (int)(h->tuned_far_ms * 1000.0f + 0.5f);
   else if(!std::strcmp(key, "test_skip_post"))
     *value = h->skip_post;
+  else if(!std::strcmp(key, "tune_group"))
+    *value = h->tune_group ? 1 : 0;
   else
     return qg_fail(QG_ERR_INVALID_ARG, "qg_get_option: unknown key '%s'", key);
   return QG_OK;

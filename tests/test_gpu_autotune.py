@@ -54,3 +54,31 @@ def test_far_variants_are_timed_and_identical(golden_weights):
                 assert sim.get_option("tuned_far_us") > 0
     for r in res[1:]:
         np.testing.assert_array_equal(r, res[0])
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_group_search_is_reported_and_within_rounding(golden_weights, precision):
+    """"tune_group" adds source tiles per warp (1, 2, 4, 8) to the search: a
+    different association of the far sums, so the tuned handle agrees with
+    the default grouping to rounding and bitwise with the same group set by
+    hand."""
+    wl = I.plain_table(seed=5, n=2048, steps=96, pulse_delay=0.02)
+    wl.dots[:, 6:9] *= 0.1
+
+    def run(**opts):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights, precision=precision,
+                             coef_mode=capi.COEF_TABLE) as sim:
+            for k, v in opts.items():
+                sim.set_option(k, v)
+            r = sim.run(96)
+            return r, sim.get_option("far_group"), sim.get_option("far_variant"), sim.get_option("tune_group")
+
+    default, g0, _, _ = run()
+    tuned, g, v, flag = run(tune_group=1)
+    assert flag == 1 and g in (1, 2, 4, 8, g0)
+    by_hand, g2, _, _ = run(far_group=g, far_variant=v)
+    assert g2 == g
+    np.testing.assert_array_equal(tuned, by_hand)
+    tol = 1e-12 if precision == capi.PREC_FP64 else 1e-6
+    for k in range(2):
+        assert rel_err(tuned[..., k], default[..., k]) < tol
