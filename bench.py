@@ -234,6 +234,7 @@ FAR_VARIANTS = {0: "far_kernel<5,false>", 1: "far_kernel_r4<5,false>", 2: "far_k
 FAR_VARIANTS[7] = FAR_VARIANTS[0]
 FAR_VARIANTS[8] = FAR_VARIANTS[3]
 FAR_VARIANTS[9] = "far_kernel_bulk<5,false>"
+FAR_VARIANTS[10] = FAR_VARIANTS[11] = "far_kernel_wstage<5,false>"
 TRAFFIC_NOTE = ("DRAM bytes need a profiler capture; they are not measured inside this run (null). "
                 "The committed ncu summaries of the same kernel give them.")
 

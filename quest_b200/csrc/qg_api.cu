@@ -2253,7 +2253,7 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
       h->group = value;
       h->nG = (h->nT + value - 1) / value;
     } else if(!std::strcmp(key, "far_variant")) {
-      if(value < 0 || value > 9) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..9");
+      if(value < 0 || value > 11) return qg_fail(QG_ERR_INVALID_ARG, "qg_set_option: far_variant in 0..11");
       h->far_variant = value;
       h->tune_pending = false;  // an explicit choice is kept
     } else {

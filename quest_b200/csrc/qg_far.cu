@@ -389,6 +389,165 @@ __global__ void __launch_bounds__(128) far_kernel_bulk(FarArgs a)
   far_body_bulk<Q, LAB, kFarStages>(a, warp_task(), st[threadIdx.x >> 5], bars[threadIdx.x >> 5]);
 }
 
+// ---- history windows staged in shared memory --------------------------------
+// Variants 10 and 11 (11: source-group-major order): each source's history
+// window union staged in shared memory.  For source b the 32 lanes' windows
+// (one per target's delay d_l) cover steps t0 - max_l d_l - q ..
+// t0 - min_l d_l + K - 1 of b's ring row: one contiguous run of at most
+// kWinCap samples for compact target tiles.  The warp copies that run with
+// coalesced 16-byte cp.async (each lane up to kWinCap / 32 chunks, bypassing
+// L1) one source ahead of the convolution, and the lanes read their windows
+// from shared memory at offset max d - d_l; the table is staged as in
+// variant 3.  A source whose run is longer than kWinCap is read from global
+// memory as in variant 0.  The products and their order are variant 0's, so
+// the sums are identical.
+//
+// Pipeline (cp.async groups, committed in this order at iteration it): the
+// table stage of source it + 2, then, once source it + 1's delays have
+// landed, its window run.  Waiting for all but the newest group therefore
+// completes source it + 1's table stage and source it's window.
+constexpr int kWinCap = 128;  // samples per staged window run (2 KB)
+constexpr int kWinStages = 3;
+
+template <int Q>
+struct FarWinStage {
+  FarStage<Q, kWinStages> tab;
+  double2 win[2][kWinCap];
+};
+
+template <int Q, bool LAB, int K>
+__device__ __forceinline__ void window_conv_shared(const double2 *w, int tau0, const double2 (&c)[Q + 1],
+                                                   double2 (&acc)[K])
+{
+#pragma unroll
+  for(int m = 0; m < K + Q; ++m) {
+    if(tau0 < -kWindow && tau0 + m < -kWindow) continue;
+    const double2 r = w[m];
+    const double2 v = LAB ? make_double2(2 * r.x, 0.0) : r;
+#pragma unroll
+    for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfma(acc[k], c[k + Q - m], v);
+  }
+}
+
+__device__ __forceinline__ void cp_async16_l2(void *dst, const void *src)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src));
+}
+
+template <int Q, bool LAB, int K = kTimeBlock>
+__device__ __forceinline__ void far_body_wstage(const FarArgs &a, int task, FarWinStage<Q> &ws)
+{
+  constexpr int P = kWinStages;
+  const int lane = threadIdx.x & 31;
+  if(task >= a.nT * a.nG) return;  // uniform per warp
+  const int I = a.gmajor ? task % a.nT : task / a.nG, g = a.gmajor ? task / a.nT : task % a.nG;
+  const int J0 = g * a.group;
+  const int nJ = min(a.group, a.nT - J0);
+  const int t0 = *a.d_t0;
+  if(task == 0 && lane == 0) *a.far_t0_out = t0;
+  const int W = a.W;
+  unsigned long long pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  FarStage<Q, P> &st = ws.tab;
+
+  double2 acc[K];
+#pragma unroll
+  for(int k = 0; k < K; ++k) acc[k] = make_double2(0.0, 0.0);
+
+  const long long tile0 = (long long)I * a.nT + J0;
+  const int iters = nJ * kTile;
+  auto issue_table = [&](int it) {
+    if(it < iters) {
+      const int slot = it % P;
+      const long long tile = tile0 + it / kTile;
+      const int e = (it % kTile) * kTile + lane;
+#pragma unroll
+      for(int i = 0; i <= Q; ++i)
+        cp_async16(&st.coef[slot][i][lane], a.coef + (tile * (Q + 1) + i) * kTilePairs + e, pol);
+      cp_async4(&st.delay[slot][lane], a.delay + tile * kTilePairs + e, pol);
+    }
+    cp_async_commit();
+  };
+  auto row_of = [&](int it) { return a.ring + (long long)((J0 + it / kTile) * kTile + (it % kTile)) * a.stride; };
+  // source it's window run, its delays having landed: returns the largest
+  // delay among the lanes that need the source (-1: none does), and whether
+  // the run was staged (it fits kWinCap)
+  auto issue_window = [&](int it, bool &staged) {
+    int dmax = -1;
+    staged = false;
+    if(it < iters) {
+      const int d = st.delay[it % P][lane];
+      const bool need = d >= kTimeBlock;
+      dmax = __reduce_max_sync(0xffffffffu, need ? d : -1);
+      const int dmin = __reduce_min_sync(0xffffffffu, need ? d : 0x7fffffff);
+      const int span = dmax - dmin + K + Q;
+      if(dmax >= 0 && span <= kWinCap) {
+        staged = true;
+        int lo = (t0 - dmax - Q) % W;
+        if(lo < 0) lo += W;
+        const double2 *row = row_of(it);
+        double2 *dst = ws.win[it & 1];
+#pragma unroll
+        for(int r = 0; r < kWinCap / 32; ++r) {
+          const int m = lane + 32 * r;
+          if(m < span) {
+            int sl = lo + m;
+            if(sl >= W) sl -= W;
+            cp_async16_l2(dst + m, row + sl);
+          }
+        }
+      }
+    }
+    cp_async_commit();
+    return dmax;
+  };
+
+  // prologue: table stages 0 and 1, then source 0's window
+  issue_table(0);
+  issue_table(1);
+  cp_async_wait<1>();
+  __syncwarp();
+  bool staged_cur;
+  int dmax_cur = issue_window(0, staged_cur);
+  for(int it = 0; it < iters; ++it) {
+    // every lane has finished with source it - 1's table stage and window
+    __syncwarp();
+    issue_table(it + 2);
+    cp_async_wait<1>();  // source it + 1's table stage and source it's window
+    __syncwarp();
+    bool staged_next;
+    const int dmax_next = issue_window(it + 1, staged_next);
+    const int slot = it % P;
+    const int d = st.delay[slot][lane];
+    if(d >= kTimeBlock) {
+      double2 c[Q + 1];
+#pragma unroll
+      for(int i = 0; i <= Q; ++i) c[i] = st.coef[slot][i][lane];
+      const int tau0 = t0 - d - Q;
+      if(staged_cur) {
+        window_conv_shared<Q, LAB, K>(&ws.win[it & 1][dmax_cur - d], tau0, c, acc);
+      } else {
+        int slot0 = tau0 % W;
+        if(slot0 < 0) slot0 += W;
+        window_conv<Q, LAB, K>(row_of(it), slot0, tau0, c, acc);
+      }
+    }
+    staged_cur = staged_next;
+    dmax_cur = dmax_next;
+  }
+  cp_async_wait<0>();
+  group_partials_reduce<K>(a, I, g, acc);
+}
+
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128) far_kernel_wstage(FarArgs a)
+{
+  extern __shared__ double2 far_smem[];
+  FarWinStage<Q> *ws = reinterpret_cast<FarWinStage<Q> *>(far_smem);
+  far_body_wstage<Q, LAB>(a, warp_task(), ws[threadIdx.x >> 5]);
+}
+
 // Variant 6 is held to 128 registers (4 blocks, 16 warps per SM); uncapped
 // it takes 132 and fits 3 blocks.
 template <int Q, bool LAB, int VEC>
@@ -587,6 +746,21 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
     far_kernel_r4<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else if(a.variant == 2)
     far_kernel_v2<Q, LAB><<<blocks, 128, 0, s>>>(a);
+  else if(a.variant == 10 || a.variant == 11) {
+    // 10: windows staged in shared memory (3 table stages + 2 window runs per
+    // warp: 54 KB a block at q = 5); 11: the same in the source-group-major
+    // order
+    a.gmajor = a0.variant == 11;
+    const size_t smem = 4 * sizeof(FarWinStage<Q>);
+    static bool attr_w[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if(dev >= 64 || !attr_w[dev]) {
+      cudaFuncSetAttribute(far_kernel_wstage<Q, LAB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if(dev < 64) attr_w[dev] = true;
+    }
+    far_kernel_wstage<Q, LAB><<<blocks, 128, smem, s>>>(a);
+  }
   else if((a.variant >= 3 && a.variant <= 6) || a.variant == 9) {
     // 38 KB at q = 5, 51 KB at q = 7 (above the 48 KB default: opt in);
     // variant 5 keeps one more stage

@@ -51,7 +51,7 @@ def test_mixed_table_reports_the_fp32_pipe():
 
 
 def test_every_far_variant_has_a_kernel_name():
-    for v in range(10):
+    for v in range(12):
         assert bench.FAR_VARIANTS[v].startswith("far_kernel")
 
 

@@ -43,7 +43,7 @@ def test_tuned_choice_is_reported_and_agrees_with_both_forms(golden_weights, pre
 def test_far_variants_are_timed_and_identical(golden_weights):
     wl = I.plain_table(seed=2, n=1024, steps=64, pulse_delay=0.3)
     res = []
-    for v in (None, 0, 3, 5, 6, 7, 8, 9):
+    for v in (None, 0, 3, 5, 6, 7, 8, 9, 10, 11):
         with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights,
                              coef_mode=capi.COEF_TABLE) as sim:
             if v is not None:

@@ -311,13 +311,37 @@ def test_far_kernel_variants_agree_bitwise(golden_weights):
     task order; their arithmetic, and so their results, are identical."""
     wl = stable_small(300, 160, 0.06)
     outs = []
-    variants = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9)
+    variants = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11)
     for v in variants:
         with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
             sim.set_option("far_variant", v)
             outs.append(sim.run(160))
     for i in range(1, len(variants)):
         np.testing.assert_array_equal(outs[0], outs[i])
+
+
+@pytest.mark.parametrize("geometry", ["line", "cluster_and_line"])
+def test_staged_window_variants_on_long_and_short_runs(golden_weights, geometry):
+    """Variants 10 and 11 copy a source's window run (all 32 targets'
+    windows) into shared memory when it fits 128 samples and read global
+    memory when it does not: a line of dots 5 c dt apart gives every source
+    runs of ~180 samples, a tight cluster beside it gives short ones.  Both
+    paths, and the ring's wrap, give variant 0's bits."""
+    if geometry == "line":
+        wl = line_of_dots(256, 5e-3)
+    else:
+        wl = line_of_dots(256, 4e-3)
+        rng = np.random.default_rng(8)
+        wl.dots[:128, 0:3] = rng.uniform(-0.01, 0.01, size=(128, 3))
+        wl.dots[:128, 8] = 2e-5
+    outs = []
+    for v in (0, 10, 11):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+            sim.set_option("far_variant", v)
+            outs.append(sim.run(300))
+    assert np.abs(outs[0][..., 1]).max() > 1e-8
+    for o in outs[1:]:
+        np.testing.assert_array_equal(outs[0], o)
 
 
 def test_far_autotuner_runs_at_the_first_run_and_keeps_an_explicit_choice(golden_weights):
