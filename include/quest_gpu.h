@@ -316,12 +316,14 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  * "profile" (1 = CUDA events around the far-pair kernel and the step
  * kernels: event nodes inside the block graphs, or around each launch when
  * "graph" is 0),
- * "far_variant" (0..9: resource shape and task order of the far-pair
+ * "far_variant" (0..11: resource shape and task order of the far-pair
  *   kernel, same results; 7 and 8 are 0 and 3 with each block's warps on one
  *   source group of consecutive target tiles; the first qg_run of an FP64
- *   table handle of 512 dots or more picks the fastest of 0, 3, 5, 6, 7, 8
- *   and 9 (9: the table staged by bulk-copy-engine copies on an mbarrier)
- *   by timing launches of each, unless a variant was set; mixed-precision
+ *   table handle of 512 dots or more picks the fastest of 0, 3, 5, 6, 7, 8,
+ *   9, 10 and 11 (9: the table staged by bulk-copy-engine copies on an
+ *   mbarrier; 10 and 11: each source's history window run staged in shared
+ *   memory, in the two task orders) by timing launches of each, unless a
+ *   variant was set; mixed-precision
  *   table handles choose the same way among 0, 7 (its kernel at 150
  *   registers, target-tile and source-group major) and 1, 8 (at 128);
  *   on-the-fly handles take 7 for the source-group-major order; the

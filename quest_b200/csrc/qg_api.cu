@@ -1054,7 +1054,7 @@ static qg_status autotune_far(qg_handle *h)
     h->eval_cached = -0x7fffffff;
     return QG_OK;
   }
-  static const int candidates[] = {0, 3, 5, 6, 7, 8, 9};
+  static const int candidates[] = {0, 3, 5, 6, 7, 8, 9, 10, 11};
   const int t_test = h->max_delay + h->q + 2 * kTimeBlock;
   cudaEvent_t e0, e1;
   QG_CUDA(cudaEventCreate(&e0));

@@ -50,7 +50,7 @@ def test_far_variants_are_timed_and_identical(golden_weights):
                 sim.set_option("far_variant", v)
             res.append(sim.run(64))
             if v is None:
-                assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8, 9)
+                assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8, 9, 10, 11)
                 assert sim.get_option("tuned_far_us") > 0
     for r in res[1:]:
         np.testing.assert_array_equal(r, res[0])

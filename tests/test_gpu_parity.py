@@ -352,7 +352,7 @@ def test_far_autotuner_runs_at_the_first_run_and_keeps_an_explicit_choice(golden
     outs = []
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         outs.append(sim.run(48))
-        assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8, 9)
+        assert sim.get_option("far_variant") in (0, 3, 5, 6, 7, 8, 9, 10, 11)
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
         sim.set_option("far_variant", 4)
         outs.append(sim.run(48))
