@@ -708,6 +708,8 @@ def batched_record(args, world, rank, capi_precision, weights) -> dict:
     prec = capi.PREC_MIXED if capi_precision == "mixed" else capi.PREC_FP64
     sims = [capi.Simulation(r.dots, r.pulse, r.constants, weights=weights, precision=prec) for r in reqs]
     batch = capi.Batch(len(sims))
+    if args.batch_tune_group:
+        batch.set_option("tune_group", 1)
     for s in sims:
         batch.add(s)
     total = sum(r.pair_updates for r in reqs)
@@ -720,6 +722,12 @@ def batched_record(args, world, rank, capi_precision, weights) -> dict:
         nonfinite = 0
         while live:
             batch.run(args.blocks_per_round)
+            if blocks == 0:
+                tuned = {"tuned_far_us": batch.get_option("tuned_far_us"),
+                         "far_packed": batch.get_option("far_packed"),
+                         "far_gmajor": batch.get_option("far_gmajor"),
+                         "tune_group": batch.get_option("tune_group"),
+                         "far_group_class": [batch.get_option(f"far_group_class{c}") for c in range(4)]}
             blocks += args.blocks_per_round
             for r, s in [(r, s) for r, s in live if s.next_step >= r.constants.num_timesteps]:
                 nonfinite += s.bad_step() >= 0
@@ -736,7 +744,7 @@ def batched_record(args, world, rank, capi_precision, weights) -> dict:
             "unit": "pair-updates/s", "precision": capi_precision, "wall_s": wall, "blocks": blocks,
             "ensembles": args.ensembles, "N_min": int(ns.min()), "N_max": int(ns.max()), "sum_N2T": total,
             "timing": "wall clock of the whole batch (graph replays, membership changes, retirement)",
-            "nonfinite_members": int(nonfinite),
+            "nonfinite_members": int(nonfinite), "autotuned": tuned,
             "nonfinite_note": "members whose state overflowed (the reference's domain_error) still run every step: "
                               "the work per step does not depend on the values",
             "clocks": clocks.summary()}
@@ -820,6 +828,8 @@ def parse_args(argv=None):
     ap.add_argument("--otf-n", type=int, default=65536)
     ap.add_argument("--otf-blocks", type=int, default=2)
     ap.add_argument("--ensembles", type=int, default=256)
+    ap.add_argument("--batch-tune-group", action="store_true",
+                    help="batched workload: let the batch tuner pick source tiles per far warp per size class")
     ap.add_argument("--blocks-per-round", type=int, default=8)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0)

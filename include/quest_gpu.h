@@ -241,15 +241,22 @@ qg_status qg_batch_size(const qg_batch *b, int *members, int *tasks, int *blocks
  * source-group-major order, so a thread block's warps read the same history
  * rows, the default; same results), "mid_pipe" (1 = the step launches fetch
  * several mid-range pair entries per thread before summing them, which helps
- * members with long mid lists; same results). */
+ * members with long mid lists; same results), "tune_group" (1 = the next
+ * run's autotuner also times source tiles per far-kernel warp, 1, 2, 4 and
+ * 8, for each size class of members present (fewer than 4 tiles, fewer than
+ * 16, fewer than 64, more) and gives every member of a class, present or
+ * joining later, that class's group; a member's results then equal a solo
+ * run with the same "far_group", not one with its default; off by default),
+ * "autotune" (1 = time again at the next run). */
 qg_status qg_batch_set_option(qg_batch *b, const char *key, int value);
 /* Reads a batch option back: "far_packed", "far_gmajor", "mid_pipe",
- * "profile", "tuned_far_us" (the far launch's time the batch's autotuner
- * measured for its choice, microseconds; 0 if it did not run).  The
- * autotuner times the far launch's forms that sum the same terms (far_packed
- * for mixed members x far_gmajor) at the batch's first qg_batch_run and keeps
- * the fastest, unless one was set; "autotune" (1) asks for it again at the
- * next run. */
+ * "profile", "tune_group", "far_group_class0" .. "far_group_class3" (the
+ * group tuned for each size class, 0 = members keep their own),
+ * "tuned_far_us" (the far launch's time the batch's autotuner measured for
+ * its choice, microseconds; 0 if it did not run).  The autotuner times the
+ * far launch's forms that sum the same terms (far_packed for mixed members x
+ * far_gmajor) at the batch's first qg_batch_run and keeps the fastest, unless
+ * one was set; "autotune" (1) asks for it again at the next run. */
 qg_status qg_batch_get_option(const qg_batch *b, const char *key, int *value);
 /* Device time in milliseconds of the batch's far-pair launches and step
  * launches (each nullable), accumulated while "profile" is on. */

@@ -1567,6 +1567,12 @@ struct qg_batch_s {
   // run, unless set explicitly; tuned_far_us reads the winner's time back
   bool tune_pending = true;
   float tuned_far_ms = 0;
+  // "tune_group": the tuner also times source tiles per warp (1, 2, 4, 8)
+  // for each size class of members (tiles < 4, < 16, < 64, more); a member
+  // of a tuned class takes its class's group when the batch is rebuilt
+  // (0: the member's own)
+  bool tune_group = false;
+  int class_group[4] = {0, 0, 0, 0};
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double far_ms = 0, step_ms = 0;
   int far_launches = 0, step_launches = 0;
@@ -1670,9 +1676,36 @@ extern "C" qg_status qg_batch_remove(qg_batch *b, qg_handle *h)
   return QG_OK;
 }
 
+static int size_class(int nT) { return nT < 4 ? 0 : nT < 16 ? 1 : nT < 64 ? 2 : 3; }
+
+static void drop_graphs(qg_handle *h)
+{
+  for(auto &g : h->graph)
+    if(g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for(auto &row : h->gprof)
+    for(auto &g : row)
+      if(g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+}
+
 static qg_status batch_rebuild(qg_batch *b)
 {
   const int n = (int)b->members.size();
+  if(b->tune_group)
+    for(qg_handle *h : b->members) {
+      const int g = b->class_group[size_class(h->nT)];
+      if(g > 0 && g != h->group && !h->otf && (h->nT + g - 1) / g <= h->max_groups) {
+        h->group = g;
+        h->nG = (h->nT + g - 1) / g;
+        h->far_block = -0x7fffffff;
+        drop_graphs(h);
+      }
+    }
   // members with the longest mid lists per 32-dot block first: the step
   // launches' blocks are dispatched about in index order and those blocks
   // take longest, so starting them first shortens the launch's tail (the
@@ -1756,10 +1789,40 @@ static qg_status batch_autotune(qg_batch *b)
         best_g = b->far_gmajor;
       }
     }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   b->far_packed = best_p;
   b->far_gmajor = best_g;
+  if(b->tune_group) {
+    // one pass over the size classes present, each keeping the group that
+    // made the whole launch fastest with the others fixed
+    bool present[4] = {false, false, false, false};
+    for(const qg_handle *h : b->members) present[size_class(h->nT)] = true;
+    for(int c = 0; c < 4; ++c) {
+      if(!present[c]) continue;
+      int best_c = b->class_group[c];
+      for(int g : {1, 2, 4, 8}) {
+        b->class_group[c] = g;
+        QG_TRY(batch_rebuild(b));
+        float t = 1e30f;
+        for(int r = 0; r < 3; ++r) {
+          QG_CUDA(cudaEventRecord(e0, b->stream));
+          launch_far_batch(b->d_far, b->d_task_off, n, b->q, b->frame, b->mixed ? (b->far_packed ? 2 : 1) : 0,
+                           b->far_grid, b->stream);
+          QG_CUDA(cudaEventRecord(e1, b->stream));
+          QG_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if(r > 0) t = std::min(t, ms);
+        }
+        if(t < best) {
+          best = t;
+          best_c = g;
+        }
+      }
+      b->class_group[c] = best_c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   b->tuned_far_ms = best;
   return batch_rebuild(b);
 }
@@ -1844,6 +1907,12 @@ extern "C" qg_status qg_batch_set_option(qg_batch *b, const char *key, int value
     b->dirty = true;
     return QG_OK;
   }
+  if(!std::strcmp(key, "tune_group")) {
+    b->tune_group = value != 0;
+    if(b->tune_group) b->tune_pending = true;
+    b->dirty = true;
+    return QG_OK;
+  }
   return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_set_option: unknown key '%s'", key);
 }
 
@@ -1860,6 +1929,10 @@ extern "C" qg_status qg_batch_get_option(const qg_batch *b, const char *key, int
     *value = b->profile ? 1 : 0;
   else if(!std::strcmp(key, "tuned_far_us"))
     *value = (int)(b->tuned_far_ms * 1000.0f + 0.5f);
+  else if(!std::strcmp(key, "tune_group"))
+    *value = b->tune_group ? 1 : 0;
+  else if(!std::strncmp(key, "far_group_class", 15) && key[15] >= '0' && key[15] <= '3' && !key[16])
+    *value = b->class_group[key[15] - '0'];
   else
     return qg_fail(QG_ERR_INVALID_ARG, "qg_batch_get_option: unknown key '%s'", key);
   return QG_OK;

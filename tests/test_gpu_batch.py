@@ -153,3 +153,30 @@ def test_batch_autotuner_times_the_far_forms_and_keeps_the_bits(golden_weights):
         batch.remove(s)
         s.close()
     batch.close()
+
+
+def test_batch_group_search_per_size_class(golden_weights):
+    """"tune_group" times source tiles per far warp for each size class of
+    members; each member then equals a solo run with its class's group set
+    by hand."""
+    specs = [(51, 100, 0.08, 64, 5.0), (52, 700, 0.15, 64, 20.0), (53, 2500, 0.25, 64, 10.0)]
+    ens = [ensemble(*s) for s in specs]
+    batch = capi.Batch(4)
+    batch.set_option("tune_group", 1)
+    sims = [capi.Simulation(d, p, c, weights=golden_weights, precision=capi.PREC_MIXED) for d, p, c in ens]
+    for s in sims:
+        batch.add(s)
+    batch.run(4)
+    assert batch.get_option("tune_group") == 1
+    classes = [batch.get_option(f"far_group_class{c}") for c in range(4)]
+    assert any(g in (1, 2, 4, 8) for g in classes)
+    for (d, p, c), sim in zip(ens, sims):
+        g = sim.get_option("far_group")
+        with capi.Simulation(d, p, c, weights=golden_weights, precision=capi.PREC_MIXED) as solo_sim:
+            solo_sim.set_option("far_group", g)
+            solo_sim.run(64, record=False)
+            np.testing.assert_array_equal(sim.state(), solo_sim.state())
+    for s in sims:
+        batch.remove(s)
+        s.close()
+    batch.close()
