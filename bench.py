@@ -549,6 +549,7 @@ def run_ours(args, world, rank, local):
     t0 = time.perf_counter()
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=prec,
                          coef_mode=cmode) as sim2:
+        t_created = time.perf_counter()
         if args.far_variant is not None:
             sim2.set_option("far_variant", args.far_variant)
         try:
@@ -561,6 +562,7 @@ def run_ours(args, world, rank, local):
                 sim2.run(e2e_steps, out=rho_host)
         except capi.NonFiniteError:
             pass
+        t_ran = time.perf_counter()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)
@@ -593,6 +595,7 @@ def run_ours(args, world, rank, local):
         "config": config_dict(args, warm, timed),
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "pair-updates/s", "seconds": e2e_s, "steps": e2e_steps,
+                "create_s": t_created - t0, "run_s": t_ran - t_created,
                 "h2d_bytes_per_step": (n * 72 + 80) / e2e_steps, "d2h_bytes_per_step": d2h,
                 "includes": "qg_create (dots upload + %s) + qg_run with %s rho read back" %
                             ("max-delay and pair-list kernels" if otf else "table build",
@@ -784,7 +787,7 @@ def run_batched(args, world, rank, local):
             "config": {"workload": r["workload"], "ensembles": args.ensembles, "N_min": r["N_min"],
                        "N_max": r["N_max"], "sum_N2T": r["sum_N2T"], "precision": args.precision,
                        "coef_mode": "table"},
-            "wall_s": r["wall_s"], "clocks": r["clocks"]}
+            "wall_s": r["wall_s"], "autotuned": r.get("autotuned"), "clocks": r["clocks"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
