@@ -533,6 +533,8 @@ def run_ours(args, world, rank, local):
     info = sim.info()
     if args.far_variant is not None:
         sim.set_option("far_variant", args.far_variant)
+    if args.tune_group and not otf:
+        sim.set_option("tune_group", 1)
     t = timed_run(sim, warm, timed, world)
     variant = sim.get_option("far_variant") if not (mixed or otf) else None  # FP64 table only
     tuned = {k: sim.get_option(k) for k in ("far_group", "block_step")}
@@ -552,6 +554,8 @@ def run_ours(args, world, rank, local):
         t_created = time.perf_counter()
         if args.far_variant is not None:
             sim2.set_option("far_variant", args.far_variant)
+        if args.tune_group and not otf:
+            sim2.set_option("tune_group", 1)
         try:
             if otf:
                 # 65536 dots x 2 complex per step: read back the last block's states only
@@ -637,6 +641,8 @@ def sub_mixed(args, weights) -> dict:
     with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=weights, precision=capi.PREC_MIXED,
                          coef_mode=capi.COEF_TABLE) as sim:
         info = sim.info()
+        if args.tune_group:
+            sim.set_option("tune_group", 1)
         t = timed_run(sim, warm, timed, 1)
         group = sim.get_option("far_group")
     torch.cuda.synchronize()
@@ -763,7 +769,8 @@ def serving_record(args, world, rank, precision: str, rate: float, weights) -> d
     from quest_b200 import capi, serving
     reqs = serving.serving_requests(args.requests, rate, seed=70 + rank, n_range=(32, args.serve_nmax))
     srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=weights,
-                         precision=capi.PREC_MIXED if precision == "mixed" else capi.PREC_FP64)
+                         precision=capi.PREC_MIXED if precision == "mixed" else capi.PREC_FP64,
+                         tune_group=args.batch_tune_group)
     barrier(world)
     with ClockSampler(torch.cuda.current_device(), period=0.05) as clocks:
         stats = srv.serve(reqs)
@@ -831,6 +838,8 @@ def parse_args(argv=None):
     ap.add_argument("--otf-n", type=int, default=65536)
     ap.add_argument("--otf-blocks", type=int, default=2)
     ap.add_argument("--ensembles", type=int, default=256)
+    ap.add_argument("--tune-group", action="store_true",
+                    help="table workloads: let the autotuner also pick source tiles per far warp")
     ap.add_argument("--batch-tune-group", action="store_true",
                     help="batched workload: let the batch tuner pick source tiles per far warp per size class")
     ap.add_argument("--blocks-per-round", type=int, default=8)

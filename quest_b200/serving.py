@@ -77,13 +77,18 @@ class Result:
 
 class Server:
     def __init__(self, budget_bytes: float = 150e9, capacity: int = 1024, weights=None,
-                 blocks_per_round: int = 1, precision: int = capi.PREC_FP64):
+                 blocks_per_round: int = 1, precision: int = capi.PREC_FP64, tune_group: bool = False):
         self.precision = precision
         self.budget = float(budget_bytes)
         self.capacity = capacity
         self.weights = weights if weights is not None else capi.pc_weights()
         self.blocks_per_round = blocks_per_round
         self.batch = capi.Batch(capacity)
+        if tune_group:
+            # the batch's first run also times source tiles per far warp for
+            # each size class present; later requests of a tuned class take
+            # its group (their results then match solo runs with that group)
+            self.batch.set_option("tune_group", 1)
         self.running: dict[int, tuple[Request, capi.Simulation, float, int]] = {}
         # builds in flight, in admission order: (request, future, admitted, footprint)
         self.building: collections.deque = collections.deque()
