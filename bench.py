@@ -708,8 +708,11 @@ def batched_record(args, world, rank, capi_precision, weights) -> dict:
     [64, 4096], side U[0.05, 0.3], E_0 U[1, 30], steps U[2000, 20000],
     all in one batch (one persistent far-pair launch + the step launches per
     16-step block, replayed as a CUDA graph); finished ensembles are retired
-    as they finish.  Wall time of the whole job (all members to their last
-    step), pair-updates = sum of N^2 x steps."""
+    as they finish.  Unless --no-batch-tune-group, the batch's first run
+    also times source tiles per far warp for each member size class (the
+    choice is in the record).  Wall time of the whole job (all members to
+    their last step, the tuning included), pair-updates = sum of N^2 x
+    steps."""
     import torch
 
     from quest_b200 import capi, serving
@@ -770,7 +773,7 @@ def serving_record(args, world, rank, precision: str, rate: float, weights) -> d
     reqs = serving.serving_requests(args.requests, rate, seed=70 + rank, n_range=(32, args.serve_nmax))
     srv = serving.Server(budget_bytes=args.budget_gb * 1e9, weights=weights,
                          precision=capi.PREC_MIXED if precision == "mixed" else capi.PREC_FP64,
-                         tune_group=args.batch_tune_group)
+                         tune_group=args.serve_tune_group)
     barrier(world)
     with ClockSampler(torch.cuda.current_device(), period=0.05) as clocks:
         stats = srv.serve(reqs)
@@ -840,8 +843,11 @@ def parse_args(argv=None):
     ap.add_argument("--ensembles", type=int, default=256)
     ap.add_argument("--tune-group", action="store_true",
                     help="table workloads: let the autotuner also pick source tiles per far warp")
-    ap.add_argument("--batch-tune-group", action="store_true",
-                    help="batched workload: let the batch tuner pick source tiles per far warp per size class")
+    ap.add_argument("--no-batch-tune-group", dest="batch_tune_group", action="store_false",
+                    help="batched workload: keep every member's own source tiles per far warp (by default the "
+                         "batch tuner picks them per size class; members then equal solo runs with that group)")
+    ap.add_argument("--serve-tune-group", action="store_true",
+                    help="serving workload: the batch tuner's group search at the service's first run")
     ap.add_argument("--blocks-per-round", type=int, default=8)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0)

@@ -90,7 +90,6 @@ struct qg_handle_s {
   int *d_ints = nullptr;
   unsigned long long *d_u64 = nullptr;
   double2 *d_traj = nullptr;  // 2 * traj_k steps x N x 2
-  double2 *h_traj = nullptr;  // pinned, same size
   int traj_k = 0;
   double2 *d_io = nullptr;    // N complex device staging for evaluate / set_history
   double2 *h_io = nullptr;    // pinned N complex
@@ -301,7 +300,6 @@ static void destroy_handle(qg_handle *h)
     if(h->ev_copy[i]) cudaEventDestroy(h->ev_copy[i]);
   }
   for(void *p : h->allocs) cudaFree(p);
-  if(h->h_traj) cudaFreeHost(h->h_traj);
   if(h->h_io) cudaFreeHost(h->h_io);
   if(h->stream) cudaStreamDestroy(h->stream);
   if(h->copy_stream) cudaStreamDestroy(h->copy_stream);
@@ -402,10 +400,11 @@ static int ring_depth(int max_delay, int q)
   return w + (w & 1);
 }
 
-// Steps per trajectory staging chunk: a multiple of K, about 32 MiB.
+// Steps per trajectory chunk: a multiple of K, about 4 MiB (small chunks
+// let each chunk's copy to the host overlap the next chunk's steps).
 static int traj_steps(int n)
 {
-  long long k = std::min<long long>(256, (32ll << 20) / (32ll * n));
+  long long k = std::min<long long>(256, (4ll << 20) / (32ll * n));
   k = std::max<long long>(kTimeBlock, k - k % kTimeBlock);
   return (int)k;
 }
@@ -1272,13 +1271,6 @@ static qg_status launch_prof_block(qg_handle *h, int traj)
 
 // Host-side resources made on first use: pinned trajectory staging (a
 // recorded qg_run or qg_get_state) and the profiling events.
-static qg_status ensure_host_staging(qg_handle *h)
-{
-  if(h->h_traj) return QG_OK;
-  QG_CUDA(cudaMallocHost((void **)&h->h_traj, sizeof(double2) * (size_t)2 * h->traj_k * h->n * 2));
-  return QG_OK;
-}
-
 static qg_status ensure_events(qg_handle *h)
 {
   if(h->events_ready) return QG_OK;
@@ -1492,33 +1484,43 @@ extern "C" qg_status qg_run(qg_handle *h, int n_steps, double *rho_out, int *bad
   if(!rho_out) {
     QG_TRY(launch_steps(h, t_start, n_steps, false));
   } else {
-    QG_TRY(ensure_host_staging(h));
+    // Every step's state straight into the caller's buffer.  Chunks of
+    // traj_k steps alternate between the two halves of d_traj.  Chunk c's
+    // copy is issued after chunk c + 1's launches are queued: a copy into
+    // pageable memory returns only when it is done, and meanwhile the device
+    // computes the next chunk; chunk c + 2 waits for chunk c's copy before
+    // it reuses that half.
     const int K = h->traj_k;
     const int nchunks = (n_steps + K - 1) / K;
-    auto drain = [&](int c) -> qg_status {
+    auto copy_out = [&](int c) -> cudaError_t {
       const int b = c & 1;
       const int k = std::min(K, n_steps - c * K);
-      QG_CUDA(cudaEventSynchronize(h->ev_copy[b]));
-      std::memcpy(rho_out + (size_t)c * K * row * 2, h->h_traj + (size_t)b * K * row,
-                  sizeof(double2) * row * k);
-      return QG_OK;
+      cudaError_t e = cudaStreamWaitEvent(h->copy_stream, h->ev_chunk[b], 0);
+      if(e == cudaSuccess)
+        e = cudaMemcpyAsync(rho_out + (size_t)c * K * row * 2, h->d_traj + (size_t)b * K * row,
+                            sizeof(double2) * row * k, cudaMemcpyDeviceToHost, h->copy_stream);
+      if(e == cudaSuccess) e = cudaEventRecord(h->ev_copy[b], h->copy_stream);
+      return e;
     };
-    for(int c = 0; c < nchunks; ++c) {
+    qg_status st = QG_OK;
+    cudaError_t ce = cudaSuccess;
+    for(int c = 0; c < nchunks && st == QG_OK && ce == cudaSuccess; ++c) {
       const int b = c & 1;
       const int k = std::min(K, n_steps - c * K);
-      if(c >= 2) {
-        QG_TRY(drain(c - 2));
-        QG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_copy[b], 0));
-      }
+      if(c >= 2) ce = cudaStreamWaitEvent(h->stream, h->ev_copy[b], 0);
+      if(ce != cudaSuccess) break;
       launch_set_int(h->d_ints + 3, t_start + c * K - b * K, h->stream);
-      QG_TRY(launch_steps(h, t_start + c * K, k, true));
-      QG_CUDA(cudaEventRecord(h->ev_chunk[b], h->stream));
-      QG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ev_chunk[b], 0));
-      QG_CUDA(cudaMemcpyAsync(h->h_traj + (size_t)b * K * row, h->d_traj + (size_t)b * K * row,
-                              sizeof(double2) * row * k, cudaMemcpyDeviceToHost, h->copy_stream));
-      QG_CUDA(cudaEventRecord(h->ev_copy[b], h->copy_stream));
+      st = launch_steps(h, t_start + c * K, k, true);
+      if(st != QG_OK) break;
+      ce = cudaEventRecord(h->ev_chunk[b], h->stream);
+      if(ce == cudaSuccess && c >= 1) ce = copy_out(c - 1);
+      if(ce == cudaSuccess && c == nchunks - 1) ce = copy_out(c);
     }
-    for(int c = std::max(0, nchunks - 2); c < nchunks; ++c) QG_TRY(drain(c));
+    // no copy into the caller's buffer may outlive the call
+    const cudaError_t ce2 = cudaStreamSynchronize(h->copy_stream);
+    if(st != QG_OK) return st;
+    QG_CUDA(ce);
+    QG_CUDA(ce2);
   }
   int bad = kBadNone;
   QG_CUDA(cudaMemcpyAsync(&bad, h->d_ints + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1980,14 +1982,12 @@ extern "C" qg_status qg_get_state(qg_handle *h, double *rho_out)
 {
   if(!h || !rho_out) return qg_fail(QG_ERR_INVALID_ARG, "qg_get_state: NULL argument");
   QG_CUDA(cudaSetDevice(h->device));
-  QG_TRY(ensure_host_staging(h));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   launch_state_read(h->step_args(true), h->next_step - 1, h->d_traj, h->stream);
   QG_CUDA(cudaGetLastError());
-  QG_CUDA(cudaMemcpyAsync(h->h_traj, h->d_traj, sizeof(double2) * 2 * (size_t)h->n, cudaMemcpyDeviceToHost,
+  QG_CUDA(cudaMemcpyAsync(rho_out, h->d_traj, sizeof(double2) * 2 * (size_t)h->n, cudaMemcpyDeviceToHost,
                           h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
-  std::memcpy(rho_out, h->h_traj, sizeof(double2) * 2 * (size_t)h->n);
   return QG_OK;
 }
 
