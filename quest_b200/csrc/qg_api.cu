@@ -1269,8 +1269,7 @@ static qg_status launch_prof_block(qg_handle *h, int traj)
   return QG_OK;
 }
 
-// Host-side resources made on first use: pinned trajectory staging (a
-// recorded qg_run or qg_get_state) and the profiling events.
+// The profiling events, made on first use.
 static qg_status ensure_events(qg_handle *h)
 {
   if(h->events_ready) return QG_OK;
