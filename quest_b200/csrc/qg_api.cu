@@ -251,16 +251,78 @@ struct qg_handle_s {
   }
 };
 
+// ---- device memory -------------------------------------------------------------
+// Handle buffers come from one stream-ordered pool per device that keeps the
+// blocks freed by destroyed handles (up to half the device's memory) for the
+// next ones: a service that creates and destroys handles then neither maps
+// memory again for each nor synchronises the device on every free, as
+// cudaFree does, so freeing a 27 GB table does not stall a batch running on
+// another stream.  An allocation the device cannot hold first returns the
+// pool's unused blocks and tries again.
+static cudaMemPool_t handle_pool(int device)
+{
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(device);
+  if(it != pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if(cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  unsigned long long keep = total_b / 2;  // cudaMemPoolAttrReleaseThreshold: a 64-bit count
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[device] = pool;
+  return pool;
+}
+
+// `bytes` from the device's pool on the handle's stream; the stream is
+// synchronised so the memory can be used from any stream at once.
+static cudaError_t pool_alloc(qg_handle *h, void **ptr, size_t bytes)
+{
+  cudaMemPool_t pool = handle_pool(h->device);
+  if(!pool) return cudaMalloc(ptr, bytes);
+  cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, pool, h->stream);
+  if(e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    // blocks freed on other streams return to the device once those frees
+    // have run
+    cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(ptr, bytes, pool, h->stream);
+  }
+  if(e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e;
+}
+
+// Returns a block to the pool once the handle's stream reaches this point
+// (the callers have synchronised every stream that used it).
+static void pool_free(qg_handle *h, void *p)
+{
+  if(!p) return;
+  if(handle_pool(h->device))
+    cudaFreeAsync(p, h->stream);
+  else
+    cudaFree(p);
+}
+
 template <typename T>
 static qg_status dalloc(qg_handle *h, T **p, size_t count)
 {
   void *ptr = nullptr;
   const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  cudaError_t e = cudaMalloc(&ptr, bytes);
+  cudaError_t e = pool_alloc(h, &ptr, bytes);
   if(e != cudaSuccess) {
     cudaGetLastError();
     return qg_fail(e == cudaErrorMemoryAllocation ? QG_ERR_OOM : QG_ERR_CUDA,
-                   "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+                   "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
   }
   h->allocs.push_back(ptr);
   h->bytes += bytes;
@@ -299,7 +361,7 @@ static void destroy_handle(qg_handle *h)
     if(h->ev_chunk[i]) cudaEventDestroy(h->ev_chunk[i]);
     if(h->ev_copy[i]) cudaEventDestroy(h->ev_copy[i]);
   }
-  for(void *p : h->allocs) cudaFree(p);
+  for(void *p : h->allocs) pool_free(h, p);
   if(h->h_io) cudaFreeHost(h->h_io);
   if(h->stream) cudaStreamDestroy(h->stream);
   if(h->copy_stream) cudaStreamDestroy(h->copy_stream);
@@ -425,8 +487,8 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   for(int pass = 0; pass < 2; ++pass) {
     const unsigned long long cap = pass == 0 ? 0 : std::max<unsigned long long>(cnt, 1);
     if(pass == 1) {
-      QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
-      QG_CUDA(cudaMalloc(&d_mc, sizeof(double2) * q1 * cap));
+      QG_CUDA(pool_alloc(h, (void **)&d_pairs, sizeof(int) * 3 * cap));
+      QG_CUDA(pool_alloc(h, (void **)&d_mc, sizeof(double2) * q1 * cap));
     }
     QG_CUDA(cudaMemsetAsync(h->d_u64 + 2, 0, sizeof(unsigned long long), h->stream));
     launch_near_find(h->d_pos, h->d_user, h->n_pad, c0dt, kTimeBlock, d_pairs, h->d_u64 + 2, cap, h->stream);
@@ -443,8 +505,8 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 3 * cap, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaMemcpyAsync(mc.data(), d_mc, sizeof(double2) * q1 * cap, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
-  cudaFree(d_pairs);
-  cudaFree(d_mc);
+  pool_free(h, d_pairs);
+  pool_free(h, d_mc);
   const long long m = h->mid_pairs;
   const int n = h->n_pad;  // internal indices (padding holes have no pairs)
 
@@ -577,13 +639,14 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
 
   auto upload_i = [&](int **dst, const std::vector<int> &v) -> qg_status {
     QG_TRY(dalloc(h, dst, v.size()));
-    if(!v.empty()) QG_CUDA(cudaMemcpy(*dst, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice));
+    if(!v.empty())
+      QG_CUDA(cudaMemcpyAsync(*dst, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, h->stream));
     return QG_OK;
   };
   auto upload_c = [&](double2 **dst, const std::vector<double2> &v) -> qg_status {
     QG_TRY(dalloc(h, dst, v.size()));
     if(!v.empty())
-      QG_CUDA(cudaMemcpy(*dst, v.data(), sizeof(double2) * v.size(), cudaMemcpyHostToDevice));
+      QG_CUDA(cudaMemcpyAsync(*dst, v.data(), sizeof(double2) * v.size(), cudaMemcpyHostToDevice, h->stream));
     return QG_OK;
   };
   QG_TRY(upload_i(&h->d_mid_ptr, mptr));
@@ -650,28 +713,31 @@ static qg_status order_for_near_groups(qg_handle *h, const qg_dot *dots, const s
   double *d_pos = nullptr;
   int *d_user = nullptr, *d_pairs = nullptr;
   unsigned long long *d_cnt = nullptr;
-  QG_CUDA(cudaMalloc(&d_pos, sizeof(double) * pos.size()));
-  QG_CUDA(cudaMalloc(&d_user, sizeof(int) * user.size()));
-  QG_CUDA(cudaMalloc(&d_cnt, sizeof(unsigned long long)));
-  QG_CUDA(cudaMemcpy(d_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice));
-  QG_CUDA(cudaMemcpy(d_user, user.data(), sizeof(int) * user.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(pool_alloc(h, (void **)&d_pos, sizeof(double) * pos.size()));
+  QG_CUDA(pool_alloc(h, (void **)&d_user, sizeof(int) * user.size()));
+  QG_CUDA(pool_alloc(h, (void **)&d_cnt, sizeof(unsigned long long)));
+  QG_CUDA(cudaMemcpyAsync(d_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(d_user, user.data(), sizeof(int) * user.size(), cudaMemcpyHostToDevice, h->stream));
   const double c0dt = h->params.c0 * h->params.dt;
   unsigned long long cnt = 0;
   for(int pass = 0; pass < 2; ++pass) {
     const unsigned long long cap = pass == 0 ? 0 : std::max<unsigned long long>(cnt, 1);
-    if(pass == 1) QG_CUDA(cudaMalloc(&d_pairs, sizeof(int) * 3 * cap));
-    QG_CUDA(cudaMemset(d_cnt, 0, sizeof(unsigned long long)));
+    if(pass == 1) QG_CUDA(pool_alloc(h, (void **)&d_pairs, sizeof(int) * 3 * cap));
+    QG_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), h->stream));
     launch_near_find(d_pos, d_user, np0, c0dt, 2, d_pairs, d_cnt, cap, h->stream);
     QG_CUDA(cudaGetLastError());
     QG_CUDA(cudaMemcpyAsync(&cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
     QG_CUDA(cudaStreamSynchronize(h->stream));
   }
   std::vector<int> pairs(3 * std::max<unsigned long long>(cnt, 1));
-  if(cnt) QG_CUDA(cudaMemcpy(pairs.data(), d_pairs, sizeof(int) * 3 * cnt, cudaMemcpyDeviceToHost));
-  cudaFree(d_pos);
-  cudaFree(d_user);
-  cudaFree(d_cnt);
-  if(d_pairs) cudaFree(d_pairs);
+  if(cnt) {
+    QG_CUDA(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(int) * 3 * cnt, cudaMemcpyDeviceToHost, h->stream));
+    QG_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  pool_free(h, d_pos);
+  pool_free(h, d_user);
+  pool_free(h, d_cnt);
+  pool_free(h, d_pairs);
 
   // groups over Morton positions: the connected components of the pairs at
   // floor delay <= 1 when each fits in a block (then the delay-1 partners
@@ -800,16 +866,16 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_TRY(dalloc(h, &h->d_t1, t1.size()));
   QG_TRY(dalloc(h, &h->d_t2, t2.size()));
   QG_TRY(dalloc(h, &h->d_user, user.size()));
-  QG_CUDA(cudaMemcpy(h->d_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice));
-  QG_CUDA(cudaMemcpy(h->d_dip, dip.data(), sizeof(double) * dip.size(), cudaMemcpyHostToDevice));
-  QG_CUDA(cudaMemcpy(h->d_freq, fr.data(), sizeof(double) * fr.size(), cudaMemcpyHostToDevice));
-  QG_CUDA(cudaMemcpy(h->d_t1, t1.data(), sizeof(double) * t1.size(), cudaMemcpyHostToDevice));
-  QG_CUDA(cudaMemcpy(h->d_t2, t2.data(), sizeof(double) * t2.size(), cudaMemcpyHostToDevice));
-  QG_CUDA(cudaMemcpy(h->d_user, user.data(), sizeof(int) * user.size(), cudaMemcpyHostToDevice));
+  QG_CUDA(cudaMemcpyAsync(h->d_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(h->d_dip, dip.data(), sizeof(double) * dip.size(), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(h->d_freq, fr.data(), sizeof(double) * fr.size(), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(h->d_t1, t1.data(), sizeof(double) * t1.size(), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(h->d_t2, t2.data(), sizeof(double) * t2.size(), cudaMemcpyHostToDevice, h->stream));
+  QG_CUDA(cudaMemcpyAsync(h->d_user, user.data(), sizeof(int) * user.size(), cudaMemcpyHostToDevice, h->stream));
   QG_TRY(dalloc(h, &h->d_ints, 16));
   QG_TRY(dalloc(h, &h->d_u64, 4));
-  QG_CUDA(cudaMemset(h->d_ints, 0, sizeof(int) * 16));
-  QG_CUDA(cudaMemset(h->d_u64, 0, sizeof(unsigned long long) * 4));
+  QG_CUDA(cudaMemsetAsync(h->d_ints, 0, sizeof(int) * 16, h->stream));
+  QG_CUDA(cudaMemsetAsync(h->d_u64, 0, sizeof(unsigned long long) * 4, h->stream));
 
   // coefficients: a table when asked for, or (auto) when it takes at most
   // half of the free device memory; otherwise computed in the far kernel
@@ -988,7 +1054,7 @@ static qg_status switch_to_otf(qg_handle *h)
     if(!p) continue;
     auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
     if(it != h->allocs.end()) h->allocs.erase(it);
-    QG_CUDA(cudaFree(p));
+    pool_free(h, p);
   }
   h->bytes -= table_bytes(h->nT, h->q, h->mixed);
   h->d_delay = nullptr;
