@@ -26,7 +26,9 @@
  *    handle must not overlap (the reference's objects are not reentrant
  *    either); different handles are independent.
  *  - The library allocates its device memory in qg_create and frees it in
- *    qg_destroy; no call in between allocates device memory.  The memory
+ *    qg_destroy; no call in between allocates device memory (the first
+ *    evaluate or history copy of a handle allocates its small pinned host
+ *    staging buffer).  The memory
  *    comes from a stream-ordered pool per device that keeps freed blocks (up
  *    to half the device's memory) for later handles, so qg_destroy does not
  *    synchronise the device; an allocation that does not fit first returns

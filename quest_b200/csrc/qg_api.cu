@@ -92,7 +92,7 @@ struct qg_handle_s {
   double2 *d_traj = nullptr;  // 2 * traj_k steps x N x 2
   int traj_k = 0;
   double2 *d_io = nullptr;    // N complex device staging for evaluate / set_history
-  double2 *h_io = nullptr;    // pinned N complex
+  double2 *h_io = nullptr;    // pinned N complex, made at the first evaluate / history copy
 
   bool fused = true;
   int step_blocks = 0;
@@ -510,18 +510,32 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   const long long m = h->mid_pairs;
   const int n = h->n_pad;  // internal indices (padding holes have no pairs)
 
-  // mid list: both directions, partners in increasing order
+  // mid list: both directions, partners in increasing order (a counting
+  // pass places each dot's entries, then its short segment is sorted: the
+  // pairs arrive in the device's append order, which varies run to run)
   struct MidEntry {
     int b, d;
     long long k;  // index into pairs / mc
   };
-  std::vector<std::vector<MidEntry>> mid(n);
+  std::vector<int> mptr(n + 1, 0);  // n = n_pad here
+  for(long long k = 0; k < m; ++k) {
+    ++mptr[pairs[3 * k] + 1];
+    ++mptr[pairs[3 * k + 1] + 1];
+  }
+  for(int i = 0; i < n; ++i) mptr[i + 1] += mptr[i];
+  std::vector<MidEntry> ment((size_t)mptr[n]);
+  {
+    std::vector<int> fill(mptr.begin(), mptr.end() - 1);
+    for(long long k = 0; k < m; ++k) {
+      const int a = pairs[3 * k], b = pairs[3 * k + 1], d = pairs[3 * k + 2];
+      ment[fill[a]++] = {b, d, k};
+      ment[fill[b]++] = {a, d, k};
+    }
+  }
   std::vector<std::vector<std::pair<int, double2>>> adj(n);  // delay-0 tap-0 coupling
   DSU dsu(n);
   for(long long k = 0; k < m; ++k) {
     const int a = pairs[3 * k], b = pairs[3 * k + 1], d = pairs[3 * k + 2];
-    mid[a].push_back({b, d, k});
-    mid[b].push_back({a, d, k});
     if(d == 0) {
       if(h->otf) ++h->near_pairs;
       adj[a].push_back({b, mc[k * q1]});
@@ -529,19 +543,16 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
       dsu.unite(a, b);
     }
   }
-  std::vector<int> mptr(n + 1, 0), midx, mdel;  // n = n_pad here
-  std::vector<double2> mcoef;
-  midx.reserve(2 * m);
-  mdel.reserve(2 * m);
-  mcoef.reserve(2 * m * q1);
+  std::vector<int> midx((size_t)mptr[n]), mdel((size_t)mptr[n]);
+  std::vector<double2> mcoef((size_t)mptr[n] * q1);
   for(int i = 0; i < n; ++i) {
-    std::sort(mid[i].begin(), mid[i].end(), [](const MidEntry &x, const MidEntry &y) { return x.b < y.b; });
-    for(auto &e : mid[i]) {
-      midx.push_back(e.b);
-      mdel.push_back(e.d);
-      for(int t = 0; t < q1; ++t) mcoef.push_back(mc[e.k * q1 + t]);
+    std::sort(ment.begin() + mptr[i], ment.begin() + mptr[i + 1],
+              [](const MidEntry &x, const MidEntry &y) { return x.b < y.b; });
+    for(int e = mptr[i]; e < mptr[i + 1]; ++e) {
+      midx[e] = ment[e].b;
+      mdel[e] = ment[e].d;
+      std::memcpy(&mcoef[(size_t)e * q1], &mc[ment[e].k * q1], sizeof(double2) * q1);
     }
-    mptr[i + 1] = (int)midx.size();
   }
   for(auto &v : adj)
     std::sort(v.begin(), v.end(), [](const std::pair<int, double2> &x,
@@ -551,8 +562,8 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   std::vector<double2> ncoef;
   bool lag = true;
   for(int i = 0; i < n; ++i) {
-    for(auto &e : mid[i])
-      if(e.d <= 1) {
+    for(int j = mptr[i]; j < mptr[i + 1]; ++j)
+      if(const MidEntry &e = ment[j]; e.d <= 1) {
         nidx.push_back(e.b);
         ncoef.push_back(mc[e.k * q1 + (1 - e.d)]);
         if(e.b / 32 != i / 32) lag = false;
@@ -600,25 +611,35 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   // the step-block kernel: all blocks resident, each with its part of the
   // mid list in shared memory when that still fits
   // and, again when it fits, the history of each block's distinct partners
+  // per block: its distinct partners in order of first use (mpj[e] = the
+  // entry's partner's position among them) and the blocks that hold them
+  // (the block itself first); stamps instead of sorts, one pass per block
   int max_e = 0, max_p = 0;
   std::vector<int> bptr(1, 0), bidx, mpj(midx.size()), pbptr(1, 0), pbidx;
+  std::vector<int> seen(np, -1), where(np, 0), bseen(std::max(h->step_blocks, 1), -1);
   for(int b = 0; b < h->step_blocks; ++b) {
     const int e0 = mptr[32 * b], e1 = mptr[32 * (b + 1)];
     max_e = std::max(max_e, e1 - e0);
-    std::vector<int> parts(midx.begin() + e0, midx.begin() + e1);
-    std::sort(parts.begin(), parts.end());
-    parts.erase(std::unique(parts.begin(), parts.end()), parts.end());
-    for(int e = e0; e < e1; ++e)
-      mpj[e] = (int)(std::lower_bound(parts.begin(), parts.end(), midx[e]) - parts.begin());
-    std::vector<int> blks(1, b);
-    for(int pp : parts) blks.push_back(pp / 32);
-    std::sort(blks.begin(), blks.end());
-    blks.erase(std::unique(blks.begin(), blks.end()), blks.end());
-    pbidx.insert(pbidx.end(), blks.begin(), blks.end());
+    const int p0 = (int)bidx.size();
+    for(int e = e0; e < e1; ++e) {
+      const int pp = midx[e];
+      if(seen[pp] != b) {
+        seen[pp] = b;
+        where[pp] = (int)bidx.size() - p0;
+        bidx.push_back(pp);
+      }
+      mpj[e] = where[pp];
+    }
+    bseen[b] = b;
+    pbidx.push_back(b);
+    for(int j = p0; j < (int)bidx.size(); ++j)
+      if(bseen[bidx[j] / 32] != b) {
+        bseen[bidx[j] / 32] = b;
+        pbidx.push_back(bidx[j] / 32);
+      }
     pbptr.push_back((int)pbidx.size());
-    bidx.insert(bidx.end(), parts.begin(), parts.end());
     bptr.push_back((int)bidx.size());
-    max_p = std::max(max_p, (int)parts.size());
+    max_p = std::max(max_p, (int)bidx.size() - p0);
   }
   h->mid_cache = 0;
   h->hist_cap = 0;
@@ -968,7 +989,6 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   h->traj_k = traj_steps(n);
   QG_TRY(dalloc(h, &h->d_traj, (size_t)2 * h->traj_k * n * 2));
   QG_TRY(dalloc(h, &h->d_io, (size_t)n));
-  QG_CUDA(cudaMallocHost((void **)&h->h_io, sizeof(double2) * (size_t)n));
   for(int i = 0; i < 2; ++i) {
     QG_CUDA(cudaEventCreateWithFlags(&h->ev_chunk[i], cudaEventDisableTiming));
     QG_CUDA(cudaEventCreateWithFlags(&h->ev_copy[i], cudaEventDisableTiming));
@@ -2173,8 +2193,17 @@ extern "C" qg_status qg_next_step(const qg_handle *h, int *step)
   return QG_OK;
 }
 
+// The pinned staging of evaluate and the history copies, made on first use
+// (a pinned allocation costs about a millisecond; most handles never need it).
+static qg_status ensure_h_io(qg_handle *h)
+{
+  if(!h->h_io) QG_CUDA(cudaMallocHost((void **)&h->h_io, sizeof(double2) * (size_t)h->n));
+  return QG_OK;
+}
+
 static qg_status upload_io(qg_handle *h, const double *src)
 {
+  QG_TRY(ensure_h_io(h));
   std::memcpy(h->h_io, src, sizeof(double2) * h->n);
   QG_CUDA(cudaMemcpyAsync(h->d_io, h->h_io, sizeof(double2) * h->n, cudaMemcpyHostToDevice, h->stream));
   return QG_OK;
@@ -2182,6 +2211,7 @@ static qg_status upload_io(qg_handle *h, const double *src)
 
 static qg_status download_io(qg_handle *h, double *dst)
 {
+  QG_TRY(ensure_h_io(h));
   QG_CUDA(cudaMemcpyAsync(h->h_io, h->d_io, sizeof(double2) * h->n, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   std::memcpy(dst, h->h_io, sizeof(double2) * h->n);
