@@ -346,6 +346,9 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  *   own),
  * "autotune" (1 = time the far-kernel variants again now; at a block
  *   boundary between runs),
+ * "far_early" (1 = the default: far variants 0 and 7 use their first-blocks
+ *   form in the blocks where some windows start before step -22, one loop
+ *   for all lanes of a warp instead of two; 0 = never; same results),
  * "far_group" (source tiles each far-kernel warp sums before writing its
  *   partial, table handles; default 4, mixed precision 2 below 256 tiles;
  *   changes the summation grouping, so results change in the last bits),
@@ -369,7 +372,7 @@ qg_status qg_set_option(qg_handle *h, const char *key, int value);
 
 /* Reads an option back: "graph", "profile", "far_variant" (the variant in
  * use, which after the first qg_run is the autotuner's choice), "block_step",
- * "far_group", "tune_group", "wait_limit", "test_skip_post", "coef_mode" (QG_COEF_TABLE or
+ * "far_group", "tune_group", "far_early", "wait_limit", "test_skip_post", "coef_mode" (QG_COEF_TABLE or
  * QG_COEF_ON_THE_FLY: the form in use), "tuned_far_us" (the far kernel's
  * launch time the autotuner measured for its choice, microseconds; 0 if it
  * did not run).  No reference counterpart (the reference has no options). */

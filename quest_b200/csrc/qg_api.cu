@@ -111,12 +111,14 @@ struct qg_handle_s {
   int next_step = 0;
   int eval_cached = -0x7fffffff;
 
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // K-step block: [traj off, traj on]
+  // K-step block graphs, [traj off, traj on] + 2 for blocks whose far launch
+  // takes its first-blocks form (some windows start before step -22)
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   // profiling in graph mode: kProfRing instances of the block graph, each
   // with its own events around the far kernel and around the K step kernels;
   // an instance's times are collected when it is reused, so the stream stays full
   static constexpr int kProfRing = 8;
-  cudaGraphExec_t gprof[2][kProfRing] = {};
+  cudaGraphExec_t gprof[4][kProfRing] = {};
   cudaEvent_t pev[kProfRing][3];
   bool pev_ready = false, pending[kProfRing] = {};
   int prof_next = 0;
@@ -125,6 +127,7 @@ struct qg_handle_s {
   float tuned_far_ms = 0;  // far-kernel time of the autotuner's choice
   bool tune_coef = false;  // QG_COEF_TUNED: also time the on-the-fly kernel against the table
   bool tune_group = false;  // "tune_group": also time source tiles per warp 1, 2, 4, 8
+  bool far_early = true;    // "far_early": the far kernels' first-blocks form where it applies
   bool tune_pending = false;  // the far-kernel autotuner runs at the first qg_run
   bool profile = false;
   // first bad step as the last batch run read it (qg_bad_step answers from it
@@ -1267,7 +1270,11 @@ static void record_event(qg_handle *h, cudaEvent_t e)
     cudaEventRecord(e, h->stream);
 }
 
-static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, cudaEvent_t eb)
+// Far blocks before this step start some windows before step -22 (the far
+// kernels' first-blocks form is faster there; both forms give the same bits).
+static bool early_block(const qg_handle *h, int t0) { return h->far_early && t0 < h->max_delay + h->q - kWindow; }
+
+static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, cudaEvent_t eb, bool early)
 {
   // at a boundary the previous block's last step kernel (or launch_steps)
   // has stored t0 in d_ints[0]; that read keeps the launch graph-capturable
@@ -1277,7 +1284,9 @@ static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, 
     src = h->d_ints + 7;
   }
   if(ea) record_event(h, ea);
-  launch_far(h->far_args(src, h->d_ints + 6), h->stream);
+  FarArgs fa = h->far_args(src, h->d_ints + 6);
+  fa.early = early ? 1 : 0;
+  launch_far(fa, h->stream);
   if(eb) record_event(h, eb);
 }
 
@@ -1302,11 +1311,13 @@ static void enqueue_dot_step(qg_handle *h, int k, bool traj)
 
 // One K-step block starting on a boundary: far kernel + K dot steps
 // (prof >= 0: instance `prof` of the profiling ring, with event nodes).
-static qg_status capture_block(qg_handle *h, int traj, int prof, cudaGraphExec_t *out)
+static qg_status capture_block(qg_handle *h, int gi, int prof, cudaGraphExec_t *out)
 {
+  const int traj = gi & 1;
   cudaGraph_t g;
   QG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_far(h, 0, true, prof >= 0 ? h->pev[prof][0] : nullptr, prof >= 0 ? h->pev[prof][1] : nullptr);
+  enqueue_far(h, 0, true, prof >= 0 ? h->pev[prof][0] : nullptr, prof >= 0 ? h->pev[prof][1] : nullptr,
+              gi >= 2);
   if(h->block_step)
     enqueue_step_block(h, 0, kTimeBlock, traj != 0);
   else
@@ -1318,10 +1329,10 @@ static qg_status capture_block(qg_handle *h, int traj, int prof, cudaGraphExec_t
   return QG_OK;
 }
 
-static qg_status ensure_graph(qg_handle *h, int traj)
+static qg_status ensure_graph(qg_handle *h, int gi)
 {
-  if(h->graph[traj]) return QG_OK;
-  return capture_block(h, traj, -1, &h->graph[traj]);
+  if(h->graph[gi]) return QG_OK;
+  return capture_block(h, gi, -1, &h->graph[gi]);
 }
 
 static qg_status collect_prof(qg_handle *h, int i)
@@ -1339,7 +1350,7 @@ static qg_status collect_prof(qg_handle *h, int i)
   return QG_OK;
 }
 
-static qg_status launch_prof_block(qg_handle *h, int traj)
+static qg_status launch_prof_block(qg_handle *h, int gi)
 {
   if(!h->pev_ready) {
     for(auto &row : h->pev)
@@ -1349,8 +1360,8 @@ static qg_status launch_prof_block(qg_handle *h, int traj)
   const int i = h->prof_next;
   h->prof_next = (h->prof_next + 1) % qg_handle_s::kProfRing;
   QG_TRY(collect_prof(h, i));
-  if(!h->gprof[traj][i]) QG_TRY(capture_block(h, traj, i, &h->gprof[traj][i]));
-  QG_CUDA(cudaGraphLaunch(h->gprof[traj][i], h->stream));
+  if(!h->gprof[gi][i]) QG_TRY(capture_block(h, gi, i, &h->gprof[gi][i]));
+  QG_CUDA(cudaGraphLaunch(h->gprof[gi][i], h->stream));
   h->pending[i] = true;
   return QG_OK;
 }
@@ -1401,10 +1412,11 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
     const int t0 = t - t % kTimeBlock;
     if(t == t0 && count >= kTimeBlock && h->use_graph) {
       if(h->profile) {
-        QG_TRY(launch_prof_block(h, traj ? 1 : 0));
+        QG_TRY(launch_prof_block(h, (traj ? 1 : 0) + (early_block(h, t0) ? 2 : 0)));
       } else {
-        QG_TRY(ensure_graph(h, traj ? 1 : 0));
-        QG_CUDA(cudaGraphLaunch(h->graph[traj ? 1 : 0], h->stream));
+        const int gi = (traj ? 1 : 0) + (early_block(h, t0) ? 2 : 0);
+        QG_TRY(ensure_graph(h, gi));
+        QG_CUDA(cudaGraphLaunch(h->graph[gi], h->stream));
       }
       h->far_block = t0;
       t += kTimeBlock;
@@ -1413,7 +1425,7 @@ static qg_status launch_steps(qg_handle *h, int t, int count, bool traj)
     }
     if(h->far_block != t0) {
       enqueue_far(h, t0, t == t0, h->profile ? h->ev_a[nev] : nullptr,
-                  h->profile ? h->ev_b[nev] : nullptr);
+                  h->profile ? h->ev_b[nev] : nullptr, early_block(h, t0));
       if(h->profile) ++nev;
       h->far_block = t0;
     }
@@ -1520,7 +1532,7 @@ extern "C" qg_status qg_shard_step(qg_handle *h, double *d_slice)
   h->batch_bad_valid = false;
   const int t = h->next_step, t0 = t - t % kTimeBlock;
   if(h->far_block != t0) {
-    enqueue_far(h, t0, false, nullptr, nullptr);
+    enqueue_far(h, t0, false, nullptr, nullptr, early_block(h, t0));
     h->far_block = t0;
   }
   enqueue_dot_step(h, t - t0, false);
@@ -2402,8 +2414,11 @@ extern "C" qg_status qg_set_option(qg_handle *h, const char *key, int value)
     h->profile = value != 0;
   } else if(!std::strcmp(key, "far_variant") || !std::strcmp(key, "block_step") ||
             !std::strcmp(key, "far_group") || !std::strcmp(key, "wait_limit") ||
-            !std::strcmp(key, "test_skip_post") || !std::strcmp(key, "tune_group")) {
-    if(!std::strcmp(key, "tune_group")) {
+            !std::strcmp(key, "test_skip_post") || !std::strcmp(key, "tune_group") ||
+            !std::strcmp(key, "far_early")) {
+    if(!std::strcmp(key, "far_early")) {
+      h->far_early = value != 0;
+    } else if(!std::strcmp(key, "tune_group")) {
       if(h->otf) return qg_fail(QG_ERR_UNSUPPORTED, "qg_set_option: tune_group is for table handles");
       h->tune_group = value != 0;
       if(h->tune_group) h->tune_pending = true;  // the next run times the groups
@@ -2495,6 +2510,8 @@ extern "C" qg_status qg_get_option(const qg_handle *h, const char *key, int *val
     *value = h->skip_post;
   else if(!std::strcmp(key, "tune_group"))
     *value = h->tune_group ? 1 : 0;
+  else if(!std::strcmp(key, "far_early"))
+    *value = h->far_early ? 1 : 0;
   else
     return qg_fail(QG_ERR_INVALID_ARG, "qg_get_option: unknown key '%s'", key);
   return QG_OK;

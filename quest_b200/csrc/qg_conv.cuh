@@ -50,6 +50,48 @@ __device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int 
   }
 }
 
+__device__ __forceinline__ bool finite2(double2 v) { return isfinite(v.x) && isfinite(v.y); }
+
+// window_conv's result for the first blocks of a run, where some lanes'
+// windows start before step -22 and others do not: rather than split such a
+// warp between window_conv's two loops, every lane runs one loop in which a
+// sample before step -22 is replaced by zero.  Its products are +-0, and
+// adding +-0 leaves an accumulator that started at +0 bit for bit as it was
+// (a sum is -0 only when both addends are), so each lane gets the skipping
+// loop's result.  A pair with a non-finite coefficient (an integer delay)
+// takes window_conv itself, so its NaN appears at the step where the
+// reference's does.
+template <int Q, bool LAB, int K>
+__device__ __forceinline__ void window_conv_uniform(const double2 *ring, int slot0, int tau0,
+                                                    const double2 (&c)[Q + 1], double2 (&acc)[K])
+{
+  // A warp whose windows are all live, or all partly dead, takes
+  // window_conv, which then runs one loop for all its lanes (the second
+  // skips the dead samples' work); only a warp with both kinds runs the
+  // zeroing loop.  The votes only pick a loop: every loop gives the same
+  // bits for its lane.
+  const unsigned act = __activemask();
+  const bool live = tau0 >= -kWindow;
+  if(__all_sync(act, live) || __all_sync(act, !live)) {
+    window_conv<Q, LAB, K>(ring, slot0, tau0, c, acc);
+    return;
+  }
+  bool fin = true;
+#pragma unroll
+  for(int i = 0; i <= Q; ++i) fin = fin && finite2(c[i]);
+  if(!fin) {
+    window_conv<Q, LAB, K>(ring, slot0, tau0, c, acc);
+    return;
+  }
+#pragma unroll
+  for(int m = 0; m < K + Q; ++m) {
+    double2 w = ring_pref<LAB>(ring + slot0 + m);
+    if(tau0 + m < -kWindow) w = make_double2(0.0, 0.0);
+#pragma unroll
+    for(int k = (m - Q > 0 ? m - Q : 0); k <= (m < K - 1 ? m : K - 1); ++k) cfma(acc[k], c[k + Q - m], w);
+  }
+}
+
 // Two samples per 32-byte load (ld.global.nc.v4.f64).  Ring rows start on
 // 32-byte boundaries (even row stride, 16-byte samples), so a load must start
 // at an even slot.

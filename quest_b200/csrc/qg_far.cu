@@ -78,7 +78,7 @@ __device__ __forceinline__ void window_conv2(const double2 *ring, int slot_even,
 // K outputs: the first K steps of the block (K = kTimeBlock in the run; 1 for
 // a single-step evaluation).  Pairs with delay < kTimeBlock are left to the
 // mid list in either case.
-template <int Q, bool LAB, int VEC, int K = kTimeBlock>
+template <int Q, bool LAB, int VEC, int K = kTimeBlock, bool EARLY = false>
 __device__ __forceinline__ void far_body(const FarArgs &a, int task)
 {
   const int lane = threadIdx.x & 31;
@@ -127,6 +127,8 @@ __device__ __forceinline__ void far_body(const FarArgs &a, int task)
           window_conv2<Q, LAB, 1, K>(row, slot0 - 1, tau0, c, acc);
         else
           window_conv2<Q, LAB, 0, K>(row, slot0, tau0, c, acc);
+      } else if(EARLY) {
+        window_conv_uniform<Q, LAB, K>(row, slot0, tau0, c, acc);
       } else {
         window_conv<Q, LAB, K>(row, slot0, tau0, c, acc);
       }
@@ -631,6 +633,15 @@ __device__ __forceinline__ void far_body_mixed(const FarArgs &a, int task)
 
 template <int Q, bool LAB>
 __global__ void __launch_bounds__(128) far_kernel(FarArgs a) { far_body<Q, LAB, 0>(a, warp_task()); }
+// The same for the first blocks of a run (some windows start before step
+// -22): one loop for all lanes of a warp (window_conv_uniform), same
+// results; held to 3 blocks per SM like far_kernel (uncapped, its extra loop
+// takes 182 registers and 2 blocks).
+template <int Q, bool LAB>
+__global__ void __launch_bounds__(128, 3) far_kernel_early(FarArgs a)
+{
+  far_body<Q, LAB, 0, kTimeBlock, true>(a, warp_task());
+}
 template <int Q, bool LAB>
 __global__ void __launch_bounds__(128, 4) far_kernel_r4(FarArgs a) { far_body<Q, LAB, 0>(a, warp_task()); }
 template <int Q, bool LAB>
@@ -787,6 +798,8 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
     else
       far_kernel_async<Q, LAB, 2><<<blocks, 128, smem5, s>>>(a);
   }
+  else if(a.early)
+    far_kernel_early<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else
     far_kernel<Q, LAB><<<blocks, 128, 0, s>>>(a);
 }

@@ -87,6 +87,9 @@ struct FarArgs {
   // the same sums either way
   int gmajor;
   int *d_bad;           // a far-kernel wait that ran out sets it to -3
+  // 1: some windows may start before step -22 (the first blocks of a run);
+  // variants 0 and 7 then take their one-loop form (same results)
+  int early;
   // on-the-fly coefficients (no table): dot data, constants, and the source
   // tiles per warp (nG = ceil(nT / group) groups)
   int otf;

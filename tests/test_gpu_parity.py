@@ -344,6 +344,25 @@ def test_staged_window_variants_on_long_and_short_runs(golden_weights, geometry)
         np.testing.assert_array_equal(outs[0], o)
 
 
+@pytest.mark.parametrize("variant", [0, 7])
+def test_first_blocks_form_changes_nothing(golden_weights, variant):
+    """The far kernel's first-blocks form (warps whose lanes' windows are
+    partly live run one loop with dead samples zeroed) gives the bits of the
+    two-loop form through all the blocks where windows still start before
+    step -22 (max delay ~300 steps here)."""
+    wl = I.plain_table(seed=4, n=1024, steps=400, pulse_delay=0.05)
+    wl.dots[:, 6:9] *= 0.1
+    outs = []
+    for early in (1, 0):
+        with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights) as sim:
+            sim.set_option("far_variant", variant)
+            sim.set_option("far_early", early)
+            assert sim.get_option("far_early") == early
+            outs.append(sim.run(400))
+    assert np.abs(outs[0][..., 1]).max() > 1e-8
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
 def test_far_autotuner_runs_at_the_first_run_and_keeps_an_explicit_choice(golden_weights):
     """FP64 table handles of 512 dots or more time the far variants at their
     first qg_run and keep the fastest; a variant set before that run is kept.
