@@ -1360,7 +1360,11 @@ static qg_status launch_prof_block(qg_handle *h, int gi)
   const int i = h->prof_next;
   h->prof_next = (h->prof_next + 1) % qg_handle_s::kProfRing;
   QG_TRY(collect_prof(h, i));
-  if(!h->gprof[gi][i]) QG_TRY(capture_block(h, gi, i, &h->gprof[gi][i]));
+  // a form's whole ring at its first use, so that the instances are made
+  // while a caller warms up, not in a later timed block
+  if(!h->gprof[gi][i])
+    for(int j = 0; j < qg_handle_s::kProfRing; ++j)
+      if(!h->gprof[gi][j]) QG_TRY(capture_block(h, gi, j, &h->gprof[gi][j]));
   QG_CUDA(cudaGraphLaunch(h->gprof[gi][i], h->stream));
   h->pending[i] = true;
   return QG_OK;
