@@ -128,6 +128,7 @@ struct qg_handle_s {
   bool tune_coef = false;  // QG_COEF_TUNED: also time the on-the-fly kernel against the table
   bool tune_group = false;  // "tune_group": also time source tiles per warp 1, 2, 4, 8
   bool far_early = true;    // "far_early": the far kernels' first-blocks form where it applies
+  bool far_nonfinite = false;  // a far pair's table coefficient is not finite (integer delay)
   bool tune_pending = false;  // the far-kernel autotuner runs at the first qg_run
   bool profile = false;
   // first bad step as the last batch run read it (qg_bad_step answers from it
@@ -956,7 +957,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaGetLastError());
   QG_CUDA(cudaEventRecord(e1, h->stream));
   int md = 0;
-  unsigned long long nn[2] = {0, 0};
+  unsigned long long nn[4] = {0, 0, 0, 0};
   QG_CUDA(cudaMemcpyAsync(&md, h->d_ints + 5, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaMemcpyAsync(nn, h->d_u64, sizeof nn, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
@@ -971,6 +972,7 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   h->max_delay = md;
   h->near_pairs = (long long)nn[0];  // on the fly: counted from the mid list below
   h->mid_pairs = (long long)nn[1];
+  h->far_nonfinite = nn[3] > 0;
 
   // rings and scratch.  W covers the oldest sample a far block reads
   // (t0 - max_delay - q) even when the block is recomputed up to K - 1
@@ -1272,7 +1274,10 @@ static void record_event(qg_handle *h, cudaEvent_t e)
 
 // Far blocks before this step start some windows before step -22 (the far
 // kernels' first-blocks form is faster there; both forms give the same bits).
-static bool early_block(const qg_handle *h, int t0) { return h->far_early && t0 < h->max_delay + h->q - kWindow; }
+static bool early_block(const qg_handle *h, int t0)
+{
+  return h->far_early && !h->far_nonfinite && t0 < h->max_delay + h->q - kWindow;
+}
 
 static void enqueue_far(qg_handle *h, int t0, bool at_boundary, cudaEvent_t ea, cudaEvent_t eb, bool early)
 {

@@ -50,17 +50,15 @@ __device__ __forceinline__ void window_conv(const double2 *ring, int slot0, int 
   }
 }
 
-__device__ __forceinline__ bool finite2(double2 v) { return isfinite(v.x) && isfinite(v.y); }
-
 // window_conv's result for the first blocks of a run, where some lanes'
 // windows start before step -22 and others do not: rather than split such a
 // warp between window_conv's two loops, every lane runs one loop in which a
-// sample before step -22 is replaced by zero.  Its products are +-0, and
-// adding +-0 leaves an accumulator that started at +0 bit for bit as it was
-// (a sum is -0 only when both addends are), so each lane gets the skipping
-// loop's result.  A pair with a non-finite coefficient (an integer delay)
-// takes window_conv itself, so its NaN appears at the step where the
-// reference's does.
+// sample before step -22 is replaced by zero.  Its products are +-0 (the
+// coefficients are finite: a table with a non-finite far coefficient, from
+// an integer delay, never takes this form, so such a NaN still appears at
+// the step where the reference's does), and adding +-0 leaves an
+// accumulator that started at +0 bit for bit as it was (a sum is -0 only
+// when both addends are), so each lane gets the skipping loop's result.
 template <int Q, bool LAB, int K>
 __device__ __forceinline__ void window_conv_uniform(const double2 *ring, int slot0, int tau0,
                                                     const double2 (&c)[Q + 1], double2 (&acc)[K])
@@ -73,13 +71,6 @@ __device__ __forceinline__ void window_conv_uniform(const double2 *ring, int slo
   const unsigned act = __activemask();
   const bool live = tau0 >= -kWindow;
   if(__all_sync(act, live) || __all_sync(act, !live)) {
-    window_conv<Q, LAB, K>(ring, slot0, tau0, c, acc);
-    return;
-  }
-  bool fin = true;
-#pragma unroll
-  for(int i = 0; i <= Q; ++i) fin = fin && finite2(c[i]);
-  if(!fin) {
     window_conv<Q, LAB, K>(ring, slot0, tau0, c, acc);
     return;
   }

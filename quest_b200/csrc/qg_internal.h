@@ -58,7 +58,9 @@ struct TableArgs {
   float2 *coef32;      // mixed: [nT][nT][q+2][kTilePairs] (taps, then their sum)
   int mixed;
   int *max_delay;      // atomicMax
-  unsigned long long *near_count;  // [0] pairs with delay 0, [1] pairs with delay < K
+  // [0] pairs with delay 0, [1] pairs with delay < K, [3] pairs with delay
+  // >= K and a non-finite coefficient ([2] is the list builder's counter)
+  unsigned long long *near_count;
   CoefParams cp;
 };
 
@@ -87,8 +89,9 @@ struct FarArgs {
   // the same sums either way
   int gmajor;
   int *d_bad;           // a far-kernel wait that ran out sets it to -3
-  // 1: some windows may start before step -22 (the first blocks of a run);
-  // variants 0 and 7 then take their one-loop form (same results)
+  // 1: some windows may start before step -22 (the first blocks of a run)
+  // and every far pair's coefficients are finite; variants 0 and 7 then take
+  // their first-blocks form (same results)
   int early;
   // on-the-fly coefficients (no table): dot data, constants, and the source
   // tiles per warp (nG = ceil(nT / group) groups)

@@ -99,6 +99,14 @@ __global__ void __launch_bounds__(128) table_build_kernel(TableArgs a)
   atomicMax(a.max_delay, fd);
   if(fd == 0) atomicAdd(a.near_count, 1ULL);
   if(fd < kTimeBlock) atomicAdd(a.near_count + 1, 1ULL);
+  if(fd >= kTimeBlock) {
+    // far pairs with a non-finite coefficient (an integer delay): the far
+    // kernels' first-blocks form is not used for such a table
+    bool fin = true;
+#pragma unroll
+    for(int i = 0; i <= Q; ++i) fin = fin && isfinite(coef[i].x) && isfinite(coef[i].y);
+    if(!fin) atomicAdd(a.near_count + 3, 1ULL);
+  }
 }
 
 template <bool MIXED>
