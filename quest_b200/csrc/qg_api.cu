@@ -486,6 +486,15 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   // their FP64 coefficients: the mid list is FP64 in both precisions
   int *d_pairs = nullptr;
   double2 *d_mc = nullptr;
+  // the temporaries go back to the pool on every return path
+  struct Temp {
+    qg_handle *h;
+    void **p;
+    ~Temp()
+    {
+      if(*p) pool_free(h, *p);
+    }
+  } keep_pairs{h, (void **)&d_pairs}, keep_mc{h, (void **)&d_mc};
   unsigned long long cnt = 0;
   const double c0dt = h->params.c0 * h->params.dt;
   for(int pass = 0; pass < 2; ++pass) {
@@ -510,7 +519,7 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   QG_CUDA(cudaMemcpyAsync(mc.data(), d_mc, sizeof(double2) * q1 * cap, cudaMemcpyDeviceToHost, h->stream));
   QG_CUDA(cudaStreamSynchronize(h->stream));
   pool_free(h, d_pairs);
-  pool_free(h, d_mc);
+  d_pairs = nullptr;
   const long long m = h->mid_pairs;
   const int n = h->n_pad;  // internal indices (padding holes have no pairs)
 
@@ -547,15 +556,17 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
       dsu.unite(a, b);
     }
   }
+  // the entries' coefficients are gathered into list order on the device
+  // (msrc[e] = the entry's pair), from the pair-order array still there
   std::vector<int> midx((size_t)mptr[n]), mdel((size_t)mptr[n]);
-  std::vector<double2> mcoef((size_t)mptr[n] * q1);
+  std::vector<long long> msrc((size_t)mptr[n]);
   for(int i = 0; i < n; ++i) {
     std::sort(ment.begin() + mptr[i], ment.begin() + mptr[i + 1],
               [](const MidEntry &x, const MidEntry &y) { return x.b < y.b; });
     for(int e = mptr[i]; e < mptr[i + 1]; ++e) {
       midx[e] = ment[e].b;
       mdel[e] = ment[e].d;
-      std::memcpy(&mcoef[(size_t)e * q1], &mc[ment[e].k * q1], sizeof(double2) * q1);
+      msrc[e] = ment[e].k;
     }
   }
   for(auto &v : adj)
@@ -677,7 +688,23 @@ static qg_status build_lists(qg_handle *h, const TableArgs &ta)
   QG_TRY(upload_i(&h->d_mid_ptr, mptr));
   QG_TRY(upload_i(&h->d_mid_idx, midx));
   QG_TRY(upload_i(&h->d_mid_delay, mdel));
-  QG_TRY(upload_c(&h->d_mid_coef, mcoef));
+  {
+    const long long ne = (long long)midx.size();
+    QG_TRY(dalloc(h, &h->d_mid_coef, (size_t)ne * q1));
+    long long *d_msrc = nullptr;
+    cudaError_t ce = pool_alloc(h, (void **)&d_msrc, sizeof(long long) * (size_t)std::max<long long>(ne, 1));
+    if(ce == cudaSuccess && ne > 0)
+      ce = cudaMemcpyAsync(d_msrc, msrc.data(), sizeof(long long) * (size_t)ne, cudaMemcpyHostToDevice, h->stream);
+    if(ce == cudaSuccess) {
+      launch_gather_rows(d_mc, d_msrc, q1, ne, h->d_mid_coef, h->stream);
+      ce = cudaGetLastError();
+    }
+    if(ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+    pool_free(h, d_msrc);
+    pool_free(h, d_mc);
+    d_mc = nullptr;
+    QG_CUDA(ce);
+  }
   QG_TRY(upload_i(&h->d_gnear_ptr, gptr));
   QG_TRY(upload_i(&h->d_gnear_idx, gidx));
   QG_TRY(upload_c(&h->d_gnear_coef, gcoef));

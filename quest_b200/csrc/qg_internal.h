@@ -214,6 +214,9 @@ void launch_max_delay(const double *pos, const int *user, int n_pad, double c0dt
 void launch_near_find(const double *pos, const int *user, int n_pad, double c0dt, int below, int *out_pairs,
                       unsigned long long *counter, unsigned long long cap, void *stream);
 void launch_pair_list_coef(const TableArgs &a, int q, const int *pairs, long long m, double2 *out, void *stream);
+// dst[j][0 .. width) = src[rows[j]][0 .. width), j < n
+void launch_gather_rows(const double2 *src, const long long *rows, int width, long long n, double2 *dst,
+                        void *stream);
 void launch_step_fused(const StepArgs &a, int k, int nblocks, void *stream);
 void launch_step_general(const StepArgs &a, int k, int phase, void *stream);
 void launch_eval_field(const StepArgs &a, const int *d_eval_step, double2 *out_user, void *stream);

@@ -234,6 +234,25 @@ __global__ void pair_list_coef_kernel(TableArgs a, const int *pairs, long long m
   for(int i = 0; i <= Q; ++i) out[k * (Q + 1) + i] = coef[i];
 }
 
+// dst row j (width values) = src row rows[j]: the mid list's coefficients
+// placed in list order on the device, from the pair-order array
+__global__ void gather_rows_kernel(const double2 *__restrict__ src, const long long *__restrict__ rows, int width,
+                                   long long n, double2 *__restrict__ dst)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n * width) return;
+  const long long j = i / width;
+  dst[i] = src[rows[j] * width + (i - j * width)];
+}
+
+void launch_gather_rows(const double2 *src, const long long *rows, int width, long long n, double2 *dst,
+                        void *stream)
+{
+  const long long total = n * width;
+  if(total <= 0) return;
+  gather_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(src, rows, width, n, dst);
+}
+
 void launch_pair_list_coef(const TableArgs &a, int q, const int *pairs, long long m, double2 *out, void *stream)
 {
   if(m <= 0) return;
