@@ -339,7 +339,9 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  *   variant was set; mixed-precision
  *   table handles choose the same way among 0, 7 (its kernel at 150
  *   registers, target-tile and source-group major) and 1, 8 (at 128);
- *   on-the-fly handles take 7 for the source-group-major order; the
+ *   on-the-fly handles take 8 (source-group-major order, held to 3 blocks
+ *   per SM; 0 and 3: target-tile major, 1: held, 7: source-group major,
+ *   all with the same results); the
  *   choice is remembered for the process, and later handles of the same kind
  *   (device, size, order, frame, precision, coefficient mode) take it
  *   without timing; batch members are not timed, the batch kernel having its

@@ -49,6 +49,10 @@ extern "C" const char *qg_version(void) { return "quest_b200 0.1 (sm_100a)"; }
     }                                                                                        \
   } while(0)
 
+// The on-the-fly far kernel's form: source-group-major tasks, held to 3
+// blocks per SM (qg_otf.cu variant 8).
+constexpr int kOtfVariant = 8;
+
 struct qg_handle_s {
   int n = 0, n_pad = 0, nT = 0, q = 0, T = 0;
   long long nblk = 0, P = 0;
@@ -937,6 +941,10 @@ static qg_status create_impl(const qg_dot *dots, int n, const qg_pulse *pulse, c
   QG_CUDA(cudaMemGetInfo(&free_b, &total_b));
   const bool rule = p->coef_mode == QG_COEF_AUTO || p->coef_mode == QG_COEF_TUNED;
   h->otf = p->coef_mode == QG_COEF_ON_THE_FLY || (rule && tb > free_b / 2);
+  // on the fly: source-group-major tasks, 3 blocks per SM (measured at
+  // N = 65536: 274 against 322 ms per FP64 launch for 7, 168 against 177
+  // mixed; same sums)
+  if(h->otf) h->far_variant = kOtfVariant;
   h->tune_coef = p->coef_mode == QG_COEF_TUNED && !h->otf;
   if(!h->otf && tb > free_b * 0.9)
     return qg_fail(QG_ERR_OOM, "qg_create: coefficient table needs %zu bytes, %zu free", tb, free_b);
@@ -1076,16 +1084,18 @@ static qg_status time_far(qg_handle *h, int rounds_untimed, int rounds_timed, fl
 // table.
 static qg_status autotune_coef(qg_handle *h)
 {
-  const int group_t = h->group, nG_t = h->nG;
+  const int group_t = h->group, nG_t = h->nG, variant_t = h->far_variant;
   h->otf = true;
   h->group = (h->nT + 15) / 16;
   h->nG = (h->nT + h->group - 1) / h->group;
+  h->far_variant = kOtfVariant;
   float otf_ms = 0;
   const qg_status st = time_far(h, 2, 3, &otf_ms);
   if(st != QG_OK || otf_ms >= h->tuned_far_ms) {
     h->otf = false;
     h->group = group_t;
     h->nG = nG_t;
+    h->far_variant = variant_t;
     return st;
   }
   // the on-the-fly kernel is faster: keep it, return the table's memory
@@ -1099,6 +1109,7 @@ static qg_status autotune_coef(qg_handle *h)
 static qg_status switch_to_otf(qg_handle *h)
 {
   h->otf = true;
+  h->far_variant = kOtfVariant;
   h->group = (h->nT + 15) / 16;
   h->nG = (h->nT + h->group - 1) / h->group;
   QG_CUDA(cudaStreamSynchronize(h->stream));

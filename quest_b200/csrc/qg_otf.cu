@@ -109,38 +109,57 @@ __global__ void __launch_bounds__(128) far_otf_kernel(FarArgs a)
   far_body_otf<Q, LAB, MIXED>(a, blockIdx.x * 4 + (threadIdx.x >> 5));
 }
 
+// The same held to 3 blocks per SM (the FP64 form takes 186 registers and
+// fits 2 uncapped); same results.
+template <int Q, bool LAB, bool MIXED>
+__global__ void __launch_bounds__(128, 3) far_otf_kernel_r3(FarArgs a)
+{
+  far_body_otf<Q, LAB, MIXED>(a, blockIdx.x * 4 + (threadIdx.x >> 5));
+}
+
 template <bool LAB, bool MIXED>
-static void launch_otf_q(const FarArgs &a, cudaStream_t s)
+static void launch_otf_q(const FarArgs &a, bool r3, cudaStream_t s)
 {
   const unsigned blocks = (unsigned)(((long long)(a.tile_n > 0 ? a.tile_n : a.nT) * a.nG + 3) / 4);
+#define QG_OTF_CASE(QQ)                                                  \
+  case QQ:                                                               \
+    if(r3)                                                               \
+      far_otf_kernel_r3<QQ, LAB, MIXED><<<blocks, 128, 0, s>>>(a);       \
+    else                                                                 \
+      far_otf_kernel<QQ, LAB, MIXED><<<blocks, 128, 0, s>>>(a);          \
+    break;
   switch(a.q) {
-    case 1: far_otf_kernel<1, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
-    case 2: far_otf_kernel<2, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
-    case 3: far_otf_kernel<3, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
-    case 4: far_otf_kernel<4, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
-    case 5: far_otf_kernel<5, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
-    case 6: far_otf_kernel<6, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
-    case 7: far_otf_kernel<7, LAB, MIXED><<<blocks, 128, 0, s>>>(a); break;
+    QG_OTF_CASE(1)
+    QG_OTF_CASE(2)
+    QG_OTF_CASE(3)
+    QG_OTF_CASE(4)
+    QG_OTF_CASE(5)
+    QG_OTF_CASE(6)
+    QG_OTF_CASE(7)
     default: break;
   }
+#undef QG_OTF_CASE
 }
 
 void launch_far_otf(const FarArgs &a0, void *stream)
 {
   if(a0.nT <= 0) return;
   FarArgs a = a0;
-  a.gmajor = a0.variant == 7;  // source-group-major task order (same sums)
+  // 7 and 8: source-group-major task order; 1 and 8: held to 3 blocks per
+  // SM (same sums either way)
+  a.gmajor = a0.variant == 7 || a0.variant == 8;
+  const bool r3 = a0.variant == 1 || a0.variant == 8;
   cudaStream_t s = (cudaStream_t)stream;
   if(a.frame == 0) {
     if(a.mixed)
-      launch_otf_q<false, true>(a, s);
+      launch_otf_q<false, true>(a, r3, s);
     else
-      launch_otf_q<false, false>(a, s);
+      launch_otf_q<false, false>(a, r3, s);
   } else {
     if(a.mixed)
-      launch_otf_q<true, true>(a, s);
+      launch_otf_q<true, true>(a, r3, s);
     else
-      launch_otf_q<true, false>(a, s);
+      launch_otf_q<true, false>(a, r3, s);
   }
 }
 

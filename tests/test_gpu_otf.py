@@ -199,14 +199,16 @@ def test_otf_n65536_evaluate_sampled_targets_against_oracle(golden_weights):
 
 @pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
 def test_otf_task_orders_agree_bitwise(golden_weights, precision):
-    """far_variant 7 runs the on-the-fly kernel's tasks source-group major;
-    each target's sums are unchanged."""
+    """far_variant 7 runs the on-the-fly kernel's tasks source-group major,
+    1 holds it to 3 blocks per SM, 8 does both; each target's sums are
+    unchanged."""
     wl = stable(1000, 96, 0.1)
     outs = []
-    for v in (None, 7):
+    for v in (None, 7, 1, 8):
         with capi.Simulation(wl.dots, wl.pulse, wl.constants, weights=golden_weights, precision=precision,
                              coef_mode=capi.COEF_ON_THE_FLY) as sim:
             if v is not None:
                 sim.set_option("far_variant", v)
             outs.append(sim.run(96))
-    np.testing.assert_array_equal(outs[0], outs[1])
+    for o in outs[1:]:
+        np.testing.assert_array_equal(outs[0], o)
