@@ -348,9 +348,10 @@ qg_status qg_kernel_time(qg_handle *h, int reset, double *pair_ms, int *pair_lau
  *   own),
  * "autotune" (1 = time the far-kernel variants again now; at a block
  *   boundary between runs),
- * "far_early" (1 = the default: far variants 0 and 7 use their first-blocks
- *   form in the blocks where some windows start before step -22, one loop
- *   for all lanes of a warp instead of two; 0 = never; same results),
+ * "far_early" (1 = the default: FP64 table handles use the far kernel's
+ *   first-blocks form, whatever the variant, in the blocks where some
+ *   windows start before step -22: one loop for all lanes of a warp instead
+ *   of two; 0 = never; same results),
  * "far_group" (source tiles each far-kernel warp sums before writing its
  *   partial, table handles; default 4, mixed precision 2 below 256 tiles;
  *   changes the summation grouping, so results change in the last bits),

@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(128) far_kernel_wstage(FarArgs a)
 // Variant 6 is held to 128 registers (4 blocks, 16 warps per SM); uncapped
 // it takes 132 and fits 3 blocks.
 template <int Q, bool LAB, int VEC>
-__global__ void __launch_bounds__(128, VEC == 3 ? 4 : 1) far_kernel_async(FarArgs a)
+__global__ void __launch_bounds__(128, VEC == 3 ? 4 : 3) far_kernel_async(FarArgs a)
 {
   extern __shared__ double2 far_smem[];
   constexpr int P = VEC == 2 ? kFarStages + 1 : kFarStages;
@@ -748,6 +748,13 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
       far_kernel_mixed<Q, LAB><<<blocks, 128, 0, s>>>(a);
     return;
   }
+  // the first blocks of a run take the first-blocks form whatever the
+  // variant (every variant gives the same bits), source-group major
+  if(a.early) {
+    a.gmajor = 1;
+    far_kernel_early<Q, LAB><<<blocks, 128, 0, s>>>(a);
+    return;
+  }
   // variants 7 and 8 are 0 and 3 with the source-group-major task order
   if(a.variant == 7 || a.variant == 8) {
     a.gmajor = 1;
@@ -798,8 +805,6 @@ static void launch_far_q(const FarArgs &a0, cudaStream_t s)
     else
       far_kernel_async<Q, LAB, 2><<<blocks, 128, smem5, s>>>(a);
   }
-  else if(a.early)
-    far_kernel_early<Q, LAB><<<blocks, 128, 0, s>>>(a);
   else
     far_kernel<Q, LAB><<<blocks, 128, 0, s>>>(a);
 }

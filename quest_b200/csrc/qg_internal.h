@@ -90,8 +90,8 @@ struct FarArgs {
   int gmajor;
   int *d_bad;           // a far-kernel wait that ran out sets it to -3
   // 1: some windows may start before step -22 (the first blocks of a run)
-  // and every far pair's coefficients are finite; variants 0 and 7 then take
-  // their first-blocks form (same results)
+  // and every far pair's coefficients are finite; the FP64 table launch then
+  // takes the first-blocks form whatever the variant (same results)
   int early;
   // on-the-fly coefficients (no table): dot data, constants, and the source
   // tiles per warp (nG = ceil(nT / group) groups)
